@@ -1,0 +1,649 @@
+// fcb_backproject.cu -- voxel-driven cone-beam backprojection for sm_100a.
+//
+// Replaces GPU_Feldkamp_backproject_sinogram / GPU_Katsevich_backproject_sinogram
+// (coneBeamGPU.cu:258-420), GPU_unweighted_backproject_sinogram (:178-255), their launchers
+// (:565-704) and the problem-solver drivers (unit_coneBeamGPU.cu:173-305).
+//
+// Two kernels:
+//  * fdk_tma_kernel -- aligned circular/helical geometry (FDK weight U^2, Katsevich U with
+//    optional Tam-Danielsson window, or unweighted).  A CTA owns a 16 x 16 x NZ voxel
+//    tile; per view a producer warp stages the tile's detector footprint (a fixed
+//    BW x BH box, zero-filled outside the caller's window) into shared memory with a TMA
+//    load, and 8 consumer warps interpolate bilinearly in FP32 from it.  Each thread owns
+//    one (x, y) column and NZ z-voxels held in registers; along z only the detector row
+//    changes, so the per-view work (U, w, weight) is amortised over NZ updates.  Per-view
+//    parameters travel in the kernel's parameter space (a constant bank).
+//  * bp_generic_kernel -- any detector orientation (misalignments) through a per-view 3x4
+//    projective matrix, bilinear gathers from global memory; also the fallback for
+//    projection buffers whose layout a TMA descriptor cannot describe.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "fcb_internal.h"
+
+namespace fcb {
+
+// =====================================================================================
+// TMA-staged FDK / Katsevich kernel
+// =====================================================================================
+struct FdkView {
+  float c0, c1;  // den = 1 + c0 x + c1 y ; U = 1 / den
+  float a0, a1;  // w = (a0 x + a1 y) U + wc
+  float wc, hc;  // local window index of the detector centre (w) / source height (h)
+  float e;       // h = U (hb z + e) + hc
+  float wt;      // normalisation factor of the view
+};
+
+constexpr int FDK_MAXV = 900;
+constexpr int FDK_TX = 16, FDK_TY = 16;
+constexpr int FDK_CWARPS = 8;                          // consumer warps
+constexpr int FDK_THREADS = (FDK_CWARPS + 1) * 32;     // + producer warp
+
+struct FdkParams {
+  float* vol;
+  int* status;
+  int nx, ny, nz;               // local sub-volume extents (x fastest)
+  int tiles_x, tiles_y, tiles_z;
+  float ox, oy, oz;             // coordinate of local voxel (0,0,0) relative to volDim/2
+  int nviews, view0;
+  int BW, BH, stages, wshift;
+  float hb;                     // 1 / pixelWidth
+  int wexp;                     // weight exponent: 2 FDK, 1 Katsevich, 0 unweighted
+  int piwin;                    // Tam-Danielsson window on/off
+  float td_a;                   // window half-height scale P / (2 pi pw), pixels
+  float td_r;                   // source-axis distance in pixels (D / pw)
+  float td_sign;                // +1/-1: sense of the helix relative to the w axis
+  FdkView v[FDK_MAXV];
+};
+
+static_assert(sizeof(FdkParams) + sizeof(CUtensorMap) < 32000, "kernel parameter space");
+
+__device__ __forceinline__ void fdk_footprint(const FdkParams& P, const FdkView& V, float x0,
+                                              float x1, float y0, float y1, float z0, float z1,
+                                              float& wmin, float& wmax, float& hmin, float& hmax)
+{
+  wmin = 3.0e38f; wmax = -3.0e38f; hmin = 3.0e38f; hmax = -3.0e38f;
+  const float hz0 = fmaf(P.hb, z0, V.e), hz1 = fmaf(P.hb, z1, V.e);
+#pragma unroll
+  for (int c = 0; c < 4; c++) {
+    const float x = (c & 1) ? x1 : x0, y = (c & 2) ? y1 : y0;
+    const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
+    const float U = __frcp_rn(den);
+    const float w = fmaf(fmaf(V.a0, x, V.a1 * y), U, V.wc);
+    const float ha = fmaf(U, hz0, V.hc), hb = fmaf(U, hz1, V.hc);
+    wmin = fminf(wmin, w); wmax = fmaxf(wmax, w);
+    hmin = fminf(hmin, fminf(ha, hb)); hmax = fmaxf(hmax, fmaxf(ha, hb));
+  }
+}
+
+__device__ __forceinline__ void fdk_tile(const FdkParams& P, int tile, int& tx, int& ty, int& tz)
+{
+  tx = tile % P.tiles_x;
+  const int r = tile / P.tiles_x;
+  ty = r % P.tiles_y;
+  tz = r / P.tiles_y;
+}
+
+// Box origin of (tile, view): the footprint's lower corner minus one pixel, w aligned down
+// to the TMA 16-byte rule.
+__device__ __forceinline__ void fdk_box_origin(const FdkParams& P, const FdkView& V, int tx,
+                                               int ty, int tz, int nzt, int& w0, int& h0,
+                                               int& needw, int& needh)
+{
+  const float x0 = P.ox + tx * FDK_TX, y0 = P.oy + ty * FDK_TY, z0 = P.oz + tz * nzt;
+  float wmin, wmax, hmin, hmax;
+  fdk_footprint(P, V, x0, x0 + (FDK_TX - 1), y0, y0 + (FDK_TY - 1), z0, z0 + (nzt - 1), wmin,
+                wmax, hmin, hmax);
+  // clamp far-away footprints so the integer math below stays defined
+  wmin = fminf(fmaxf(wmin, -1.0e6f), 1.0e6f); wmax = fminf(fmaxf(wmax, -1.0e6f), 1.0e6f);
+  hmin = fminf(fmaxf(hmin, -1.0e6f), 1.0e6f); hmax = fminf(fmaxf(hmax, -1.0e6f), 1.0e6f);
+  const int wlo = __float2int_rd(wmin) - 1;
+  w0 = (wlo >> P.wshift) << P.wshift;
+  h0 = __float2int_rd(hmin) - 1;
+  needw = __float2int_rd(wmax) + 3 - w0;
+  needh = __float2int_rd(hmax) + 3 - h0;
+}
+
+// Pre-pass: the largest footprint over all (tile, view) pairs sizes the staging box.
+__global__ void fdk_footprint_kernel(const __grid_constant__ FdkParams P, int nzt, int ntiles,
+                                     int* out_need)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long total = (long long)ntiles * P.nviews;
+  int mw = 0, mh = 0;
+  if (i < total) {
+    const int tile = (int)(i / P.nviews), v = (int)(i % P.nviews);
+    int tx, ty, tz;
+    fdk_tile(P, tile, tx, ty, tz);
+    int w0, h0, nw, nh;
+    fdk_box_origin(P, P.v[v], tx, ty, tz, nzt, w0, h0, nw, nh);
+    mw = nw;
+    mh = nh;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mw = max(mw, __shfl_xor_sync(0xffffffffu, mw, o));
+    mh = max(mh, __shfl_xor_sync(0xffffffffu, mh, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out_need, mw);
+    atomicMax(out_need + 1, mh);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ float ld_tap(const T* p);
+template <>
+__device__ __forceinline__ float ld_tap<float>(const float* p) { return *p; }
+template <>
+__device__ __forceinline__ float ld_tap<__half>(const __half* p) { return __half2float(*p); }
+template <>
+__device__ __forceinline__ float ld_tap<__nv_bfloat16>(const __nv_bfloat16* p)
+{
+  return __uint_as_float(((uint32_t)(*reinterpret_cast<const unsigned short*>(p))) << 16);
+}
+
+template <typename T, int NZ>
+__global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_constant__ CUtensorMap tmap,
+                                                              const __grid_constant__ FdkParams P)
+{
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int stage_elems = P.BW * P.BH;
+  const int stage_bytes = ((stage_elems * (int)sizeof(T)) + 127) & ~127;
+  T* stages = reinterpret_cast<T*>(smem_raw);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)P.stages * stage_bytes);
+  uint64_t* empty = full + P.stages;
+  int2* origin = reinterpret_cast<int2*>(empty + P.stages);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int tx, ty, tz;
+  fdk_tile(P, blockIdx.x, tx, ty, tz);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < P.stages; s++) {
+      dev::mbar_init(&full[s], 1);
+      dev::mbar_init(&empty[s], FDK_CWARPS);
+    }
+    dev::fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == FDK_CWARPS) {
+    // ------------------------------------------------------------- producer warp
+    if (lane != 0) return;
+    dev::tma_prefetch(&tmap);
+    const uint32_t bytes = (uint32_t)(stage_elems * (int)sizeof(T));
+    int issued = 0;
+    bool failed = false;
+    for (int v = 0; v < P.nviews; v++) {
+      const int s = v % P.stages;
+      if (v >= P.stages) {
+        if (!dev::mbar_wait(&empty[s], ((v / P.stages) - 1) & 1)) {
+          failed = true;
+          break;
+        }
+      }
+      int w0, h0, nw, nh;
+      fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, w0, h0, nw, nh);
+      if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
+      origin[s] = make_int2(w0, h0);
+      dev::mbar_arrive_expect_tx(&full[s], bytes);
+      dev::tma_load_3d(stages + (size_t)s * (stage_bytes / sizeof(T)), &tmap, &full[s], w0, h0,
+                       P.view0 + v);
+      issued = v + 1;
+    }
+    if (failed) {
+      dev::record_status(P.status, DEV_TIMEOUT);
+      // drain: wait (bounded) for the copies still in flight before leaving
+      for (int v = max(0, issued - P.stages); v < issued; v++)
+        dev::mbar_wait(&full[v % P.stages], (v / P.stages) & 1, 100000000ull);
+    }
+    return;
+  }
+
+  // --------------------------------------------------------------- consumer warps
+  const int xl = tx * FDK_TX + (warp & 1) * 8 + (lane & 7);
+  const int yl = ty * FDK_TY + (warp >> 1) * 4 + (lane >> 3);
+  const int zl = tz * NZ;
+  const float x = P.ox + (float)xl, y = P.oy + (float)yl, zf = P.oz + (float)zl;
+  const float MAGIC = 12582912.0f;  // 1.5 * 2^23: adding it in round-down mode floors
+  const unsigned MAGIC_BITS = 0x4B400000u;
+
+  float acc[NZ];
+#pragma unroll
+  for (int k = 0; k < NZ; k++) acc[k] = 0.0f;
+
+  for (int v = 0; v < P.nviews; v++) {
+    const int s = v % P.stages;
+    if (!dev::mbar_wait(&full[s], (v / P.stages) & 1)) {
+      dev::record_status(P.status, DEV_TIMEOUT);
+      return;
+    }
+    const FdkView& V = P.v[v];
+    const int2 org = origin[s];
+    const T* S = stages + (size_t)s * (stage_bytes / sizeof(T));
+
+    const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
+    const float U = __frcp_rn(den);
+    const float wabs = fmaf(fmaf(V.a0, x, V.a1 * y), U, V.wc);
+    float wl = wabs - (float)org.x;
+    float h0 = fmaf(U, fmaf(P.hb, zf, V.e), V.hc) - (float)org.y;
+    float dh = U * P.hb;
+    float wt = V.wt;
+    if (P.wexp >= 1) wt *= U;
+    if (P.wexp >= 2) wt *= U;
+
+    // memory safety: every tap must stay inside the staged box
+    int iw = __float2int_rd(wl);
+    const float hl = fmaf((float)(NZ - 1), dh, h0);
+    if (iw < 0 || iw > P.BW - 2 || !(h0 >= 0.0f) || !(hl < (float)(P.BH - 1))) {
+      dev::record_status(P.status, DEV_RANGE);
+      iw = 0; wl = 0.0f; h0 = 0.0f; dh = 0.0f; wt = 0.0f;
+    }
+    const float fw = wl - (float)iw;
+
+    float lo = -3.0e38f, hi = 3.0e38f;  // Tam-Danielsson bounds (local h)
+    if (P.piwin) {
+      const float u = (wabs - V.wc) * P.td_sign / P.td_r;
+      const float q = P.td_a * (1.0f + u * u);
+      const float at = atanf(u);
+      const float hsrc = V.hc - (float)org.y;
+      hi = hsrc + q * (1.5707963267948966f - at);
+      lo = hsrc - q * (1.5707963267948966f + at);
+    }
+
+    const unsigned base = (unsigned)iw - MAGIC_BITS * (unsigned)P.BW;
+#pragma unroll
+    for (int k = 0; k < NZ; k++) {
+      const float hk = fmaf((float)k, dh, h0);
+      const float t = __fadd_rd(hk, MAGIC);
+      const unsigned idx = (unsigned)__float_as_int(t) * (unsigned)P.BW + base;
+      const float fh = hk - (t - MAGIC);
+      const T* p = S + idx;
+      const float a = ld_tap<T>(p), b = ld_tap<T>(p + 1);
+      const float c = ld_tap<T>(p + P.BW), d = ld_tap<T>(p + P.BW + 1);
+      const float r0 = fmaf(fw, b - a, a);
+      const float r1 = fmaf(fw, d - c, c);
+      const float val = fmaf(fh, r1 - r0, r0);
+      float wk = wt;
+      if (P.piwin) wk = (hk >= lo && hk <= hi) ? wt : 0.0f;
+      acc[k] = fmaf(wk, val, acc[k]);
+    }
+    __syncwarp();
+    if (lane == 0) dev::mbar_arrive(&empty[s]);
+  }
+
+  if (xl < P.nx && yl < P.ny) {
+    float* out = P.vol + (size_t)yl * P.nx + xl;
+    const size_t plane = (size_t)P.nx * P.ny;
+#pragma unroll
+    for (int k = 0; k < NZ; k++) {
+      if (zl + k < P.nz) out[(size_t)(zl + k) * plane] += acc[k];
+    }
+  }
+}
+
+// =====================================================================================
+// Generic projective-matrix kernel
+// =====================================================================================
+constexpr int GEN_MAXV = 560;
+struct GenView {
+  float m[12];
+  float kappa;
+  float wt;
+};
+struct GenParams {
+  float* vol;
+  const void* proj;
+  int ptype;
+  int nx, ny, nz;
+  float ox, oy, oz;
+  int WH0, WH1;
+  int nviews, view0;
+  int wexp;
+  int piwin;
+  float td_a, td_r, td_sign, pw;
+  GenView v[GEN_MAXV];
+};
+static_assert(sizeof(GenParams) < 32000, "kernel parameter space");
+
+__device__ __forceinline__ float gen_load(const void* base, int ptype, size_t i)
+{
+  if (ptype == FCB_F32) return __ldg(reinterpret_cast<const float*>(base) + i);
+  const unsigned short u = __ldg(reinterpret_cast<const unsigned short*>(base) + i);
+  if (ptype == FCB_F16) return __half2float(__ushort_as_half(u));
+  return __uint_as_float(((uint32_t)u) << 16);
+}
+
+__global__ void __launch_bounds__(256) bp_generic_kernel(const __grid_constant__ GenParams P)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nvox = (long long)P.nx * P.ny * P.nz;
+  if (i >= nvox) return;
+  const int xi = (int)(i % P.nx);
+  const long long r = i / P.nx;
+  const int yi = (int)(r % P.ny), zi = (int)(r / P.ny);
+  const float x = P.ox + xi, y = P.oy + yi, z = P.oz + zi;
+  float acc = 0.0f;
+  for (int v = 0; v < P.nviews; v++) {
+    const GenView& V = P.v[v];
+    const float uu = fmaf(V.m[0], x, fmaf(V.m[1], y, fmaf(V.m[2], z, V.m[3])));
+    const float vv = fmaf(V.m[4], x, fmaf(V.m[5], y, fmaf(V.m[6], z, V.m[7])));
+    const float ss = fmaf(V.m[8], x, fmaf(V.m[9], y, fmaf(V.m[10], z, V.m[11])));
+    const float rs = 1.0f / ss;
+    const float wl = uu * rs, hl = vv * rs;
+    float wt = V.wt;
+    if (P.wexp >= 1) wt *= V.kappa * rs;
+    if (P.wexp >= 2) wt *= V.kappa * rs;
+    if (!(wl > -1.0f && wl < (float)P.WH0 && hl > -1.0f && hl < (float)P.WH1)) continue;
+    const float fw0 = floorf(wl), fh0 = floorf(hl);
+    const int iw = (int)fw0, ih = (int)fh0;
+    const float a = wl - fw0, b = hl - fh0;
+    const size_t vb = (size_t)(P.view0 + v) * P.WH0 * P.WH1;
+    float t00 = 0.f, t10 = 0.f, t01 = 0.f, t11 = 0.f;
+    if (ih >= 0) {
+      if (iw >= 0) t00 = gen_load(P.proj, P.ptype, vb + (size_t)ih * P.WH0 + iw);
+      if (iw + 1 < P.WH0) t10 = gen_load(P.proj, P.ptype, vb + (size_t)ih * P.WH0 + iw + 1);
+    }
+    if (ih + 1 < P.WH1) {
+      if (iw >= 0) t01 = gen_load(P.proj, P.ptype, vb + (size_t)(ih + 1) * P.WH0 + iw);
+      if (iw + 1 < P.WH0) t11 = gen_load(P.proj, P.ptype, vb + (size_t)(ih + 1) * P.WH0 + iw + 1);
+    }
+    const float r0 = fmaf(a, t10 - t00, t00), r1 = fmaf(a, t11 - t01, t01);
+    acc = fmaf(wt, fmaf(b, r1 - r0, r0), acc);
+  }
+  P.vol[i] += acc;
+}
+
+}  // namespace fcb
+
+// =====================================================================================
+// Plans
+// =====================================================================================
+using namespace fcb;
+
+struct fcb_bp_plan {
+  Problem pb;
+  int mode = 2;
+  int ptype = FCB_F32;
+  int path = 0;  // 0 generic, 1 tma
+  int device = 0;
+  int nz_tile = 32;
+  int maxv = FDK_MAXV;
+  int BW = 0, BH = 0, stages = 0, wshift = 2;
+  long long updates = 0;
+  std::vector<FdkParams> fdk;  // one per view chunk
+  std::vector<GenParams> gen;
+};
+
+namespace {
+
+template <typename T, int NZ>
+int launch_fdk(const fcb_bp_plan* pl, const CUtensorMap& map, int chunk, cudaStream_t st)
+{
+  const size_t stage_bytes = ((size_t)pl->BW * pl->BH * sizeof(T) + 127) & ~(size_t)127;
+  const size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int2));
+  auto kern = fdk_tma_kernel<T, NZ>;
+  FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (int c = 0; c < (int)pl->fdk.size(); c++) {
+    if (chunk >= 0 && c != chunk) continue;
+    const FdkParams& P = pl->fdk[c];
+    const int ntiles = P.tiles_x * P.tiles_y * P.tiles_z;
+    kern<<<ntiles, FDK_THREADS, smem, st>>>(map, P);
+    FCB_CUDA_TRY(cudaGetLastError());
+  }
+  return FCB_OK;
+}
+
+bool aligned_geometry(const Problem& pb) { return !pb.misaligned; }
+
+// Fill FdkParams for views [v0, v0+n) (sizes/box filled by the caller).
+void fill_fdk_views(const Problem& pb, int mode, int v0, int n, FdkParams* P)
+{
+  P->nviews = n;
+  P->view0 = v0;
+  for (int k = 0; k < n; k++) {
+    const int t = v0 + k;
+    const ViewGeom& g = pb.views[t];
+    FdkView& V = P->v[k];
+    V.c0 = (float)(g.ca / pb.D);
+    V.c1 = (float)(g.sa / pb.D);
+    V.a0 = (float)(-g.sa / pb.pw);
+    V.a1 = (float)(g.ca / pb.pw);
+    V.wc = (float)(pb.projDim[0] / 2 - pb.woff[t]);
+    V.hc = (float)(pb.projDim[1] / 2 - pb.hoff[t]);
+    V.e = (float)(-g.hmp / pb.pw);
+    V.wt = (float)pb.norm[t];
+  }
+  (void)mode;
+}
+
+}  // namespace
+
+namespace fcb {
+int bp_plan_create_ex(const fcb_geometry* g, int kernelMode, int projType, int maxViewsPerLaunch,
+                      fcb_bp_plan** out)
+{
+  if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
+  *out = nullptr;
+  if (projType != FCB_F32 && projType != FCB_F16 && projType != FCB_BF16)
+    return set_error(FCB_ERR_INVALID, "unknown projection storage type");
+  auto* pl = new fcb_bp_plan();
+  pl->maxv = std::max(1, std::min(FDK_MAXV, maxViewsPerLaunch));
+  int rc = make_problem(g, &pl->pb);
+  if (rc) { delete pl; return rc; }
+  Problem& pb = pl->pb;
+  pl->mode = kernelMode == 0 ? 0 : (kernelMode == 1 ? 1 : 2);
+  pl->ptype = projType;
+  cudaGetDevice(&pl->device);
+  const int nx = pb.volEnd[0] - pb.volStart[0], ny = pb.volEnd[1] - pb.volStart[1],
+            nz = pb.volEnd[2] - pb.volStart[2];
+  pl->updates = (long long)nx * ny * nz * pb.nviews;
+  // every voxel must lie in front of the source
+  const double rx = std::max(fabs((double)(pb.volStart[0] - pb.volDim[0] / 2)),
+                             fabs((double)(pb.volEnd[0] - pb.volDim[0] / 2)));
+  const double ry = std::max(fabs((double)(pb.volStart[1] - pb.volDim[1] / 2)),
+                             fabs((double)(pb.volEnd[1] - pb.volDim[1] / 2)));
+  if (sqrt(rx * rx + ry * ry) + 16.0 >= pb.D && !pb.misaligned) {
+    delete pl;
+    return set_error(FCB_ERR_INVALID, "volume reaches the source trajectory");
+  }
+  const float ox = (float)(pb.volStart[0] - pb.volDim[0] / 2);
+  const float oy = (float)(pb.volStart[1] - pb.volDim[1] / 2);
+  const float oz = (float)(pb.volStart[2] - pb.volDim[2] / 2);
+  const int wexp = pl->mode == 0 ? 0 : (pl->mode == 1 ? 1 : 2);
+  const bool piwin = pl->mode == 1 && pb.piWindow;
+  const float td_a = (float)(pb.pitch / (2.0 * M_PI * pb.pw));
+  const float td_r = (float)(pb.D / pb.pw);
+
+  if (aligned_geometry(pb)) {
+    pl->path = 1;
+    pl->wshift = projType == FCB_F32 ? 2 : 3;
+    const int NZ = pl->nz_tile;
+    const int tiles_x = (nx + FDK_TX - 1) / FDK_TX, tiles_y = (ny + FDK_TY - 1) / FDK_TY,
+              tiles_z = (nz + NZ - 1) / NZ;
+    for (int v0 = 0; v0 < pb.nviews; v0 += pl->maxv) {
+      FdkParams P;
+      memset(&P, 0, sizeof(P));
+      P.nx = nx; P.ny = ny; P.nz = nz;
+      P.tiles_x = tiles_x; P.tiles_y = tiles_y; P.tiles_z = tiles_z;
+      P.ox = ox; P.oy = oy; P.oz = oz;
+      P.hb = (float)(1.0 / pb.pw);
+      P.wshift = pl->wshift;
+      P.wexp = wexp;
+      P.piwin = piwin ? 1 : 0;
+      P.td_a = td_a; P.td_r = td_r; P.td_sign = 1.0f;
+      fill_fdk_views(pb, pl->mode, v0, std::min(pl->maxv, pb.nviews - v0), &P);
+      pl->fdk.push_back(P);
+    }
+    // footprint pre-pass -> staging box
+    int* scratch = nullptr;
+    rc = device_status_ptr(&scratch);
+    if (rc) { delete pl; return rc; }
+    int* need = scratch + 1;
+    const int ntiles = tiles_x * tiles_y * tiles_z;
+    cudaMemset(need, 0, 2 * sizeof(int));
+    for (const FdkParams& P : pl->fdk) {
+      const long long total = (long long)ntiles * P.nviews;
+      const int blocks = (int)((total + 255) / 256);
+      fdk_footprint_kernel<<<blocks, 256>>>(P, NZ, ntiles, need);
+    }
+    int h[2] = {0, 0};
+    cudaError_t e = cudaMemcpy(h, need, sizeof h, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) { delete pl; return set_error(FCB_ERR_CUDA, cudaGetErrorString(e)); }
+    const int align = 1 << pl->wshift;
+    pl->BW = ((h[0] + align - 1) / align) * align;
+    pl->BH = h[1];
+    if (pl->BW < align) pl->BW = align;
+    if (pl->BH < 2) pl->BH = 2;
+    if (pl->BW > 256 || pl->BH > 256) {
+      pl->path = 0;  // footprint too large for one TMA box: generic kernel
+      pl->fdk.clear();
+    } else {
+      const size_t es = dtype_size(projType);
+      const size_t stage_bytes = (((size_t)pl->BW * pl->BH * es) + 127) & ~(size_t)127;
+      int st = (int)((100 * 1024) / stage_bytes);
+      pl->stages = std::max(2, std::min(8, st));
+      for (FdkParams& P : pl->fdk) {
+        P.BW = pl->BW; P.BH = pl->BH; P.stages = pl->stages;
+        P.status = scratch;
+      }
+    }
+  }
+  if (pl->path == 0) {
+    const int gmax = std::min(GEN_MAXV, pl->maxv);
+    for (int v0 = 0; v0 < pb.nviews; v0 += gmax) {
+      GenParams P;
+      memset(&P, 0, sizeof(P));
+      P.nx = nx; P.ny = ny; P.nz = nz;
+      P.ox = ox; P.oy = oy; P.oz = oz;
+      P.WH0 = pb.projWHSize[0]; P.WH1 = pb.projWHSize[1];
+      P.ptype = projType;
+      P.wexp = wexp;
+      P.nviews = std::min(gmax, pb.nviews - v0);
+      P.view0 = v0;
+      for (int k = 0; k < P.nviews; k++) {
+        double M[12], kappa;
+        view_matrix(pb, v0 + k, M, &kappa);
+        for (int j = 0; j < 12; j++) P.v[k].m[j] = (float)M[j];
+        P.v[k].kappa = (float)kappa;
+        P.v[k].wt = (float)pb.norm[v0 + k];
+      }
+      pl->gen.push_back(P);
+    }
+  }
+  *out = pl;
+  return ok();
+}
+
+int bp_plan_chunks(const fcb_bp_plan* pl, std::vector<std::pair<int, int>>* ranges)
+{
+  ranges->clear();
+  if (pl->path == 1) {
+    for (const FdkParams& P : pl->fdk) ranges->push_back({P.view0, P.view0 + P.nviews});
+  } else {
+    for (const GenParams& P : pl->gen) ranges->push_back({P.view0, P.view0 + P.nviews});
+  }
+  return FCB_OK;
+}
+
+// Launch chunk `chunk` of the plan (-1: all chunks).
+int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* volume,
+                          cudaStream_t st)
+{
+  if (!pl || !proj || !volume) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
+  const Problem& pb = pl->pb;
+  const size_t es = dtype_size(pl->ptype);
+  bool tma_ok = pl->path == 1 && ((uintptr_t)proj % 16 == 0) &&
+                ((size_t)pb.projWHSize[0] * es) % 16 == 0;
+  if (pl->path == 1 && tma_ok) {
+    CUtensorMap map;
+    const CUtensorMapDataType dt = pl->ptype == FCB_F32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                                   : pl->ptype == FCB_F16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                          : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    FCB_TRY(encode_tmap_3d(&map, dt, const_cast<void*>(proj), pb.projWHSize[0], pb.projWHSize[1],
+                           pb.nviews, (uint64_t)pb.projWHSize[0] * es,
+                           (uint64_t)pb.projWHSize[0] * pb.projWHSize[1] * es, pl->BW, pl->BH, 1));
+    for (FdkParams& P : pl->fdk) P.vol = volume;
+    if (pl->ptype == FCB_F32) FCB_TRY((launch_fdk<float, 32>(pl, map, chunk, st)));
+    else if (pl->ptype == FCB_F16) FCB_TRY((launch_fdk<__half, 32>(pl, map, chunk, st)));
+    else FCB_TRY((launch_fdk<__nv_bfloat16, 32>(pl, map, chunk, st)));
+    return ok();
+  }
+  if (pl->gen.empty()) {
+    // TMA path planned but this buffer cannot be described by a descriptor: build the
+    // generic parameters on the fly, with the same view chunks.
+    for (int v0 = 0; v0 < pb.nviews; v0 += pl->maxv) {
+      GenParams P;
+      memset(&P, 0, sizeof(P));
+      const FdkParams& F = pl->fdk[0];
+      P.nx = F.nx; P.ny = F.ny; P.nz = F.nz;
+      P.ox = F.ox; P.oy = F.oy; P.oz = F.oz;
+      P.WH0 = pb.projWHSize[0]; P.WH1 = pb.projWHSize[1];
+      P.ptype = pl->ptype;
+      P.wexp = F.wexp;
+      P.nviews = std::min(pl->maxv, pb.nviews - v0);
+      P.view0 = v0;
+      for (int k = 0; k < P.nviews; k++) {
+        double M[12], kappa;
+        view_matrix(pb, v0 + k, M, &kappa);
+        for (int j = 0; j < 12; j++) P.v[k].m[j] = (float)M[j];
+        P.v[k].kappa = (float)kappa;
+        P.v[k].wt = (float)pb.norm[v0 + k];
+      }
+      pl->gen.push_back(P);
+    }
+  }
+  for (int c = 0; c < (int)pl->gen.size(); c++) {
+    if (chunk >= 0 && c != chunk) continue;
+    GenParams& P = pl->gen[c];
+    P.vol = volume;
+    P.proj = proj;
+    const long long nvox = (long long)P.nx * P.ny * P.nz;
+    bp_generic_kernel<<<(unsigned)((nvox + 255) / 256), 256, 0, st>>>(P);
+    FCB_CUDA_TRY(cudaGetLastError());
+  }
+  return ok();
+}
+
+}  // namespace fcb
+
+extern "C" int fcb_bp_plan_create(const fcb_geometry* g, int kernelMode, int projType,
+                                  fcb_bp_plan** out)
+{
+  return bp_plan_create_ex(g, kernelMode, projType, FDK_MAXV, out);
+}
+
+extern "C" int fcb_bp_plan_execute(fcb_bp_plan* pl, const void* proj, float* volume, void* stream)
+{
+  return bp_plan_execute_chunk(pl, -1, proj, volume, reinterpret_cast<cudaStream_t>(stream));
+}
+
+extern "C" int fcb_bp_plan_info(const fcb_bp_plan* pl, int* boxW, int* boxH, int* launches,
+                                long long* updates)
+{
+  if (!pl) return set_error(FCB_ERR_INVALID, "NULL plan");
+  if (boxW) *boxW = pl->path == 1 ? pl->BW : 0;
+  if (boxH) *boxH = pl->path == 1 ? pl->BH : 0;
+  if (launches) *launches = pl->path == 1 ? (int)pl->fdk.size() : (int)pl->gen.size();
+  if (updates) *updates = pl->updates;
+  return ok();
+}
+
+extern "C" int fcb_bp_plan_destroy(fcb_bp_plan* pl)
+{
+  delete pl;
+  return ok();
+}
+
+extern "C" int fcb_backproject_device(const fcb_geometry* g, int kernelMode, const void* proj,
+                                      int projType, float* volume, void* stream)
+{
+  fcb_bp_plan* pl = nullptr;
+  FCB_TRY(fcb_bp_plan_create(g, kernelMode, projType, &pl));
+  int rc = fcb_bp_plan_execute(pl, proj, volume, stream);
+  fcb_bp_plan_destroy(pl);
+  return rc;
+}

@@ -1,0 +1,346 @@
+// fcb_project.cu -- ray-driven cone-beam forward projector and its exact adjoint (sm_100a).
+//
+// Replaces GPU_new_project_volume (coneBeamGPU.cu:96-176), its launcher (:493-563) and the
+// problem solver coneBeamProject (unit_coneBeamGPU.cu:88-171).  Sample lattice as in the
+// reference: points S + m d at every integer distance m (voxels) from the source along the
+// unit ray direction d (the reference marches from the integer sweep start in unit steps,
+// coneBeamGPU.cu:160-172, :1781-1782).  Instead of sweeping a bounding sphere the kernels
+// clip each ray to the support of the trilinear interpolant (the volume box widened by one
+// voxel, which is where the reference's zero ring lets samples contribute), so every
+// sample they take is one the reference takes and empty space is skipped.
+//
+//  * FCB_PROJ_TEXTURE: trilinear sampling by the texture unit from a 3-D CUDA array with
+//    border (zero) addressing -- the reference's interpolation, 8-bit weights included;
+//  * FCB_PROJ_EXPLICIT: FP32 trilinear from global memory (read-only path), exact weights;
+//    project_adjoint_kernel scatters with the very same weights, so the pair satisfies
+//    <A x, y> = <x, A^T y> to rounding.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "fcb_internal.h"
+
+namespace fcb {
+
+constexpr int PJ_MAXV = 560;
+struct PjView {
+  float s[3];    // source, local continuous voxel-index coordinates
+  float p0[3];   // centre of local pixel (0,0), same coordinates
+  float w[3];    // one pixel step along w
+  float h[3];    // one pixel step along h
+  float wt;      // normalisation factor
+};
+struct PjParams {
+  const float* vol;
+  float* proj;
+  unsigned long long* samples;  // optional work counter
+  cudaTextureObject_t tex;
+  int nx, ny, nz;               // local volume extents
+  int WH0, WH1;                 // window size
+  int nviews, view0;
+  PjView v[PJ_MAXV];
+};
+static_assert(sizeof(PjParams) < 32000, "kernel parameter space");
+
+// Integer sample range [m0, m1] of S + m d inside the open box (-1, n) per axis.
+__device__ __forceinline__ bool ray_clip(const float s[3], const float d[3], int nx, int ny,
+                                         int nz, int& m0, int& m1)
+{
+  float lo = -3.0e38f, hi = 3.0e38f;
+  const float n[3] = {(float)nx, (float)ny, (float)nz};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (fabsf(d[a]) < 1e-12f) {
+      if (!(s[a] > -1.0f && s[a] < n[a])) return false;
+      continue;
+    }
+    const float inv = 1.0f / d[a];
+    float t0 = (-1.0f - s[a]) * inv, t1 = (n[a] - s[a]) * inv;
+    if (t0 > t1) { const float tt = t0; t0 = t1; t1 = tt; }
+    lo = fmaxf(lo, t0);
+    hi = fminf(hi, t1);
+  }
+  if (!(hi > lo)) return false;
+  m0 = (int)ceilf(lo);
+  m1 = (int)floorf(hi);
+  return m1 >= m0;
+}
+
+__device__ __forceinline__ void ray_of(const PjView& V, int wl, int hl, float s[3], float d[3])
+{
+  float p[3], len2 = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    p[a] = fmaf((float)hl, V.h[a], fmaf((float)wl, V.w[a], V.p0[a]));
+    d[a] = p[a] - V.s[a];
+    s[a] = V.s[a];
+    len2 = fmaf(d[a], d[a], len2);
+  }
+  const float r = rsqrtf(len2);
+#pragma unroll
+  for (int a = 0; a < 3; a++) d[a] *= r;
+}
+
+__device__ __forceinline__ void count_samples(unsigned long long* ctr, long long n)
+{
+  if (!ctr) return;
+  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+  if ((threadIdx.x & 31) == 0 && n) atomicAdd(ctr, (unsigned long long)n);
+}
+
+__global__ void __launch_bounds__(256) project_tex_kernel(const __grid_constant__ PjParams P)
+{
+  const int wl = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int hl = blockIdx.y * 16 + (threadIdx.x >> 4);
+  const int v = blockIdx.z;
+  long long cnt = 0;
+  if (wl < P.WH0 && hl < P.WH1) {
+    const PjView& V = P.v[v];
+    float s[3], d[3];
+    ray_of(V, wl, hl, s, d);
+    int m0, m1;
+    float acc = 0.0f;
+    if (ray_clip(s, d, P.nx, P.ny, P.nz, m0, m1)) {
+      cnt = m1 - m0 + 1;
+      // texel centres sit at index + 0.5
+      const float bx = s[0] + 0.5f, by = s[1] + 0.5f, bz = s[2] + 0.5f;
+      for (int m = m0; m <= m1; m++) {
+        const float mf = (float)m;
+        acc += tex3D<float>(P.tex, fmaf(mf, d[0], bx), fmaf(mf, d[1], by), fmaf(mf, d[2], bz));
+      }
+    }
+    P.proj[((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl] += V.wt * acc;
+  }
+  count_samples(P.samples, cnt);
+}
+
+struct Tri {
+  int i, j, k;
+  float a, b, c;
+};
+__device__ __forceinline__ Tri tri_of(float x, float y, float z)
+{
+  Tri t;
+  const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+  t.i = (int)fx; t.j = (int)fy; t.k = (int)fz;
+  t.a = x - fx; t.b = y - fy; t.c = z - fz;
+  return t;
+}
+
+__device__ __forceinline__ float tri_fetch(const float* __restrict__ vol, int nx, int ny, int nz,
+                                           const Tri& t)
+{
+  const size_t sx = 1, sy = nx, sz = (size_t)nx * ny;
+  if (t.i >= 0 && t.j >= 0 && t.k >= 0 && t.i + 1 < nx && t.j + 1 < ny && t.k + 1 < nz) {
+    const float* p = vol + t.i * sx + t.j * sy + t.k * sz;
+    const float v000 = __ldg(p), v100 = __ldg(p + sx), v010 = __ldg(p + sy), v110 = __ldg(p + sx + sy);
+    const float v001 = __ldg(p + sz), v101 = __ldg(p + sx + sz), v011 = __ldg(p + sy + sz),
+                v111 = __ldg(p + sx + sy + sz);
+    const float x00 = fmaf(t.a, v100 - v000, v000), x10 = fmaf(t.a, v110 - v010, v010);
+    const float x01 = fmaf(t.a, v101 - v001, v001), x11 = fmaf(t.a, v111 - v011, v011);
+    const float y0 = fmaf(t.b, x10 - x00, x00), y1 = fmaf(t.b, x11 - x01, x01);
+    return fmaf(t.c, y1 - y0, y0);
+  }
+  float r = 0.0f;
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int X = t.i + (q & 1), Y = t.j + ((q >> 1) & 1), Z = t.k + ((q >> 2) & 1);
+    if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
+    const float w = ((q & 1) ? t.a : 1.0f - t.a) * (((q >> 1) & 1) ? t.b : 1.0f - t.b) *
+                    (((q >> 2) & 1) ? t.c : 1.0f - t.c);
+    r = fmaf(w, __ldg(vol + X * sx + Y * sy + Z * sz), r);
+  }
+  return r;
+}
+
+__global__ void __launch_bounds__(256) project_explicit_kernel(const __grid_constant__ PjParams P)
+{
+  const int wl = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int hl = blockIdx.y * 16 + (threadIdx.x >> 4);
+  const int v = blockIdx.z;
+  long long cnt = 0;
+  if (wl < P.WH0 && hl < P.WH1) {
+    const PjView& V = P.v[v];
+    float s[3], d[3];
+    ray_of(V, wl, hl, s, d);
+    int m0, m1;
+    float acc = 0.0f;
+    if (ray_clip(s, d, P.nx, P.ny, P.nz, m0, m1)) {
+      cnt = m1 - m0 + 1;
+      for (int m = m0; m <= m1; m++) {
+        const float mf = (float)m;
+        const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
+        acc += tri_fetch(P.vol, P.nx, P.ny, P.nz, t);
+      }
+    }
+    P.proj[((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl] += V.wt * acc;
+  }
+  count_samples(P.samples, cnt);
+}
+
+// Exact transpose of project_explicit_kernel: vol += A^T (norm * proj).
+__global__ void __launch_bounds__(256) project_adjoint_kernel(const __grid_constant__ PjParams P,
+                                                              float* vol)
+{
+  const int wl = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int hl = blockIdx.y * 16 + (threadIdx.x >> 4);
+  const int v = blockIdx.z;
+  if (wl >= P.WH0 || hl >= P.WH1) return;
+  const PjView& V = P.v[v];
+  const float y = V.wt * __ldg(P.proj + ((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl);
+  if (y == 0.0f) return;
+  float s[3], d[3];
+  ray_of(V, wl, hl, s, d);
+  int m0, m1;
+  if (!ray_clip(s, d, P.nx, P.ny, P.nz, m0, m1)) return;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  for (int m = m0; m <= m1; m++) {
+    const float mf = (float)m;
+    const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int X = t.i + (q & 1), Y = t.j + ((q >> 1) & 1), Z = t.k + ((q >> 2) & 1);
+      if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
+      const float w = ((q & 1) ? t.a : 1.0f - t.a) * (((q >> 1) & 1) ? t.b : 1.0f - t.b) *
+                      (((q >> 2) & 1) ? t.c : 1.0f - t.c);
+      atomicAdd(vol + X + Y * sy + Z * sz, w * y);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------ host
+static void fill_pj_views(const Problem& pb, int v0, int n, PjParams* P)
+{
+  P->nviews = n;
+  P->view0 = v0;
+  // local continuous voxel index = coordinate + volDim/2 - volStart
+  const double off[3] = {(double)(pb.volDim[0] / 2 - pb.volStart[0]),
+                         (double)(pb.volDim[1] / 2 - pb.volStart[1]),
+                         (double)(pb.volDim[2] / 2 - pb.volStart[2])};
+  for (int k = 0; k < n; k++) {
+    const int t = v0 + k;
+    const ViewGeom& g = pb.views[t];
+    PjView& V = P->v[k];
+    const double cw = (double)(pb.woff[t] - pb.projDim[0] / 2);
+    const double ch = (double)(pb.hoff[t] - pb.projDim[1] / 2);
+    for (int a = 0; a < 3; a++) {
+      V.s[a] = (float)(g.s[a] + off[a]);
+      V.p0[a] = (float)(g.d[a] + cw * g.w[a] + ch * g.h[a] + off[a]);
+      V.w[a] = (float)g.w[a];
+      V.h[a] = (float)g.h[a];
+    }
+    V.wt = (float)pb.norm[t];
+  }
+}
+
+int project_launch(const Problem& pb, int method, const float* vol, float* proj, float* adj_vol,
+                   unsigned long long* samples, cudaStream_t st)
+{
+  const int nx = pb.volEnd[0] - pb.volStart[0], ny = pb.volEnd[1] - pb.volStart[1],
+            nz = pb.volEnd[2] - pb.volStart[2];
+  cudaArray_t arr = nullptr;
+  cudaTextureObject_t tex = 0;
+  if (method == FCB_PROJ_TEXTURE && !adj_vol) {
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    FCB_CUDA_TRY(cudaMalloc3DArray(&arr, &cd, make_cudaExtent(nx, ny, nz)));
+    cudaMemcpy3DParms cp;
+    memset(&cp, 0, sizeof(cp));
+    cp.srcPtr = make_cudaPitchedPtr(const_cast<float*>(vol), nx * sizeof(float), nx, ny);
+    cp.dstArray = arr;
+    cp.extent = make_cudaExtent(nx, ny, nz);
+    cp.kind = cudaMemcpyDeviceToDevice;
+    cudaError_t e = cudaMemcpy3DAsync(&cp, st);
+    if (e != cudaSuccess) {
+      cudaFreeArray(arr);
+      return set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 0;
+    e = cudaCreateTextureObject(&tex, &rd, &td, nullptr);
+    if (e != cudaSuccess) {
+      cudaFreeArray(arr);
+      return set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
+    }
+  }
+  std::vector<PjParams> chunks;
+  for (int v0 = 0; v0 < pb.nviews; v0 += PJ_MAXV) {
+    PjParams P;
+    memset(&P, 0, sizeof(P));
+    P.vol = vol;
+    P.proj = proj;
+    P.samples = samples;
+    P.tex = tex;
+    P.nx = nx; P.ny = ny; P.nz = nz;
+    P.WH0 = pb.projWHSize[0]; P.WH1 = pb.projWHSize[1];
+    fill_pj_views(pb, v0, std::min(PJ_MAXV, pb.nviews - v0), &P);
+    chunks.push_back(P);
+  }
+  int rc = FCB_OK;
+  for (const PjParams& P : chunks) {
+    dim3 grid((P.WH0 + 15) / 16, (P.WH1 + 15) / 16, P.nviews);
+    if (adj_vol) project_adjoint_kernel<<<grid, 256, 0, st>>>(P, adj_vol);
+    else if (method == FCB_PROJ_TEXTURE) project_tex_kernel<<<grid, 256, 0, st>>>(P);
+    else project_explicit_kernel<<<grid, 256, 0, st>>>(P);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) { rc = set_error(FCB_ERR_CUDA, cudaGetErrorString(e)); break; }
+  }
+  if (arr) {
+    // the array must outlive the kernels that sample it
+    cudaStreamSynchronize(st);
+    cudaDestroyTextureObject(tex);
+    cudaFreeArray(arr);
+  }
+  return rc;
+}
+
+}  // namespace fcb
+
+using namespace fcb;
+
+extern "C" int fcb_project_device(const fcb_geometry* g, int method, const float* volume,
+                                  float* proj, void* stream)
+{
+  if (!volume || !proj) return set_error(FCB_ERR_INVALID, "NULL buffer");
+  if (method != FCB_PROJ_TEXTURE && method != FCB_PROJ_EXPLICIT)
+    return set_error(FCB_ERR_INVALID, "unknown projector method");
+  Problem pb;
+  FCB_TRY(make_problem(g, &pb));
+  FCB_TRY(project_launch(pb, method, volume, proj, nullptr, nullptr,
+                         reinterpret_cast<cudaStream_t>(stream)));
+  return ok();
+}
+
+extern "C" int fcb_project_adjoint_device(const fcb_geometry* g, const float* proj, float* volume,
+                                          void* stream)
+{
+  if (!volume || !proj) return set_error(FCB_ERR_INVALID, "NULL buffer");
+  Problem pb;
+  FCB_TRY(make_problem(g, &pb));
+  FCB_TRY(project_launch(pb, FCB_PROJ_EXPLICIT, nullptr, const_cast<float*>(proj), volume, nullptr,
+                         reinterpret_cast<cudaStream_t>(stream)));
+  return ok();
+}
+
+// Projector with a device-side sample counter (Gsamples accounting for benchmarks).
+extern "C" int fcb_project_device_counted(const fcb_geometry* g, int method, const float* volume,
+                                          float* proj, unsigned long long* samples_dev,
+                                          void* stream)
+{
+  if (!volume || !proj) return set_error(FCB_ERR_INVALID, "NULL buffer");
+  Problem pb;
+  FCB_TRY(make_problem(g, &pb));
+  FCB_TRY(project_launch(pb, method, volume, proj, nullptr, samples_dev,
+                         reinterpret_cast<cudaStream_t>(stream)));
+  return ok();
+}

@@ -1,0 +1,150 @@
+"""Device-side operators on torch CUDA tensors, stream-ordered on torch's current stream.
+
+torch is only the plumbing here (device memory, streams); every operator is a kernel of
+libfastcone_b200.so reached through its C ABI.  There is no CPU fallback: tensors must live
+on a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import check, lib
+from .geometry import ConeGeometry
+
+_DTYPES = {torch.float32: _lib.FCB_F32, torch.float16: _lib.FCB_F16, torch.bfloat16: _lib.FCB_BF16}
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev(t: torch.Tensor, name: str, dtype=None):
+    if not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor (there is no CPU path)")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if dtype is not None and t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def backproject(proj: torch.Tensor, geom: ConeGeometry, mode: int = _lib.MODE_FDK,
+                vol: torch.Tensor | None = None) -> torch.Tensor:
+    """vol += sum_t norm[t] * w_mode(U) * bilinear(proj[t]); proj (n, h, w) float32/16/bf16."""
+    if proj.dtype not in _DTYPES:
+        raise ValueError("projection dtype must be float32, float16 or bfloat16")
+    if tuple(proj.shape) != geom.proj_shape:
+        raise ValueError(f"projection shape {tuple(proj.shape)} != {geom.proj_shape}")
+    if vol is None:
+        vol = torch.zeros(geom.vol_shape, device=proj.device, dtype=torch.float32)
+    g = geom.struct()
+    check(lib().fcb_backproject_device(ctypes.byref(g), mode, _dev(proj, "proj"), _DTYPES[proj.dtype],
+                                       _dev(vol, "vol", torch.float32), _stream()))
+    return vol
+
+
+class BackprojectPlan:
+    """Geometry digested once; ``__call__`` queues the kernels and allocates nothing."""
+
+    def __init__(self, geom: ConeGeometry, mode: int = _lib.MODE_FDK, dtype=torch.float32):
+        self.geom = geom
+        self.mode = mode
+        self.dtype = dtype
+        self._h = ctypes.c_void_p()
+        g = geom.struct()
+        check(lib().fcb_bp_plan_create(ctypes.byref(g), mode, _DTYPES[dtype], ctypes.byref(self._h)))
+
+    def info(self):
+        bw, bh, nl = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        upd = ctypes.c_longlong()
+        check(lib().fcb_bp_plan_info(self._h, ctypes.byref(bw), ctypes.byref(bh), ctypes.byref(nl),
+                                     ctypes.byref(upd)))
+        return {"box_w": bw.value, "box_h": bh.value, "launches": nl.value, "updates": upd.value}
+
+    def __call__(self, proj: torch.Tensor, vol: torch.Tensor) -> torch.Tensor:
+        if proj.dtype != self.dtype or tuple(proj.shape) != self.geom.proj_shape:
+            raise ValueError("projection dtype/shape does not match the plan")
+        if tuple(vol.shape) != self.geom.vol_shape:
+            raise ValueError("volume shape does not match the plan")
+        check(lib().fcb_bp_plan_execute(self._h, _dev(proj, "proj"), _dev(vol, "vol", torch.float32),
+                                        _stream()))
+        return vol
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            try:
+                lib().fcb_bp_plan_destroy(self._h)
+            except Exception:
+                pass
+            self._h = ctypes.c_void_p()
+
+
+def project(vol: torch.Tensor, geom: ConeGeometry, method: int = _lib.PROJ_EXPLICIT,
+            proj: torch.Tensor | None = None, sample_counter: torch.Tensor | None = None) -> torch.Tensor:
+    """proj += norm[t] * sum_m trilinear(vol, S + m d) over integer-distance samples."""
+    if tuple(vol.shape) != geom.vol_shape:
+        raise ValueError(f"volume shape {tuple(vol.shape)} != {geom.vol_shape}")
+    if proj is None:
+        proj = torch.zeros(geom.proj_shape, device=vol.device, dtype=torch.float32)
+    g = geom.struct()
+    if sample_counter is not None:
+        check(lib().fcb_project_device_counted(ctypes.byref(g), method, _dev(vol, "vol", torch.float32),
+                                               _dev(proj, "proj", torch.float32),
+                                               _dev(sample_counter, "counter", torch.int64), _stream()))
+    else:
+        check(lib().fcb_project_device(ctypes.byref(g), method, _dev(vol, "vol", torch.float32),
+                                       _dev(proj, "proj", torch.float32), _stream()))
+    return proj
+
+
+def project_adjoint(proj: torch.Tensor, geom: ConeGeometry, vol: torch.Tensor | None = None) -> torch.Tensor:
+    """vol += A^T (norm * proj), the exact transpose of project(method=PROJ_EXPLICIT)."""
+    if tuple(proj.shape) != geom.proj_shape:
+        raise ValueError(f"projection shape {tuple(proj.shape)} != {geom.proj_shape}")
+    if vol is None:
+        vol = torch.zeros(geom.vol_shape, device=proj.device, dtype=torch.float32)
+    g = geom.struct()
+    check(lib().fcb_project_adjoint_device(ctypes.byref(g), _dev(proj, "proj", torch.float32),
+                                           _dev(vol, "vol", torch.float32), _stream()))
+    return vol
+
+
+def fdk_filter(proj: torch.Tensor, geom: ConeGeometry | None = None, out_dtype=torch.float32,
+               window: int = _lib.FILTER_RAMLAK, cosine_weight: bool = True,
+               zorigin=None, D: float | None = None, out: torch.Tensor | None = None) -> torch.Tensor:
+    """Cosine weight (fastcone.fbp's) + ramp filter (fastcone.rampfilter's) on the GPU."""
+    n, H, W = proj.shape
+    if out is None:
+        out = torch.empty((n, H, W), device=proj.device, dtype=out_dtype)
+    if cosine_weight:
+        if zorigin is None:
+            zorigin = geom.hmid
+        if D is None:
+            D = geom.D
+    z = np.ascontiguousarray(np.asarray(zorigin if zorigin is not None else np.zeros(n), np.float32))
+    check(lib().fcb_fdk_filter_device(_dev(proj, "proj", torch.float32), _dev(out, "out"),
+                                      _DTYPES[out.dtype], n, H, W, float(D or 0.0),
+                                      z.ctypes.data_as(_lib.c_float_p), 1 if cosine_weight else 0,
+                                      window, _stream()))
+    return out
+
+
+def phantom(vol_xyz, params: np.ndarray, device="cuda", out: torch.Tensor | None = None) -> torch.Tensor:
+    """Voxelise an ellipsoid phantom (n x 16 parameter rows) on the GPU."""
+    nx, ny, nz = (int(v) for v in vol_xyz)
+    if out is None:
+        out = torch.empty((nz, ny, nx), device=device, dtype=torch.float32)
+    dims = np.array([nx, ny, nz], np.int32)
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    check(lib().fcb_phantom_device(_dev(out, "out", torch.float32), dims.ctypes.data_as(_lib.c_int_p),
+                                   p.ctypes.data_as(_lib.c_double_p), len(p), _stream()))
+    return out
+
+
+def sync_status():
+    """Synchronise the current stream; raise if a kernel recorded a device-side failure."""
+    check(lib().fcb_sync_status(_stream()))

@@ -1,0 +1,174 @@
+/*
+ * fastcone_b200.h -- C ABI of libfastcone_b200.so, a B200 (sm_100a) cone-beam CT
+ * projector / backprojector that is a drop-in for Fastcone's libFastcone.so.
+ *
+ * Conventions (identical to the reference ABI, wrapper.c:112-249):
+ *   - dimension arrays are [x, y, z] for volumes and [w, h, t] for projections;
+ *   - `volume` is the volStart..volEnd sub-array of a volDim grid, x fastest;
+ *   - `projections` holds projDim[2] views of projWHSize[0] x projWHSize[1] windows,
+ *     view t's window placed at (projWOffset[t], projHOffset[t]) of a
+ *     projDim[0] x projDim[1] detector; values outside a window are zero;
+ *   - voxel g sits at g - volDim/2 (integer division), detector pixel g at
+ *     (g - projDim/2) * pixelWidth; the source of view t is at distance
+ *     sourceSampleDistance from the rotation axis at angle angles[t], height
+ *     hMidPlane[t] (measured from volume element 0);
+ *   - both directions ACCUMULATE: backprojection adds into `volume`, projection adds
+ *     norm[t] * (A vol) into `projections`; backprojection multiplies view t by norm[t].
+ *
+ * Errors: the reference's void entry points record a status retrievable with
+ * fcb_last_status()/fcb_last_error() (thread-local); every other entry point returns it.
+ * No entry point exits the process or resets the device context.
+ */
+#ifndef FASTCONE_B200_H
+#define FASTCONE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define FCB_OK 0
+#define FCB_ERR_INVALID 1   /* bad argument (sizes, pointers, mode) */
+#define FCB_ERR_CUDA 2      /* a CUDA runtime/driver call failed */
+#define FCB_ERR_NOMEM 3     /* device or pinned host allocation failed */
+#define FCB_ERR_TIMEOUT 4   /* a bounded device-side wait gave up (kernel status word) */
+#define FCB_ERR_NODEVICE 5  /* GPUID does not name a CUDA device */
+#define FCB_ERR_RANGE 6     /* geometry outside what a kernel's staging window supports */
+
+/* projection storage types for the device entry points */
+#define FCB_F32 0
+#define FCB_F16 1
+#define FCB_BF16 2
+
+/* backprojection kernel modes (wrapper.c:134-143: 0 unweighted, 1 Katsevich, else FDK) */
+#define FCB_MODE_UNWEIGHTED 0
+#define FCB_MODE_KATSEVICH 1
+#define FCB_MODE_FDK 2
+
+/* forward projector variants */
+#define FCB_PROJ_TEXTURE 0   /* hardware texture trilinear (8-bit weights, like the reference) */
+#define FCB_PROJ_EXPLICIT 1  /* explicit FP32 trilinear; exact transpose is fcb_project_adjoint_device */
+
+/* ramp-filter windows for fcb_fdk_filter_device */
+#define FCB_FILTER_RAMLAK 0
+#define FCB_FILTER_SHEPPLOGAN 1
+
+int fcb_version(void);
+int fcb_last_status(void);
+const char* fcb_last_error(void);
+
+/* ====================================================================================
+ * Reference-compatible entry points: same symbols, argument order and semantics as the
+ * definitions in wrapper.c (the order fastcone.py calls them in).  Host buffers.
+ * ==================================================================================== */
+
+/* wrapper.c:112-146 (declared wrapper.h:48-62) */
+void GPU_CB_K_backproject(int GPUID, float* volume, float* projections, float* angles,
+                          float* hMidPlane, float sourceSampleDistance, float pixelWidth,
+                          int volDim[3], int volStart[3], int volEnd[3], int projDim[3],
+                          int projWHSize[2], int* projWOffset, int* projHOffset,
+                          float* normalizationFactor, int kernelMode);
+
+/* wrapper.c:177-194 (declared wrapper.h:34-45): FDK */
+void GPU_CB_backproject(int GPUID, float* volume, float* projections, float* angles,
+                        float* hMidPlane, float sourceSampleDistance, float pixelWidth,
+                        int volDim[3], int volStart[3], int volEnd[3], int projDim[3],
+                        int projWHSize[2], int* projWOffset, int* projHOffset,
+                        float* normalizationFactor);
+
+/* wrapper.c:149-174 (declared wrapper.h:64-80): unweighted, misaligned detector */
+void GPU_CB_misalign_backproject(int GPUID, float* volume, float* projections, float* angles,
+                                 float* hMidPlane, float sourceSampleDistance, float pixelWidth,
+                                 int volDim[3], int volStart[3], int volEnd[3], int projDim[3],
+                                 int projWHSize[2], int* projWOffset, int* projHOffset,
+                                 float* normalizationFactor, float* misAlignments);
+
+/* wrapper.c:203-227 (declared wrapper.h:82-95) */
+void GPU_CB_misalign_project(int GPUID, float* volume, float* projections, float* angles,
+                             float* hMidPlane, float sourceSampleDistance, float pixelWidth,
+                             int volDim[3], int volStart[3], int volEnd[3], int projDim[3],
+                             int projWHSize[2], int* projWOffset, int* projHOffset,
+                             float* normalizationFactor, float* misAlignments);
+
+/* wrapper.c:229-249 (declared wrapper.h:97-109) */
+void GPU_CB_project(int GPUID, float* volume, float* projections, float* angles,
+                    float* hMidPlane, float sourceSampleDistance, float pixelWidth,
+                    int volDim[3], int volStart[3], int volEnd[3], int projDim[3],
+                    int projWHSize[2], int* projWOffset, int* projHOffset,
+                    float* normalizationFactor);
+
+/* ====================================================================================
+ * Status-returning entry points.
+ * ==================================================================================== */
+
+/* Problem description shared by the device entry points.  All pointers are HOST
+ * pointers to small per-view arrays (nviews = projDim[2]); misAlignments may be NULL. */
+typedef struct fcb_geometry {
+  int volDim[3];
+  int volStart[3];
+  int volEnd[3];
+  int projDim[3];
+  int projWHSize[2];
+  const int* projWOffset;
+  const int* projHOffset;
+  const float* angles;
+  const float* hMidPlane;
+  float sourceSampleDistance;
+  float pixelWidth;
+  const float* normalizationFactor;
+  const float* misAlignments;
+  float helicalPitch; /* source z advance per 2*pi rad (voxels); Katsevich PI window only */
+  int piWindow;       /* Katsevich: 1 = apply the Tam-Danielsson window, 0 = dense */
+} fcb_geometry;
+
+/* Host-buffer versions of GPU_CB_K_backproject / GPU_CB_misalign_project that return
+ * the status.  Replaces unit_coneBeamGPU.cu:173-305 and :88-171. */
+int fcb_backproject_host(int device, const fcb_geometry* g, int kernelMode,
+                         const float* projections, float* volume);
+int fcb_project_host(int device, const fcb_geometry* g, int method, const float* volume,
+                     float* projections);
+
+/* Device-pointer versions, stream-ordered on `stream` (a cudaStream_t, NULL = legacy
+ * default).  `proj` holds FCB_F32/F16/BF16 values with the layout above; `volume` is
+ * float.  They return once the work is queued; a device-side failure is reported by
+ * the next call on the same thread that synchronises (fcb_sync_status). */
+int fcb_backproject_device(const fcb_geometry* g, int kernelMode, const void* proj, int projType,
+                           float* volume, void* stream);
+int fcb_project_device(const fcb_geometry* g, int method, const float* volume, float* proj,
+                       void* stream);
+int fcb_project_adjoint_device(const fcb_geometry* g, const float* proj, float* volume,
+                               void* stream);
+
+/* Reusable backprojection plan (geometry digested once: per-view parameters, staging
+ * window sizes).  execute() is asynchronous and allocates nothing. */
+typedef struct fcb_bp_plan fcb_bp_plan;
+int fcb_bp_plan_create(const fcb_geometry* g, int kernelMode, int projType, fcb_bp_plan** plan);
+int fcb_bp_plan_execute(fcb_bp_plan* plan, const void* proj, float* volume, void* stream);
+int fcb_bp_plan_info(const fcb_bp_plan* plan, int* boxW, int* boxH, int* launches,
+                     long long* voxelViewUpdates);
+int fcb_bp_plan_destroy(fcb_bp_plan* plan);
+
+/* Waits for `stream` and returns FCB_ERR_TIMEOUT / FCB_ERR_RANGE if a kernel of this
+ * library recorded a device-side failure since the previous check, else FCB_OK. */
+int fcb_sync_status(void* stream);
+
+/* FDK pre-processing on the GPU (fastcone.py:260-292): optional cosine weight
+ * D / sqrt(D^2 + (h - zOrigin[t])^2 + (w - W/2)^2) in detector pixels, then the ramp
+ * filter of fastcone.rampfilter (zero-pad rows to 2W, pi*|f| with DC = 1/8 of the first
+ * bin; FCB_FILTER_SHEPPLOGAN multiplies by sinc(f)), output stored as outType.
+ * in: float [nviews][H][W] device; out: [nviews][H][W] of outType (may alias in when
+ * outType == FCB_F32). */
+int fcb_fdk_filter_device(const float* in, void* out, int outType, int nviews, int H, int W,
+                          float D, const float* zOrigin, int cosineWeight, int window,
+                          void* stream);
+
+/* Ellipsoid phantom voxelisation: vol[z][y][x] = sum of densities of ellipsoids
+ * containing the voxel centre (g - volDim/2).  params: n x 16 doubles (host):
+ * centre(3), semi-axes(3), row-major rotation R (9, body = R^T (p - c)), density. */
+int fcb_phantom_device(float* vol, const int volDim[3], const double* params, int n,
+                       void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
