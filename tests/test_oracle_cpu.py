@@ -135,3 +135,50 @@ def test_fbp_weight_restatement_matches_reference_golden():
     w = O.fbp_cosine_weight(d["input"].astype(np.float64), float(d["D"]), d["zOrigin"])
     assert O.rel_l2(w, d["weighted"]) < 1e-7  # golden stored in float32, like the reference
     assert O.rel_l2(O.rampfilter(w), d["filtered"]) < 1e-6
+
+
+def _fixture(name):
+    path = os.path.join(GOLDEN, f"refgpu_{name}.npz")
+    if not os.path.exists(path):
+        pytest.skip("reference-output fixture missing")
+    return np.load(path)
+
+
+def _compare_fixture(d, arr):
+    if "output" in d:
+        return O.rel_l2(arr, d["output"])
+    s = int(d["sub"])
+    assert tuple(arr.shape) == tuple(d["shape"])
+    assert abs(arr.sum(dtype=np.float64) - float(d["sum"])) <= 5e-4 * abs(float(d["sum"])) + 1e-3
+    return O.rel_l2(arr[::s, ::s, ::s], d["output_sub"])
+
+
+@pytest.mark.parametrize("name", ["fdk_small", "kats_small", "unw_small", "fdk_windows", "fdk_cfg1",
+                                  "proj_small", "proj_cfg1"])
+def test_reference_path_matches_reference_gpu_outputs(name):
+    """The texture-emulating restatement vs outputs of the reference's own CUDA build
+    recorded on a B200 (tests/golden/make_golden_gpu.py).  Bound 5e-4 rel-L2: the 8-bit
+    weight rounding is reproduced; the texture unit's remaining internal arithmetic is not
+    public."""
+    from tests.golden.ref_cases import build_case
+
+    d = _fixture(name)
+    pb, proj, vol, kind, mode = build_case(name)
+    emu = O.ref_backproject(pb, proj, kernel_mode=mode, texq=1) if kind == "bp" else O.ref_project(pb, vol, texq=1)
+    assert _compare_fixture(d, emu) < 5e-4
+
+
+def test_reference_window_quirk_is_what_the_reference_does():
+    """On the 48^3 / 72-pixel case the reference's detector window (16*(1+maxW/16) wide,
+    shifted left by 8: coneBeamGPU.cu:1597-1605) ends at column 67 of 72, and clamp
+    addressing repeats column 67 beyond it.  The ideal operator differs by ~30%; the
+    restatement (with the same windows) reproduces the reference."""
+    from tests.golden.ref_cases import build_case
+
+    d = _fixture("fdk_small")
+    pb, proj, vol, kind, mode = build_case("fdk_small")
+    g = O.ref_geometry(pb)
+    assert g["wwStart"][0] + g["subProjDim"][0] < pb.projDim[0]   # window truncates the detector
+    ideal = O.backproject_f64(pb, proj, kernel_mode=2)
+    assert O.rel_l2(ideal, d["output"]) > 0.1
+    assert O.rel_l2(O.ref_backproject(pb, proj, kernel_mode=2, texq=0), d["output"]) < 1e-3
