@@ -47,15 +47,16 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default=None, choices=["fdk-slab", "fdk-slab-bf16", "proj-256"],
+    ap.add_argument("--case", default=None, choices=["fdk-slab", "fdk-slab-bf16", "proj-512"],
                     help="profiling case: run only this kernel on a reduced workload (no JSON line)")
     return ap.parse_args()
 
 
 def run_case(args):
     """Reduced single-kernel workloads for ncu captures (a few GB on the device):
-    fdk-slab[-bf16]: the 1024^3 geometry restricted to a 1024x1024x256 z-slab, 120 views;
-    proj-256: the explicit projector on 256^3, 360 views, 384x256."""
+    fdk-slab[-bf16]: the 1024^3 geometry restricted to a 1024x1024x128 z-slab (z 448..575),
+    64 views (0.5 GB volume + 0.4 GB projections);
+    proj-512: both projectors on 512^3, 90 views, 768x512 detector (0.5 GB volume)."""
     import numpy as np
     import torch
 
@@ -65,12 +66,12 @@ def run_case(args):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     if args.case.startswith("fdk-slab"):
-        n = 120
+        n = 64
         g = ConeGeometry.circular(VOL, VOXEL_MM, DET, PITCH_MM, SOD_MM, SDD_MM, NVIEWS)
         import dataclasses
 
         g = dataclasses.replace(g, angles=g.angles[:n], hmid=g.hmid[:n], norm=np.full(n, 1.0 / NVIEWS, np.float32),
-                                woff=g.woff[:n], hoff=g.hoff[:n], vol_start=(0, 0, 384), vol_end=(1024, 1024, 640))
+                                woff=g.woff[:n], hoff=g.hoff[:n], vol_start=(0, 0, 448), vol_end=(1024, 1024, 576))
         dt = torch.bfloat16 if args.case.endswith("bf16") else torch.float32
         proj = torch.randn((n, DET[1], DET[0]), device=dev).to(dt)
         vol = torch.zeros(g.vol_shape, device=dev)
@@ -78,12 +79,13 @@ def run_case(args):
         for _ in range(args.warmup + args.steps):
             plan(proj, vol)
     else:
-        g = ConeGeometry.circular((256, 256, 256), 1.0, (384, 256), 1.0, 500.0, 1000.0, 360)
+        g = ConeGeometry.circular((512, 512, 512), 1.0, (768, 512), 1.0, 1000.0, 2000.0, 90)
         from fastcone_b200.phantom import random_ellipsoids
 
         v = ops.phantom(g.vol_xyz, random_ellipsoids(10, g.vol_xyz, 1), device=dev)
         for _ in range(args.warmup + args.steps):
             ops.project(v, g, method=_lib.PROJ_EXPLICIT)
+            ops.project(v, g, method=_lib.PROJ_TEXTURE)
     ops.sync_status()
     torch.cuda.synchronize()
     print("case", args.case, "done")
