@@ -306,7 +306,9 @@ def main():
     del proj16, plan16
 
     # secondary: forward projector Gsamples/s on 256^3, 360 views, 384 x 256
-    gp = ConeGeometry.circular((256, 256, 256), 1.0, (384, 256), 1.0, 500.0, 1000.0, 360)
+    from fastcone_b200 import configs
+
+    gp = configs.diff_batch()
     from fastcone_b200.phantom import random_ellipsoids
 
     pv = ops.phantom(gp.vol_xyz, random_ellipsoids(10, gp.vol_xyz, 1), device=dev)

@@ -138,6 +138,10 @@ int fcb_project_device(const fcb_geometry* g, int method, const float* volume, f
                        void* stream);
 int fcb_project_adjoint_device(const fcb_geometry* g, const float* proj, float* volume,
                                void* stream);
+/* fcb_project_device that also adds the number of trilinear samples taken to the 64-bit
+ * device counter *samples (the Gsamples work count of benchmarks). */
+int fcb_project_device_counted(const fcb_geometry* g, int method, const float* volume,
+                               float* proj, unsigned long long* samples, void* stream);
 
 /* Reusable backprojection plan (geometry digested once: per-view parameters, staging
  * window sizes).  execute() is asynchronous and allocates nothing. */
