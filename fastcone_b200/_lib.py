@@ -41,6 +41,7 @@ EXPORTED_SYMBOLS = [
     "fcb_project_device_counted",
     "fcb_bp_plan_create", "fcb_bp_plan_execute", "fcb_bp_plan_info", "fcb_bp_plan_destroy",
     "fcb_sync_status", "fcb_fdk_filter_device", "fcb_phantom_device",
+    "fcb_backproject_device_noalloc",
 ]
 
 
@@ -93,6 +94,7 @@ def lib():
             L.fcb_project_host.argtypes = [ctypes.c_int, gp, ctypes.c_int, vp, vp]
             L.fcb_backproject_device.argtypes = [gp, ctypes.c_int, vp, ctypes.c_int, vp, vp]
             L.fcb_project_device.argtypes = [gp, ctypes.c_int, vp, vp, vp]
+            L.fcb_backproject_device_noalloc.argtypes = [gp, ctypes.c_int, vp, ctypes.c_int, vp, vp]
             L.fcb_project_device_counted.argtypes = [gp, ctypes.c_int, vp, vp, vp, vp]
             L.fcb_project_adjoint_device.argtypes = [gp, vp, vp, vp]
             L.fcb_bp_plan_create.argtypes = [gp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(vp)]

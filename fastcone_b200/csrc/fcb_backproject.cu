@@ -20,6 +20,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "fcb_internal.h"
@@ -423,8 +424,11 @@ void fill_fdk_views(const Problem& pb, int mode, int v0, int n, FdkParams* P)
 }  // namespace
 
 namespace fcb {
-int bp_plan_create_ex(const fcb_geometry* g, int kernelMode, int projType, int maxViewsPerLaunch,
-                      fcb_bp_plan** out)
+// Builds a plan.  `scratch` (>= 3 ints of device memory: status word, footprint maxima)
+// receives the kernels' status and the footprint pre-pass result; the pre-pass runs on
+// `st`.  scratch == NULL selects the library's per-device scratch word block.
+static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, int maxViewsPerLaunch,
+                         int* scratch_in, cudaStream_t st, fcb_bp_plan** out)
 {
   if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
   *out = nullptr;
@@ -479,19 +483,22 @@ int bp_plan_create_ex(const fcb_geometry* g, int kernelMode, int projType, int m
       pl->fdk.push_back(P);
     }
     // footprint pre-pass -> staging box
-    int* scratch = nullptr;
-    rc = device_status_ptr(&scratch);
-    if (rc) { delete pl; return rc; }
+    int* scratch = scratch_in;
+    if (!scratch) {
+      rc = device_status_ptr(&scratch);
+      if (rc) { delete pl; return rc; }
+    }
     int* need = scratch + 1;
     const int ntiles = tiles_x * tiles_y * tiles_z;
-    cudaMemset(need, 0, 2 * sizeof(int));
+    cudaMemsetAsync(need, 0, 2 * sizeof(int), st);
     for (const FdkParams& P : pl->fdk) {
       const long long total = (long long)ntiles * P.nviews;
       const int blocks = (int)((total + 255) / 256);
-      fdk_footprint_kernel<<<blocks, 256>>>(P, NZ, ntiles, need);
+      fdk_footprint_kernel<<<blocks, 256, 0, st>>>(P, NZ, ntiles, need);
     }
     int h[2] = {0, 0};
-    cudaError_t e = cudaMemcpy(h, need, sizeof h, cudaMemcpyDeviceToHost);
+    cudaError_t e = cudaMemcpyAsync(h, need, sizeof h, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) { delete pl; return set_error(FCB_ERR_CUDA, cudaGetErrorString(e)); }
     const int align = 1 << pl->wshift;
     pl->BW = ((h[0] + align - 1) / align) * align;
@@ -536,6 +543,12 @@ int bp_plan_create_ex(const fcb_geometry* g, int kernelMode, int projType, int m
   }
   *out = pl;
   return ok();
+}
+
+int bp_plan_create_ex(const fcb_geometry* g, int kernelMode, int projType, int maxViewsPerLaunch,
+                      fcb_bp_plan** out)
+{
+  return bp_plan_build(g, kernelMode, projType, maxViewsPerLaunch, nullptr, 0, out);
 }
 
 int bp_plan_chunks(const fcb_bp_plan* pl, std::vector<std::pair<int, int>>* ranges)
@@ -646,4 +659,65 @@ extern "C" int fcb_backproject_device(const fcb_geometry* g, int kernelMode, con
   int rc = fcb_bp_plan_execute(pl, proj, volume, stream);
   fcb_bp_plan_destroy(pl);
   return rc;
+}
+
+// =====================================================================================
+// Backprojection without device-memory allocation
+// =====================================================================================
+// Some callers cannot allocate device memory while they run: a process whose GPU memory
+// is handed out by another allocator (a framework's caching pool, a fixed per-job
+// budget on a shared GPU) or a timing-critical loop that must not stop for an
+// allocation.  For them fcb_backproject_device_noalloc takes the few words of device
+// scratch the backprojector needs (the kernels' status word and the footprint maxima of
+// the staging-box pre-pass) from this file-scope array instead of cudaMalloc.  Every GPU
+// that loads the library holds the array until the process exits.
+constexpr int NOALLOC_SCRATCH_INTS = 64;  // 256 bytes; a call needs NOALLOC_NEEDED_INTS
+constexpr int NOALLOC_NEEDED_INTS = 3;    // [0] status word, [1..2] footprint maxima
+static __device__ __align__(256) int fcb_noalloc_scratch[NOALLOC_SCRATCH_INTS];
+
+// Device address of fcb_noalloc_scratch on the current device, looked up once per device
+// with that device current (the host-side name is only a stand-in for the symbol).
+static int noalloc_scratch_address(int** out)
+{
+  static std::mutex mu;
+  static int* addr[64] = {nullptr};
+  int dev = 0;
+  FCB_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(FCB_ERR_NODEVICE, "device index out of range");
+  std::lock_guard<std::mutex> lk(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, fcb_noalloc_scratch);
+    if (e != cudaSuccess)
+      return set_error(FCB_ERR_CUDA, std::string("cudaGetSymbolAddress(fcb_noalloc_scratch): ") +
+                                         cudaGetErrorString(e));
+    addr[dev] = static_cast<int*>(p);
+  }
+  *out = addr[dev];
+  return FCB_OK;
+}
+
+extern "C" int fcb_backproject_device_noalloc(const fcb_geometry* g, int kernelMode,
+                                              const void* proj, int projType, float* volume,
+                                              void* stream)
+{
+  if (!proj || !volume) return set_error(FCB_ERR_INVALID, "NULL projection or volume pointer");
+  if (NOALLOC_NEEDED_INTS > NOALLOC_SCRATCH_INTS)
+    return set_error(FCB_ERR_RANGE, "backprojection needs more scratch than the static array holds");
+  int* scratch = nullptr;
+  FCB_TRY(noalloc_scratch_address(&scratch));
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // the array keeps the previous call's contents: clear the status word and the maxima
+  FCB_CUDA_TRY(cudaMemsetAsync(scratch, 0, NOALLOC_NEEDED_INTS * sizeof(int), st));
+  fcb_bp_plan* pl = nullptr;
+  FCB_TRY(bp_plan_build(g, kernelMode, projType, FDK_MAXV, scratch, st, &pl));
+  int rc = bp_plan_execute_chunk(pl, -1, proj, volume, st);
+  fcb_bp_plan_destroy(pl);
+  if (rc) return rc;
+  int status = 0;
+  FCB_CUDA_TRY(cudaMemcpyAsync(&status, scratch, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FCB_CUDA_TRY(cudaStreamSynchronize(st));
+  if (status & DEV_TIMEOUT) return set_error(FCB_ERR_TIMEOUT, "a bounded device-side wait timed out");
+  if (status) return set_error(FCB_ERR_RANGE, "a kernel sample fell outside its staging window");
+  return ok();
 }

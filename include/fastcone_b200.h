@@ -152,6 +152,20 @@ int fcb_bp_plan_info(const fcb_bp_plan* plan, int* boxW, int* boxH, int* launche
                      long long* voxelViewUpdates);
 int fcb_bp_plan_destroy(fcb_bp_plan* plan);
 
+/* Same backprojection as fcb_backproject_device, for callers that cannot allocate device
+ * memory while they run (GPU memory owned by another allocator or a fixed budget, or a
+ * timing-critical loop that must not stop for an allocation).  No counterpart in the
+ * reference.  It calls no cudaMalloc/cudaFree and no allocating library routine: its
+ * device scratch -- the kernels' status word and the staging-box footprint maxima, 3 ints
+ * -- lives in a static 256-byte device array (64 ints) that every GPU loading the library
+ * holds until exit; a call whose scratch need exceeded that array would be rejected with
+ * FCB_ERR_RANGE.  The first call on a device looks up the array's device address (do it
+ * before any stream capture).  All calls share the array and clear it at their start, so
+ * calls whose GPU work overlaps (concurrent streams or threads) race on it.  The call is
+ * synchronous: it waits for `stream` and returns the kernels' device-side status. */
+int fcb_backproject_device_noalloc(const fcb_geometry* g, int kernelMode, const void* proj,
+                                   int projType, float* volume, void* stream);
+
 /* Waits for `stream` and returns FCB_ERR_TIMEOUT / FCB_ERR_RANGE if a kernel of this
  * library recorded a device-side failure since the previous check, else FCB_OK. */
 int fcb_sync_status(void* stream);
