@@ -461,6 +461,10 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
   const bool piwin = pl->mode == 1 && pb.piWindow;
   const float td_a = (float)(pb.pitch / (2.0 * M_PI * pb.pw));
   const float td_r = (float)(pb.D / pb.pw);
+  // The window's w axis runs against the source's direction of travel when the helix is
+  // right-handed (angles and height increasing together); mirrored otherwise.
+  const double turn = pb.nviews > 1 ? pb.angle[pb.nviews - 1] - pb.angle[0] : 1.0;
+  const float td_sign = (turn >= 0.0) == (pb.pitch >= 0.0) ? -1.0f : 1.0f;
 
   if (aligned_geometry(pb)) {
     pl->path = 1;
@@ -478,7 +482,7 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
       P.wshift = pl->wshift;
       P.wexp = wexp;
       P.piwin = piwin ? 1 : 0;
-      P.td_a = td_a; P.td_r = td_r; P.td_sign = 1.0f;
+      P.td_a = td_a; P.td_r = td_r; P.td_sign = td_sign;
       fill_fdk_views(pb, pl->mode, v0, std::min(pl->maxv, pb.nviews - v0), &P);
       pl->fdk.push_back(P);
     }
