@@ -17,6 +17,7 @@
 //    projective matrix, bilinear gathers from global memory; also the fallback for
 //    projection buffers whose layout a TMA descriptor cannot describe.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -134,29 +135,91 @@ __global__ void fdk_footprint_kernel(const __grid_constant__ FdkParams P, int nz
   }
 }
 
-template <typename T>
-__device__ __forceinline__ float ld_tap(const T* p);
-template <>
-__device__ __forceinline__ float ld_tap<float>(const float* p) { return *p; }
-template <>
-__device__ __forceinline__ float ld_tap<__half>(const __half* p) { return __half2float(*p); }
-template <>
-__device__ __forceinline__ float ld_tap<__nv_bfloat16>(const __nv_bfloat16* p)
+// ---- shared-memory taps: 32-bit addresses, immediate offsets, converted to float
+typedef unsigned long long u64;
+
+template <typename T, int OFF>
+__device__ __forceinline__ float lds_tap(uint32_t a);
+template <int OFF>
+__device__ __forceinline__ float lds_f32(uint32_t a)
 {
-  return __uint_as_float(((uint32_t)(*reinterpret_cast<const unsigned short*>(p))) << 16);
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(a), "n"(OFF));
+  return v;
+}
+template <int OFF>
+__device__ __forceinline__ uint32_t lds_u16(uint32_t a)
+{
+  unsigned short v;
+  asm volatile("ld.shared.u16 %0, [%1+%2];" : "=h"(v) : "r"(a), "n"(OFF));
+  return v;
+}
+template <typename T, int OFF>
+struct Tap;
+template <int OFF>
+struct Tap<float, OFF> {
+  static __device__ __forceinline__ float ld(uint32_t a) { return lds_f32<OFF * 4>(a); }
+};
+template <int OFF>
+struct Tap<__half, OFF> {
+  static __device__ __forceinline__ float ld(uint32_t a)
+  {
+    return __half2float(__ushort_as_half((unsigned short)lds_u16<OFF * 2>(a)));
+  }
+};
+template <int OFF>
+struct Tap<__nv_bfloat16, OFF> {
+  static __device__ __forceinline__ float ld(uint32_t a) { return __uint_as_float(lds_u16<OFF * 2>(a) << 16); }
+};
+
+// ---- packed FP32 pairs (sm_100 f32x2 arithmetic): two z-voxels per instruction
+__device__ __forceinline__ u64 pk2(float lo, float hi)
+{
+  u64 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void up2(u64 v, float& lo, float& hi)
+{
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ u64 add2(u64 a, u64 b)
+{
+  u64 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ u64 add2_rm(u64 a, u64 b)
+{
+  u64 r;
+  asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ u64 sub2(u64 a, u64 b)
+{
+  u64 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
+{
+  u64 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
 }
 
-template <typename T, int NZ>
+template <typename T, int NZ, bool PIW, bool X2>
 __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_constant__ CUtensorMap tmap,
                                                               const __grid_constant__ FdkParams P)
 {
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int ES = (int)sizeof(T);
   const int stage_elems = P.BW * P.BH;
-  const int stage_bytes = ((stage_elems * (int)sizeof(T)) + 127) & ~127;
-  T* stages = reinterpret_cast<T*>(smem_raw);
+  const int stage_bytes = ((stage_elems * ES) + 127) & ~127;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)P.stages * stage_bytes);
   uint64_t* empty = full + P.stages;
   int2* origin = reinterpret_cast<int2*>(empty + P.stages);
+  const uint32_t smem_base = dev::smem_u32(smem_raw);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int tx, ty, tz;
@@ -175,7 +238,7 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
     // ------------------------------------------------------------- producer warp
     if (lane != 0) return;
     dev::tma_prefetch(&tmap);
-    const uint32_t bytes = (uint32_t)(stage_elems * (int)sizeof(T));
+    const uint32_t bytes = (uint32_t)(stage_elems * ES);
     int issued = 0;
     bool failed = false;
     for (int v = 0; v < P.nviews; v++) {
@@ -191,8 +254,7 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
       if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
       origin[s] = make_int2(w0, h0);
       dev::mbar_arrive_expect_tx(&full[s], bytes);
-      dev::tma_load_3d(stages + (size_t)s * (stage_bytes / sizeof(T)), &tmap, &full[s], w0, h0,
-                       P.view0 + v);
+      dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + v);
       issued = v + 1;
     }
     if (failed) {
@@ -210,11 +272,18 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
   const int zl = tz * NZ;
   const float x = P.ox + (float)xl, y = P.oy + (float)yl, zf = P.oz + (float)zl;
   const float MAGIC = 12582912.0f;  // 1.5 * 2^23: adding it in round-down mode floors
-  const unsigned MAGIC_BITS = 0x4B400000u;
+  const uint32_t MAGIC_BITS = 0x4B400000u;
+  const uint32_t rowb = (uint32_t)(P.BW * ES);  // bytes per staged row
 
-  float acc[NZ];
+  constexpr int NACC = X2 ? NZ / 2 : NZ;
+  static_assert(!X2 || (NZ % 2 == 0), "pairs");
+  u64 acc2[X2 ? NACC : 1];
+  float acc[X2 ? 1 : NACC];
 #pragma unroll
-  for (int k = 0; k < NZ; k++) acc[k] = 0.0f;
+  for (int k = 0; k < NACC; k++) {
+    if constexpr (X2) acc2[k] = 0ull;
+    else acc[k] = 0.0f;
+  }
 
   for (int v = 0; v < P.nviews; v++) {
     const int s = v % P.stages;
@@ -224,7 +293,6 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
     }
     const FdkView& V = P.v[v];
     const int2 org = origin[s];
-    const T* S = stages + (size_t)s * (stage_bytes / sizeof(T));
 
     const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
     const float U = __frcp_rn(den);
@@ -239,14 +307,15 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
     // memory safety: every tap must stay inside the staged box
     int iw = __float2int_rd(wl);
     const float hl = fmaf((float)(NZ - 1), dh, h0);
-    if (iw < 0 || iw > P.BW - 2 || !(h0 >= 0.0f) || !(hl < (float)(P.BH - 1))) {
+    // (0.01 px of slack covers the rounding of the incremental row stepping below)
+    if (iw < 0 || iw > P.BW - 2 || !(h0 >= 0.0f) || !(hl + 0.01f < (float)(P.BH - 1))) {
       dev::record_status(P.status, DEV_RANGE);
       iw = 0; wl = 0.0f; h0 = 0.0f; dh = 0.0f; wt = 0.0f;
     }
     const float fw = wl - (float)iw;
 
     float lo = -3.0e38f, hi = 3.0e38f;  // Tam-Danielsson bounds (local h)
-    if (P.piwin) {
+    if constexpr (PIW) {
       const float u = (wabs - V.wc) * P.td_sign / P.td_r;
       const float q = P.td_a * (1.0f + u * u);
       const float at = atanf(u);
@@ -255,22 +324,57 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
       lo = hsrc - q * (1.5707963267948966f + at);
     }
 
-    const unsigned base = (unsigned)iw - MAGIC_BITS * (unsigned)P.BW;
+    // byte address of tap (row r, column iw) = bits(MAGIC + r) * rowb + base
+    const uint32_t base = smem_base + (uint32_t)s * (uint32_t)stage_bytes + (uint32_t)iw * ES -
+                          MAGIC_BITS * rowb;
+    if constexpr (X2) {
+      const u64 MAG2 = pk2(MAGIC, MAGIC);
+      const u64 FW2 = pk2(fw, fw);
+      const u64 WT2 = pk2(wt, wt);
+      const u64 D2 = pk2(2.0f * dh, 2.0f * dh);
+      u64 H = pk2(h0, h0 + dh);
 #pragma unroll
-    for (int k = 0; k < NZ; k++) {
-      const float hk = fmaf((float)k, dh, h0);
-      const float t = __fadd_rd(hk, MAGIC);
-      const unsigned idx = (unsigned)__float_as_int(t) * (unsigned)P.BW + base;
-      const float fh = hk - (t - MAGIC);
-      const T* p = S + idx;
-      const float a = ld_tap<T>(p), b = ld_tap<T>(p + 1);
-      const float c = ld_tap<T>(p + P.BW), d = ld_tap<T>(p + P.BW + 1);
-      const float r0 = fmaf(fw, b - a, a);
-      const float r1 = fmaf(fw, d - c, c);
-      const float val = fmaf(fh, r1 - r0, r0);
-      float wk = wt;
-      if (P.piwin) wk = (hk >= lo && hk <= hi) ? wt : 0.0f;
-      acc[k] = fmaf(wk, val, acc[k]);
+      for (int k = 0; k < NACC; k++) {
+        const u64 T2 = add2_rm(H, MAG2);
+        const u64 FH = sub2(H, sub2(T2, MAG2));
+        float t0, t1;
+        up2(T2, t0, t1);
+        const uint32_t a0 = (uint32_t)__float_as_uint(t0) * rowb + base;
+        const uint32_t a1 = (uint32_t)__float_as_uint(t1) * rowb + base;
+        const uint32_t c0 = a0 + rowb, c1 = a1 + rowb;
+        const u64 A = pk2(Tap<T, 0>::ld(a0), Tap<T, 0>::ld(a1));
+        const u64 B = pk2(Tap<T, 1>::ld(a0), Tap<T, 1>::ld(a1));
+        const u64 C = pk2(Tap<T, 0>::ld(c0), Tap<T, 0>::ld(c1));
+        const u64 Dd = pk2(Tap<T, 1>::ld(c0), Tap<T, 1>::ld(c1));
+        const u64 R0 = fma2(FW2, sub2(B, A), A);
+        const u64 R1 = fma2(FW2, sub2(Dd, C), C);
+        const u64 VAL = fma2(FH, sub2(R1, R0), R0);
+        u64 W = WT2;
+        if constexpr (PIW) {
+          float h0k, h1k;
+          up2(H, h0k, h1k);
+          W = pk2((h0k >= lo && h0k <= hi) ? wt : 0.0f, (h1k >= lo && h1k <= hi) ? wt : 0.0f);
+        }
+        acc2[k] = fma2(W, VAL, acc2[k]);
+        H = add2(H, D2);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NZ; k++) {
+        const float hk = fmaf((float)k, dh, h0);
+        const float t = __fadd_rd(hk, MAGIC);
+        const uint32_t a = (uint32_t)__float_as_uint(t) * rowb + base;
+        const uint32_t c = a + rowb;
+        const float fh = hk - (t - MAGIC);
+        const float ta = Tap<T, 0>::ld(a), tb = Tap<T, 1>::ld(a);
+        const float tc = Tap<T, 0>::ld(c), td = Tap<T, 1>::ld(c);
+        const float r0 = fmaf(fw, tb - ta, ta);
+        const float r1 = fmaf(fw, td - tc, tc);
+        const float val = fmaf(fh, r1 - r0, r0);
+        float wk = wt;
+        if constexpr (PIW) wk = (hk >= lo && hk <= hi) ? wt : 0.0f;
+        acc[k] = fmaf(wk, val, acc[k]);
+      }
     }
     __syncwarp();
     if (lane == 0) dev::mbar_arrive(&empty[s]);
@@ -280,12 +384,27 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
     float* out = P.vol + (size_t)yl * P.nx + xl;
     const size_t plane = (size_t)P.nx * P.ny;
 #pragma unroll
-    for (int k = 0; k < NZ; k++) {
-      if (zl + k < P.nz) out[(size_t)(zl + k) * plane] += acc[k];
+    for (int k = 0; k < NACC; k++) {
+      float v0, v1;
+      int k0;
+      if constexpr (X2) {
+        up2(acc2[k], v0, v1);
+        k0 = 2 * k;
+        if (zl + k0 < P.nz) out[(size_t)(zl + k0) * plane] += v0;
+        if (zl + k0 + 1 < P.nz) out[(size_t)(zl + k0 + 1) * plane] += v1;
+      } else {
+        (void)v1;
+        v0 = acc[k];
+        k0 = k;
+        if (zl + k0 < P.nz) out[(size_t)(zl + k0) * plane] += v0;
+      }
     }
   }
 }
 
+}  // namespace fcb
+
+namespace fcb {
 // =====================================================================================
 // Generic projective-matrix kernel
 // =====================================================================================
@@ -381,12 +500,12 @@ struct fcb_bp_plan {
 
 namespace {
 
-template <typename T, int NZ>
+template <typename T, int NZ, bool PIW, bool X2>
 int launch_fdk(const fcb_bp_plan* pl, const CUtensorMap& map, int chunk, cudaStream_t st)
 {
   const size_t stage_bytes = ((size_t)pl->BW * pl->BH * sizeof(T) + 127) & ~(size_t)127;
   const size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int2));
-  auto kern = fdk_tma_kernel<T, NZ>;
+  auto kern = fdk_tma_kernel<T, NZ, PIW, X2>;
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int c = 0; c < (int)pl->fdk.size(); c++) {
     if (chunk >= 0 && c != chunk) continue;
@@ -584,9 +703,22 @@ int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* v
                            pb.nviews, (uint64_t)pb.projWHSize[0] * es,
                            (uint64_t)pb.projWHSize[0] * pb.projWHSize[1] * es, pl->BW, pl->BH, 1));
     for (FdkParams& P : pl->fdk) P.vol = volume;
-    if (pl->ptype == FCB_F32) FCB_TRY((launch_fdk<float, 32>(pl, map, chunk, st)));
-    else if (pl->ptype == FCB_F16) FCB_TRY((launch_fdk<__half, 32>(pl, map, chunk, st)));
-    else FCB_TRY((launch_fdk<__nv_bfloat16, 32>(pl, map, chunk, st)));
+    const bool piw = pl->fdk[0].piwin != 0;
+    // FCB_FDK_SCALAR=1 selects the one-voxel-per-instruction FP32 path (for comparison)
+    static const bool scalar = getenv("FCB_FDK_SCALAR") && getenv("FCB_FDK_SCALAR")[0] == '1';
+    if (pl->ptype == FCB_F32 && scalar) {
+      if (piw) FCB_TRY((launch_fdk<float, 32, true, false>(pl, map, chunk, st)));
+      else FCB_TRY((launch_fdk<float, 32, false, false>(pl, map, chunk, st)));
+    } else if (pl->ptype == FCB_F32) {
+      if (piw) FCB_TRY((launch_fdk<float, 32, true, true>(pl, map, chunk, st)));
+      else FCB_TRY((launch_fdk<float, 32, false, true>(pl, map, chunk, st)));
+    } else if (pl->ptype == FCB_F16) {
+      if (piw) FCB_TRY((launch_fdk<__half, 32, true, false>(pl, map, chunk, st)));
+      else FCB_TRY((launch_fdk<__half, 32, false, false>(pl, map, chunk, st)));
+    } else {
+      if (piw) FCB_TRY((launch_fdk<__nv_bfloat16, 32, true, false>(pl, map, chunk, st)));
+      else FCB_TRY((launch_fdk<__nv_bfloat16, 32, false, false>(pl, map, chunk, st)));
+    }
     return ok();
   }
   if (pl->gen.empty()) {

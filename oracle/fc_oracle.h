@@ -99,9 +99,7 @@ int orc_ref_backproject_points(const int* xyz, int npts, float* out,
 
 /* Voxel-driven backprojection, FP64: weight U^p with p = 2 (FDK), 1 (Katsevich) or the
  * unweighted plane-intersection form (p = 0; uses misAlignments, may be NULL).
- * vol (double, volStart..volEnd sub-array) += sum_t norm[t] * U^p * bilinear(P_t).
- * piwin != 0 (Katsevich only) multiplies by the Tam-Danielsson window indicator with
- * helix pitch `pitch_voxels` (z advance per 2*pi, voxels). */
+ * vol (double, volStart..volEnd sub-array) += sum_t norm[t] * U^p * bilinear(P_t). */
 int orc_backproject_f64(double* vol, const float* projections,
                         const int volDim[3], const int volStart[3], const int volEnd[3],
                         const int projDim[3], const int projWHSize[2],
@@ -109,6 +107,16 @@ int orc_backproject_f64(double* vol, const float* projections,
                         const float* angles, const float* hMid, double D,
                         const float* norm, double pw, int kernelMode,
                         const float* misAlignments);
+
+/* Katsevich backprojection (weight U) restricted to each voxel's PI interval (the
+ * Tam-Danielsson window on the virtual detector), FP64; *pairs = voxel-view pairs inside.
+ * pitch = source rise per turn, voxels. */
+int orc_katsevich_piwin_f64(double* vol, const float* projections,
+                            const int volDim[3], const int volStart[3], const int volEnd[3],
+                            const int projDim[3], const int projWHSize[2],
+                            const int* projWOffset, const int* projHOffset,
+                            const float* angles, const float* hMid, double D,
+                            const float* norm, double pw, double pitch, int64_t* pairs);
 
 int orc_backproject_points_f64(const int* xyz, int npts, double* out,
                                const float* projections,

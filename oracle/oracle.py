@@ -284,6 +284,20 @@ def backproject_f64(pb: Problem, proj, kernel_mode=2, mis=None):
     return vol
 
 
+def katsevich_piwin_f64(pb: Problem, proj, pitch):
+    """Katsevich backprojection (weight U) over each voxel's PI interval, FP64; returns
+    (volume, number of voxel-view pairs inside the window)."""
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    vol = np.zeros(pb.vol_shape_zyx, dtype=np.float64)
+    pairs = ctypes.c_int64(0)
+    rc = lib().orc_katsevich_piwin_f64(_p(vol, _f64p), _p(proj, _f32p), *pb.args()[:7],
+                                       _p(pb.angles, _f32p), _p(pb.hMid, _f32p), ctypes.c_double(pb.D),
+                                       _p(pb.norm, _f32p), ctypes.c_double(pb.pw), ctypes.c_double(pitch),
+                                       ctypes.byref(pairs))
+    assert rc == 0
+    return vol, int(pairs.value)
+
+
 def backproject_points_f64(pb: Problem, proj, pts, kernel_mode=2):
     proj = np.ascontiguousarray(proj, dtype=np.float32)
     pts = np.ascontiguousarray(pts, dtype=np.int32)

@@ -134,3 +134,25 @@ def test_misaligned_unweighted():
                    misAlignments=mis, pixelWidth=pb.pw)
     ref64 = O.backproject_f64(pb, proj, kernel_mode=0, mis=mis)
     assert O.rel_l2(vol, ref64) < 2e-5
+
+
+def test_katsevich_pi_window_vs_f64():
+    """Katsevich backprojection restricted to the PI window (Tam-Danielsson bounds, oriented
+    by the helix handedness) vs the FP64 oracle.  Voxel-view pairs within rounding of the
+    window boundary may flip, hence the looser bound."""
+    import torch
+
+    from fastcone_b200 import ops
+    from fastcone_b200.geometry import ConeGeometry
+
+    n, vpt = 240, 80
+    P = 24.0
+    g = ConeGeometry.helical((48, 48, 40), 1.0, (96, 24), 1.0, 150.0, 300.0, n // vpt, vpt, P,
+                             pi_window=True)
+    g = g.with_norm(np.full(n, 1.0 / vpt, np.float32))
+    pb = O.make_problem(g.vol_xyz, g.det_wh, n, D=g.D, pw=g.pw, angles=g.angles, hmid=g.hmid, norm=g.norm)
+    proj = np.random.default_rng(9).random(pb.proj_shape, dtype=np.float32) + 0.5
+    got = ops.backproject(torch.from_numpy(proj).cuda(), g, mode=1).cpu().numpy()
+    ref, pairs = O.katsevich_piwin_f64(pb, proj, g.helical_pitch)
+    assert pairs > 0
+    assert O.rel_l2(got, ref) < 2e-3, O.rel_l2(got, ref)
