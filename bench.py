@@ -76,8 +76,17 @@ def run_case(args):
         proj = torch.randn((n, DET[1], DET[0]), device=dev).to(dt)
         vol = torch.zeros(g.vol_shape, device=dev)
         plan = ops.BackprojectPlan(g, mode=_lib.MODE_FDK, dtype=dt)
-        for _ in range(args.warmup + args.steps):
+        for _ in range(args.warmup):
             plan(proj, vol)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            plan(proj, vol)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        upd = 1024 * 1024 * 128 * n
+        print(json.dumps({"case": args.case, "ms": ms, "GUPS": upd / ms / 1e6, "box": plan.info()}))
     else:
         g = ConeGeometry.circular((512, 512, 512), 1.0, (768, 512), 1.0, 1000.0, 2000.0, 90)
         from fastcone_b200.phantom import random_ellipsoids
