@@ -22,6 +22,7 @@ SOURCES = [
     "fcb_backproject.cu",
     "fcb_project.cu",
     "fcb_filter.cu",
+    "fcb_katsevich.cu",
     "fcb_capi.cpp",
 ]
 

@@ -1,0 +1,222 @@
+// fcb_katsevich.cu -- Katsevich filtering for helical cone-beam data (sm_100a).
+//
+// The reference has only the Katsevich backprojection weight (coneBeamGPU.cu:258-338) and
+// expects pre-filtered, windowed data.  This file supplies the filtering of Katsevich's
+// exact helical inversion in the flat-detector form of Noo, Pack & Heuscher (Phys. Med.
+// Biol. 48 (2003) 3787-3818), on the virtual detector through the rotation axis
+// (source-detector distance = source-axis distance D).  Detector pixel (i, j) sits at
+// w = (i - W/2) pw, v = (j - H/2) pw; the published coordinate u runs along the source's
+// direction of travel, u = s_u * w with s_u = -1 for a right-handed helix (angles and
+// height increasing together).  Stages:
+//   1. derivative at fixed ray direction  g1 = dg/dlam + (u^2+D^2)/D dg/du + u v/D dg/dv
+//      and length correction g2 = D / sqrt(u^2+D^2+v^2) g1      (deriv_kernel)
+//   2. forward height rebinning onto kappa-lines v_k(u, psi) = P/(2 pi)(psi + psi/tan(psi) u/D)
+//      (rebin_fwd_kernel, per-(kappa, column) interpolation table built on the host in FP64)
+//   3. Hilbert transform along u, band-limited kernel (1 - cos(pi n))/(pi n) (hilbert_kernel)
+//   4. backward rebinning through the kappa-line of smallest |psi| (rebin_bwd_kernel,
+//      per-(row, column) table).
+// Backprojection with weight U over each voxel's PI interval and norm dlam/(2 pi D) then
+// reconstructs (fdk_tma_kernel with the Tam-Danielsson window).
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "fcb_internal.h"
+
+namespace fcb {
+
+__global__ void kats_deriv_kernel(const float* __restrict__ g, float* __restrict__ g2, int n, int H,
+                                  int W, float dlam, float pw, float D, float su)
+{
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long tot = (long long)n * H * W;
+  if (idx >= tot) return;
+  const int i = (int)(idx % W);
+  const long long r = idx / W;
+  const int j = (int)(r % H), t = (int)(r / H);
+  const size_t plane = (size_t)H * W;
+  const float* gt = g + (size_t)t * plane;
+  // dg/dlam: central inside, one-sided at the ends (numpy.gradient, edge order 1)
+  float dl;
+  if (n == 1) dl = 0.0f;
+  else if (t == 0) dl = (g[plane + (size_t)j * W + i] - gt[(size_t)j * W + i]) / dlam;
+  else if (t == n - 1) dl = (gt[(size_t)j * W + i] - g[(size_t)(t - 1) * plane + (size_t)j * W + i]) / dlam;
+  else dl = (g[(size_t)(t + 1) * plane + (size_t)j * W + i] - g[(size_t)(t - 1) * plane + (size_t)j * W + i]) / (2.0f * dlam);
+  // dg/du with u_i = su * (i - W/2) pw
+  const float du = su * pw;
+  float dgu;
+  if (W == 1) dgu = 0.0f;
+  else if (i == 0) dgu = (gt[(size_t)j * W + 1] - gt[(size_t)j * W]) / du;
+  else if (i == W - 1) dgu = (gt[(size_t)j * W + i] - gt[(size_t)j * W + i - 1]) / du;
+  else dgu = (gt[(size_t)j * W + i + 1] - gt[(size_t)j * W + i - 1]) / (2.0f * du);
+  float dgv;
+  if (H == 1) dgv = 0.0f;
+  else if (j == 0) dgv = (gt[(size_t)W + i] - gt[i]) / pw;
+  else if (j == H - 1) dgv = (gt[(size_t)j * W + i] - gt[(size_t)(j - 1) * W + i]) / pw;
+  else dgv = (gt[(size_t)(j + 1) * W + i] - gt[(size_t)(j - 1) * W + i]) / (2.0f * pw);
+  const float u = su * (float)(i - W / 2) * pw, v = (float)(j - H / 2) * pw;
+  const float g1 = dl + ((u * u + D * D) / D) * dgu + (u * v / D) * dgv;
+  g2[idx] = g1 * (D * rsqrtf(u * u + D * D + v * v));
+}
+
+// g3[t][k][i] = g2[t][j0][i] * (1-a) + g2[t][j0+1][i] * a from the (kappa, column) table
+__global__ void kats_rebin_fwd_kernel(const float* __restrict__ g2, float* __restrict__ g3,
+                                      const int* __restrict__ j0tab, const float* __restrict__ atab,
+                                      int n, int H, int W, int K)
+{
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long tot = (long long)n * K * W;
+  if (idx >= tot) return;
+  const int i = (int)(idx % W);
+  const long long r = idx / W;
+  const int k = (int)(r % K), t = (int)(r / K);
+  const int j0 = j0tab[(size_t)k * W + i];
+  float val = 0.0f;
+  if (j0 >= 0) {
+    const float a = atab[(size_t)k * W + i];
+    const float* col = g2 + (size_t)t * H * W + i;
+    const float v0 = col[(size_t)j0 * W];
+    const float v1 = (j0 + 1 < H) ? col[(size_t)(j0 + 1) * W] : v0;
+    val = fmaf(a, v1 - v0, v0);
+  }
+  g3[idx] = val;
+}
+
+// Hilbert transform of each row along u: out[i] = sgn * sum_j h(i - j) in[j],
+// h(m) = 2 / (pi m) for odd m, 0 otherwise; one block per row, the row staged in shared memory.
+__global__ void kats_hilbert_kernel(const float* __restrict__ in, float* __restrict__ out, int W,
+                                    float sgn)
+{
+  extern __shared__ float row[];
+  const size_t r = blockIdx.x;
+  for (int j = threadIdx.x; j < W; j += blockDim.x) row[j] = in[r * W + j];
+  __syncthreads();
+  const float c = sgn * 0.63661977236758134f;  // 2 / pi
+  for (int i = threadIdx.x; i < W; i += blockDim.x) {
+    float acc = 0.0f;
+    // j = i - m with m odd: j runs over the columns of opposite parity to i
+    for (int j = (i & 1) ^ 1; j < W; j += 2) acc = fmaf(row[j], __frcp_rn((float)(i - j)), acc);
+    out[r * W + i] = c * acc;
+  }
+}
+
+// gF[t][j][i] = g4[t][k0][i] * (1-a) + g4[t][k0+1][i] * a from the (row, column) table
+__global__ void kats_rebin_bwd_kernel(const float* __restrict__ g4, float* __restrict__ gF,
+                                      const int* __restrict__ k0tab, const float* __restrict__ atab,
+                                      int n, int H, int W, int K)
+{
+  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long tot = (long long)n * H * W;
+  if (idx >= tot) return;
+  const int i = (int)(idx % W);
+  const long long r = idx / W;
+  const int j = (int)(r % H), t = (int)(r / H);
+  const int k0 = k0tab[(size_t)j * W + i];
+  const float a = atab[(size_t)j * W + i];
+  const float* col = g4 + (size_t)t * K * W + i;
+  const float v0 = col[(size_t)k0 * W], v1 = col[(size_t)(k0 + 1) * W];
+  gF[idx] = fmaf(a, v1 - v0, v0);
+}
+
+}  // namespace fcb
+
+using namespace fcb;
+
+// np.interp-style lookup on an increasing abscissa: fractional index of x in xs.
+static double frac_index(const std::vector<double>& xs, double x)
+{
+  const int n = (int)xs.size();
+  if (x <= xs[0]) return 0.0;
+  if (x >= xs[n - 1]) return (double)(n - 1);
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) / 2;
+    if (xs[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo + (x - xs[lo]) / (xs[hi] - xs[lo]);
+}
+
+extern "C" int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, int W,
+                                           const float* angles, float D, float pw, float pitch,
+                                           int nkappa, void* stream)
+{
+  if (!in || !out || !angles || nviews < 2 || H < 2 || W < 2 || !(D > 0) || !(pw > 0) || pitch == 0.0f)
+    return set_error(FCB_ERR_INVALID, "bad Katsevich filter arguments");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // mean angular step; float32 angles of several turns carry ~1e-6 rad of rounding each
+  const double dlam = ((double)angles[nviews - 1] - (double)angles[0]) / (nviews - 1);
+  for (int t = 1; t < nviews; t++) {
+    const double d = (double)angles[t] - (double)angles[t - 1];
+    if (fabs(d - dlam) > 1e-3 * fabs(dlam) + 1e-5)
+      return set_error(FCB_ERR_INVALID, "Katsevich filtering needs uniformly spaced views");
+  }
+  const double turn = (double)angles[nviews - 1] - (double)angles[0];
+  const double su = ((turn >= 0.0) == (pitch >= 0.0)) ? -1.0 : 1.0;
+  const int K = nkappa > 1 ? nkappa : 2 * H;
+  // kappa-line tables (FP64): v_k(u_i, psi_k), forward (kappa, column) and backward (row, column)
+  std::vector<double> u(W), v(H);
+  for (int i = 0; i < W; i++) u[i] = su * (double)(i - W / 2) * pw;
+  for (int j = 0; j < H; j++) v[j] = (double)(j - H / 2) * pw;
+  double umax = 0.0;
+  for (int i = 0; i < W; i++) umax = std::max(umax, fabs(u[i]));
+  const double am = atan(umax / D);
+  const double P = pitch;
+  std::vector<int> fj0((size_t)K * W), bk0((size_t)H * W);
+  std::vector<float> fa((size_t)K * W), ba((size_t)H * W);
+  std::vector<double> vk(K);
+  for (int i = 0; i < W; i++) {
+    for (int k = 0; k < K; k++) {
+      const double psi = -M_PI / 2 - am + (M_PI + 2 * am) * k / (double)(K - 1);
+      const double cot = fabs(psi) < 1e-12 ? 1.0 : psi / tan(psi);
+      vk[k] = (P / (2 * M_PI)) * (psi + cot * u[i] / D);
+      // forward: linear interpolation in v, zero outside the detector rows
+      const double x = vk[k];
+      if (x < v[0] || x > v[H - 1]) {
+        fj0[(size_t)k * W + i] = -1;
+        fa[(size_t)k * W + i] = 0.0f;
+      } else {
+        const double f = frac_index(v, x);
+        const int j0 = std::min((int)floor(f), H - 2);
+        fj0[(size_t)k * W + i] = j0;
+        fa[(size_t)k * W + i] = (float)(f - j0);
+      }
+    }
+    for (int j = 0; j < H; j++) {
+      const double f = frac_index(vk, v[j]);
+      const int k0 = std::min((int)floor(f), K - 2);
+      bk0[(size_t)j * W + i] = k0;
+      ba[(size_t)j * W + i] = (float)(f - k0);
+    }
+  }
+  const size_t nhw = (size_t)nviews * H * W, nkw = (size_t)nviews * K * W;
+  float *g2 = nullptr, *g3 = nullptr, *g4 = nullptr, *dfa = nullptr, *dba = nullptr;
+  int *dfj = nullptr, *dbk = nullptr;
+  int rc = FCB_OK;
+  do {
+    if (cudaMalloc(&g2, nhw * 4) || cudaMalloc(&g3, nkw * 4) || cudaMalloc(&g4, nkw * 4) ||
+        cudaMalloc(&dfa, fa.size() * 4) || cudaMalloc(&dba, ba.size() * 4) ||
+        cudaMalloc(&dfj, fj0.size() * 4) || cudaMalloc(&dbk, bk0.size() * 4)) {
+      cudaGetLastError();
+      rc = set_error(FCB_ERR_NOMEM, "Katsevich filter scratch");
+      break;
+    }
+    cudaMemcpyAsync(dfa, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dba, ba.data(), ba.size() * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dfj, fj0.data(), fj0.size() * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dbk, bk0.data(), bk0.size() * 4, cudaMemcpyHostToDevice, st);
+    kats_deriv_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(in, g2, nviews, H, W, (float)dlam,
+                                                                     pw, D, (float)su);
+    kats_rebin_fwd_kernel<<<(unsigned)((nkw + 255) / 256), 256, 0, st>>>(g2, g3, dfj, dfa, nviews, H, W, K);
+    // the published Hilbert transform runs along increasing u; along w it changes sign when u = -w
+    kats_hilbert_kernel<<<(unsigned)((size_t)nviews * K), 256, W * sizeof(float), st>>>(g3, g4, W,
+                                                                                        (float)su);
+    kats_rebin_bwd_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(g4, out, dbk, dba, nviews, H, W, K);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) rc = set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
+  } while (0);
+  cudaFree(g2); cudaFree(g3); cudaFree(g4); cudaFree(dfa); cudaFree(dba); cudaFree(dfj); cudaFree(dbk);
+  return rc ? rc : ok();
+}

@@ -133,6 +133,34 @@ def fdk_filter(proj: torch.Tensor, geom: ConeGeometry | None = None, out_dtype=t
     return out
 
 
+def katsevich_filter(proj: torch.Tensor, geom: ConeGeometry, n_kappa: int = 0,
+                     out: torch.Tensor | None = None) -> torch.Tensor:
+    """Katsevich filtering of helical projections (float32 (n, H, W)) for geom's helix."""
+    if geom.helical_pitch == 0.0:
+        raise ValueError("Katsevich filtering needs a helical geometry (helical_pitch != 0)")
+    n, H, W = proj.shape
+    if out is None:
+        out = torch.empty_like(proj)
+    check(lib().fcb_katsevich_filter_device(_dev(proj, "proj", torch.float32), _dev(out, "out", torch.float32),
+                                            n, H, W, geom.angles.ctypes.data_as(_lib.c_float_p), float(geom.D),
+                                            float(geom.pw), float(geom.helical_pitch), int(n_kappa), _stream()))
+    return out
+
+
+def katsevich_reconstruct(proj: torch.Tensor, geom: ConeGeometry, n_kappa: int = 0,
+                          dtype=torch.float32) -> torch.Tensor:
+    """Exact helical reconstruction: Katsevich filtering, then backprojection with weight U
+    over each voxel's PI interval, norm = (angle step) / (2 pi D)."""
+    import dataclasses
+    import math
+
+    gF = katsevich_filter(proj, geom, n_kappa)
+    dlam = (float(geom.angles[-1]) - float(geom.angles[0])) / (geom.nviews - 1)
+    g = dataclasses.replace(geom, pi_window=True,
+                            norm=np.full(geom.nviews, abs(dlam) / (2 * math.pi * geom.D), np.float32))
+    return backproject(gF.to(dtype), g, mode=_lib.MODE_KATSEVICH)
+
+
 def phantom(vol_xyz, params: np.ndarray, device="cuda", out: torch.Tensor | None = None) -> torch.Tensor:
     """Voxelise an ellipsoid phantom (n x 16 parameter rows) on the GPU."""
     nx, ny, nz = (int(v) for v in vol_xyz)

@@ -180,6 +180,18 @@ int fcb_fdk_filter_device(const float* in, void* out, int outType, int nviews, i
                           float D, const float* zOrigin, int cosineWeight, int window,
                           void* stream);
 
+/* Katsevich filtering of helical projections (no counterpart in the reference, whose
+ * Katsevich backprojection, coneBeamGPU.cu:258-338, expects pre-filtered data): derivative
+ * at fixed ray direction, length correction, rebinning onto nkappa kappa-lines (<= 1: 2H),
+ * Hilbert transform along u, backward rebinning (Noo, Pack & Heuscher 2003, flat detector
+ * through the axis).  in/out: float [nviews][H][W] device, uniformly spaced host angles,
+ * pitch = source rise per turn (voxels).  Backprojecting the output with
+ * FCB_MODE_KATSEVICH, piWindow = 1 and norm = (angle step) / (2 pi D) reconstructs.
+ * Synchronous (its scratch is freed before it returns). */
+int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, int W,
+                                const float* angles, float D, float pw, float pitch, int nkappa,
+                                void* stream);
+
 /* Ellipsoid phantom voxelisation: vol[z][y][x] = sum of densities of ellipsoids
  * containing the voxel centre (g - volDim/2).  params: n x 16 doubles (host):
  * centre(3), semi-axes(3), row-major rotation R (9, body = R^T (p - c)), density. */
