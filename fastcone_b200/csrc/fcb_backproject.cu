@@ -555,6 +555,16 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
     return set_error(FCB_ERR_INVALID, "unknown projection storage type");
   auto* pl = new fcb_bp_plan();
   pl->maxv = std::max(1, std::min(FDK_MAXV, maxViewsPerLaunch));
+  // tuning knobs: z-voxels per thread (16/32/64) and the shared-memory budget per CTA
+  if (const char* e = getenv("FCB_FDK_NZ")) {
+    const int nz = atoi(e);
+    if (nz == 16 || nz == 32 || nz == 64) pl->nz_tile = nz;
+  }
+  // only the FP32 pair path is instantiated for depths other than 32
+  const char* sc = getenv("FCB_FDK_SCALAR");
+  if (projType != FCB_F32 || (sc && sc[0] == '1')) pl->nz_tile = 32;
+  int smem_budget = 64 * 1024;
+  if (const char* e = getenv("FCB_FDK_SMEM_KB")) smem_budget = std::max(8, std::min(200, atoi(e))) * 1024;
   int rc = make_problem(g, &pl->pb);
   if (rc) { delete pl; return rc; }
   Problem& pb = pl->pb;
@@ -634,7 +644,7 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
     } else {
       const size_t es = dtype_size(projType);
       const size_t stage_bytes = (((size_t)pl->BW * pl->BH * es) + 127) & ~(size_t)127;
-      int st = (int)((100 * 1024) / stage_bytes);
+      int st = (int)(smem_budget / stage_bytes);
       pl->stages = std::max(2, std::min(8, st));
       for (FdkParams& P : pl->fdk) {
         P.BW = pl->BW; P.BH = pl->BH; P.stages = pl->stages;
@@ -709,6 +719,12 @@ int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* v
     if (pl->ptype == FCB_F32 && scalar) {
       if (piw) FCB_TRY((launch_fdk<float, 32, true, false>(pl, map, chunk, st)));
       else FCB_TRY((launch_fdk<float, 32, false, false>(pl, map, chunk, st)));
+    } else if (pl->ptype == FCB_F32 && pl->nz_tile == 16) {
+      if (piw) FCB_TRY((launch_fdk<float, 16, true, true>(pl, map, chunk, st)));
+      else FCB_TRY((launch_fdk<float, 16, false, true>(pl, map, chunk, st)));
+    } else if (pl->ptype == FCB_F32 && pl->nz_tile == 64) {
+      if (piw) FCB_TRY((launch_fdk<float, 64, true, true>(pl, map, chunk, st)));
+      else FCB_TRY((launch_fdk<float, 64, false, true>(pl, map, chunk, st)));
     } else if (pl->ptype == FCB_F32) {
       if (piw) FCB_TRY((launch_fdk<float, 32, true, true>(pl, map, chunk, st)));
       else FCB_TRY((launch_fdk<float, 32, false, true>(pl, map, chunk, st)));
