@@ -42,6 +42,7 @@ EXPORTED_SYMBOLS = [
     "fcb_bp_plan_create", "fcb_bp_plan_execute", "fcb_bp_plan_info", "fcb_bp_plan_destroy",
     "fcb_sync_status", "fcb_fdk_filter_device", "fcb_phantom_device",
     "fcb_backproject_device_noalloc", "fcb_katsevich_filter_device",
+    "fcb_conv3d16_device", "fcb_conv3d16_wgrad_device",
 ]
 
 
@@ -107,6 +108,10 @@ def lib():
                                                 ctypes.c_int, ctypes.c_float, c_float_p,
                                                 ctypes.c_int, ctypes.c_int, vp]
             L.fcb_phantom_device.argtypes = [vp, c_int_p, c_double_p, ctypes.c_int, vp]
+            L.fcb_conv3d16_device.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_int, vp]
+            L.fcb_conv3d16_wgrad_device.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,
+                                                    ctypes.c_int, vp]
             L.fcb_katsevich_filter_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                       c_float_p, ctypes.c_float, ctypes.c_float,
                                                       ctypes.c_float, ctypes.c_int, vp]

@@ -23,6 +23,7 @@ SOURCES = [
     "fcb_project.cu",
     "fcb_filter.cu",
     "fcb_katsevich.cu",
+    "fcb_conv.cu",
     "fcb_capi.cpp",
 ]
 

@@ -285,43 +285,24 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
     else acc[k] = 0.0f;
   }
 
-  // Per-view geometry of this thread's column, computed one view ahead so its parameter
-  // loads and reciprocal overlap the previous view's interpolation work.
-  struct ColGeo {
-    float wabs, habs, dh, wt, wc, hc;
-  };
-  auto col_geo = [&](const FdkView& V) {
-    ColGeo c;
-    const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
-    const float U = __frcp_rn(den);
-    c.wabs = fmaf(fmaf(V.a0, x, V.a1 * y), U, V.wc);
-    c.habs = fmaf(U, fmaf(P.hb, zf, V.e), V.hc);
-    c.dh = U * P.hb;
-    float wt = V.wt;
-    if (P.wexp >= 1) wt *= U;
-    if (P.wexp >= 2) wt *= U;
-    c.wt = wt;
-    c.wc = V.wc;
-    c.hc = V.hc;
-    return c;
-  };
-  ColGeo nxt = col_geo(P.v[0]);
-
   for (int v = 0; v < P.nviews; v++) {
     const int s = v % P.stages;
-    const ColGeo cur = nxt;
-    if (v + 1 < P.nviews) nxt = col_geo(P.v[v + 1]);
     if (!dev::mbar_wait(&full[s], (v / P.stages) & 1)) {
       dev::record_status(P.status, DEV_TIMEOUT);
       return;
     }
+    const FdkView& V = P.v[v];
     const int2 org = origin[s];
 
-    const float wabs = cur.wabs;
+    const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
+    const float U = __frcp_rn(den);
+    const float wabs = fmaf(fmaf(V.a0, x, V.a1 * y), U, V.wc);
     float wl = wabs - (float)org.x;
-    float h0 = cur.habs - (float)org.y;
-    float dh = cur.dh;
-    float wt = cur.wt;
+    float h0 = fmaf(U, fmaf(P.hb, zf, V.e), V.hc) - (float)org.y;
+    float dh = U * P.hb;
+    float wt = V.wt;
+    if (P.wexp >= 1) wt *= U;
+    if (P.wexp >= 2) wt *= U;
 
     // memory safety: every tap must stay inside the staged box
     int iw = __float2int_rd(wl);
@@ -335,10 +316,10 @@ __global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_const
 
     float lo = -3.0e38f, hi = 3.0e38f;  // Tam-Danielsson bounds (local h)
     if constexpr (PIW) {
-      const float u = (wabs - cur.wc) * P.td_sign / P.td_r;
+      const float u = (wabs - V.wc) * P.td_sign / P.td_r;
       const float q = P.td_a * (1.0f + u * u);
       const float at = atanf(u);
-      const float hsrc = cur.hc - (float)org.y;
+      const float hsrc = V.hc - (float)org.y;
       hi = hsrc + q * (1.5707963267948966f - at);
       lo = hsrc - q * (1.5707963267948966f + at);
     }

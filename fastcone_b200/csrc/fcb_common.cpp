@@ -212,6 +212,30 @@ static EncodeTiledFn get_encode()
   return fn;
 }
 
+int encode_tmap(CUtensorMap* map, CUtensorMapDataType dtype, int rank, void* base,
+                const uint64_t* dims, const uint64_t* strides_bytes, const uint32_t* box)
+{
+  EncodeTiledFn enc = get_encode();
+  if (!enc) return set_error(FCB_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+  cuuint64_t d[5], st[4];
+  cuuint32_t b[5], e[5];
+  for (int i = 0; i < rank; i++) {
+    d[i] = dims[i];
+    b[i] = box[i];
+    e[i] = 1;
+    if (i + 1 < rank) st[i] = strides_bytes[i];
+  }
+  CUresult r = enc(map, dtype, rank, base, d, st, b, e, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    char buf[96];
+    snprintf(buf, sizeof buf, "cuTensorMapEncodeTiled failed (%d), rank %d", (int)r, rank);
+    return set_error(FCB_ERR_CUDA, buf);
+  }
+  return FCB_OK;
+}
+
 int encode_tmap_3d(CUtensorMap* map, CUtensorMapDataType dtype, void* base, uint64_t d0,
                    uint64_t d1, uint64_t d2, uint64_t stride1_bytes, uint64_t stride2_bytes,
                    uint32_t b0, uint32_t b1, uint32_t b2)

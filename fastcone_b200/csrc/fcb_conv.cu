@@ -1,0 +1,347 @@
+// fcb_conv.cu -- 3x3x3 convolutions (16 -> 16 channels, stride 1, zero padding 1) for the
+// learned reconstruction's CNN, on the 5th-generation tensor cores (sm_100a tcgen05).
+//
+// Activations are channels-last BF16, [z][y][x][16] (32 bytes per voxel); weights BF16
+// [27 taps][16 out][16 in]; accumulation FP32 in tensor memory.  Implicit GEMM: a CTA owns
+// 128 consecutive x-voxels of one (y, z) row -> D[128 x 16] = sum over 27 taps of
+// A_tap[128 x 16 in] * B_tap[16 in x 16 out].  The A operands of the three x-shifts of a tap
+// row are the same TMA-loaded row of 130 voxels addressed 16 bytes apart, so 9 row loads
+// (x 2 channel halves) feed all 27 MMAs.  Out-of-volume rows/voxels arrive as zeros from the
+// TMA unit, which is the zero padding.  One elected thread issues the 27
+// tcgen05.mma.cta_group::1.kind::f16 (M=128, N=16, K=16) and commits to an mbarrier; four
+// warps read their TMEM lane quadrant back (tcgen05.ld 32x32b.x16), add the bias, apply
+// ReLU and store.
+//
+// The same kernel computes the input gradient (transposed, tap-flipped weights, prepared by
+// the caller).  The weight gradient, a 6912-entry reduction over all voxels, runs on the
+// CUDA cores (fcb_conv3d16_wgrad_device).
+#include <string.h>
+
+#include <algorithm>
+
+#include "fcb_internal.h"
+
+namespace fcb {
+namespace tc {
+
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols)
+{
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dev::smem_u32(dst)),
+               "r"(ncols)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_relinquish()
+{
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// D(tmem) (+)= A(smem desc) * B(smem desc), BF16 inputs, FP32 accumulator.
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.u32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* bar)
+{
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   dev::smem_u32(bar))
+               : "memory");
+}
+// 32 lanes x 16 consecutive 32-bit columns: thread i of the warp gets row (lane base + i).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
+{
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle ("interleaved" core matrices of 8
+// rows x 16 bytes): start address, leading byte offset (between the two 8-element K
+// halves), stride byte offset (between 8-row groups), descriptor version 1 (sm_100).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor, kind::f16: FP32 accumulator, BF16 A and B, both K-major, N, M.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
+{
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
+                                            int c2, int c3)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dev::smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(dev::smem_u32(bar))
+      : "memory");
+}
+
+}  // namespace tc
+
+constexpr int CV_TILE = 128;                  // voxels per CTA tile (MMA M)
+constexpr int CV_ROW = CV_TILE + 2;           // staged voxels per tap row (x halo)
+constexpr int CV_BOX_BYTES = CV_ROW * 16;     // one channel half of one tap row
+constexpr int CV_RB = 2176;                   // CV_BOX_BYTES rounded up to 128 B
+constexpr int CV_A_BYTES = 9 * 2 * CV_RB;     // 39168
+constexpr int CV_W_BYTES = 27 * 512;          // 13824
+constexpr int CV_SMEM = CV_A_BYTES + CV_W_BYTES + 64 + 32 + 16;
+
+struct ConvParams {
+  const __nv_bfloat16* w;  // [27][16 out][16 in]
+  const float* bias;       // [16] or null
+  void* out;               // [z][y][x][16], bf16 or f32
+  int out_f32;
+  int relu;
+  int nx, ny, nz;
+  int tiles_x;
+  int* status;
+};
+
+__global__ void __launch_bounds__(128) conv3d16_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                       const __grid_constant__ ConvParams P)
+{
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* A = smem;
+  unsigned char* Wsm = smem + CV_A_BYTES;
+  float* bias = reinterpret_cast<float*>(Wsm + CV_W_BYTES);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(Wsm + CV_W_BYTES + 64);  // [0] tma, [1] mma
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(Wsm + CV_W_BYTES + 64 + 16);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tile = blockIdx.x;
+  const int x0 = (tile % P.tiles_x) * CV_TILE;
+  const int yz = tile / P.tiles_x;
+  const int y = yz % P.ny, z = yz / P.ny;
+
+  if (threadIdx.x == 0) {
+    dev::mbar_init(&bars[0], 1);
+    dev::mbar_init(&bars[1], 1);
+    dev::fence_mbar_init();
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, 32);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before();
+  __syncthreads();
+
+  if (threadIdx.x == 0) {
+    dev::tma_prefetch(&xmap);
+    dev::mbar_arrive_expect_tx(&bars[0], 18u * CV_BOX_BYTES);
+    for (int r = 0; r < 9; r++) {
+      const int dz = r / 3, dy = r % 3;
+      for (int kh = 0; kh < 2; kh++)
+        tc::tma_load_4d(A + (r * 2 + kh) * CV_RB, &xmap, &bars[0], kh * 8, x0 - 1, y + dy - 1, z + dz - 1);
+    }
+  }
+  // weights -> core-matrix layout: tap t, K half kh, row n (out channel): 16 bytes of 8 in-channels
+  const uint4* wg = reinterpret_cast<const uint4*>(P.w);
+  for (int i = threadIdx.x; i < 27 * 16 * 2; i += blockDim.x) {
+    const int t = i / 32, n = (i / 2) % 16, kh = i % 2;
+    reinterpret_cast<uint4*>(Wsm + t * 512 + kh * 256 + n * 16)[0] = wg[(t * 16 + n) * 2 + kh];
+  }
+  if (threadIdx.x < 16) bias[threadIdx.x] = P.bias ? P.bias[threadIdx.x] : 0.0f;
+  // generic-proxy shared stores -> visible to the tensor core's async-proxy reads
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t taddr = *tslot;
+
+  bool ok = true;
+  if (threadIdx.x == 0) {
+    ok = dev::mbar_wait(&bars[0], 0);
+    if (ok) {
+      tc::fence_after();
+      const uint32_t abase = dev::smem_u32(A), wbase = dev::smem_u32(Wsm);
+      constexpr uint32_t IDESC = tc::idesc_bf16(CV_TILE, 16);
+      for (int t = 0; t < 27; t++) {
+        const int r = t / 3, dx = t % 3;
+        const uint64_t ad = tc::smem_desc(abase + r * 2 * CV_RB + dx * 16, CV_RB, 128);
+        const uint64_t bd = tc::smem_desc(wbase + t * 512, 256, 128);
+        tc::mma_bf16(taddr, ad, bd, IDESC, t > 0 ? 1u : 0u);
+      }
+      tc::mma_commit(&bars[1]);
+    } else {
+      dev::record_status(P.status, DEV_TIMEOUT);
+      dev::mbar_wait(&bars[0], 0, 100000000ull);  // let in-flight copies land before exit
+    }
+  }
+  // every thread waits (bounded) for the MMA commit; the result must be warp-uniform
+  // because tcgen05.ld is a warp-collective instruction
+  const bool done = __all_sync(0xffffffffu, dev::mbar_wait(&bars[1], 0) ? 1 : 0) != 0;
+  tc::fence_after();
+  if (done) {
+    uint32_t r[16];
+    tc::tmem_ld16(taddr + ((uint32_t)(warp * 32) << 16), r);
+    const int row = warp * 32 + lane;
+    const int xv = x0 + row;
+    if (xv < P.nx) {
+      float v[16];
+#pragma unroll
+      for (int c = 0; c < 16; c++) {
+        v[c] = __uint_as_float(r[c]) + bias[c];
+        if (P.relu) v[c] = fmaxf(v[c], 0.0f);
+      }
+      const size_t vox = ((size_t)z * P.ny + y) * P.nx + xv;
+      if (P.out_f32) {
+        float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + vox * 16);
+#pragma unroll
+        for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+      } else {
+        uint32_t pk[8];
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+          pk[q] = *reinterpret_cast<uint32_t*>(&b);
+        }
+        uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(P.out) + vox * 16);
+        o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+      }
+    }
+  } else if (threadIdx.x == 32) {
+    dev::record_status(P.status, DEV_TIMEOUT);
+  }
+  // MMAs must have finished before the accumulator columns are released
+  if (!done && threadIdx.x == 0 && ok) dev::mbar_wait(&bars[1], 0, 100000000ull);
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(taddr, 32);
+}
+
+// Weight gradient on the CUDA cores: dW[t][co][ci] += sum_v dY[v][co] * X[v + off(t)][ci].
+// Thread (co, ci) slides along a row of 128 voxels keeping the three x-neighbours of each of
+// the 9 tap rows in registers; CTAs loop over tiles and add their 27 partial sums once.
+struct WgradParams {
+  const __nv_bfloat16* x;
+  const void* dy;
+  int dy_f32;
+  float* dw;
+  int nx, ny, nz, tiles_x, ntiles;
+};
+
+__device__ __forceinline__ float ld_act(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+
+constexpr int WG_TILE = 64;
+__global__ void __launch_bounds__(256) conv3d16_wgrad_kernel(const WgradParams P)
+{
+  __shared__ float xs[9][WG_TILE + 2][17];
+  __shared__ float ds[WG_TILE][17];
+  const int co = threadIdx.x >> 4, ci = threadIdx.x & 15;
+  float acc[27];
+#pragma unroll
+  for (int t = 0; t < 27; t++) acc[t] = 0.0f;
+  for (int tile = blockIdx.x; tile < P.ntiles; tile += gridDim.x) {
+    const int x0 = (tile % P.tiles_x) * WG_TILE;
+    const int yz = tile / P.tiles_x;
+    const int y = yz % P.ny, z = yz / P.ny;
+    __syncthreads();
+    for (int i = threadIdx.x; i < 9 * (WG_TILE + 2) * 16; i += blockDim.x) {
+      const int c = i & 15, xr = (i >> 4) % (WG_TILE + 2), r = i / (16 * (WG_TILE + 2));
+      const int zz = z + r / 3 - 1, yy = y + r % 3 - 1, xx = x0 + xr - 1;
+      float v = 0.0f;
+      if (zz >= 0 && zz < P.nz && yy >= 0 && yy < P.ny && xx >= 0 && xx < P.nx)
+        v = ld_act(P.x + (((size_t)zz * P.ny + yy) * P.nx + xx) * 16 + c);
+      xs[r][xr][c] = v;
+    }
+    for (int i = threadIdx.x; i < WG_TILE * 16; i += blockDim.x) {
+      const int c = i & 15, xr = i >> 4, xx = x0 + xr;
+      float v = 0.0f;
+      if (xx < P.nx) {
+        const size_t o = (((size_t)z * P.ny + y) * P.nx + xx) * 16 + c;
+        v = P.dy_f32 ? reinterpret_cast<const float*>(P.dy)[o]
+                     : ld_act(reinterpret_cast<const __nv_bfloat16*>(P.dy) + o);
+      }
+      ds[xr][c] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+      float a = xs[r][0][ci], b = xs[r][1][ci];
+      for (int v = 0; v < WG_TILE; v++) {
+        const float c = xs[r][v + 2][ci];
+        const float g = ds[v][co];
+        acc[r * 3 + 0] = fmaf(g, a, acc[r * 3 + 0]);
+        acc[r * 3 + 1] = fmaf(g, b, acc[r * 3 + 1]);
+        acc[r * 3 + 2] = fmaf(g, c, acc[r * 3 + 2]);
+        a = b;
+        b = c;
+      }
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < 27; t++) atomicAdd(P.dw + (t * 16 + co) * 16 + ci, acc[t]);
+}
+
+}  // namespace fcb
+
+using namespace fcb;
+
+extern "C" int fcb_conv3d16_device(const void* x, const void* w, const float* bias, void* y, int yType,
+                                   int nx, int ny, int nz, int relu, void* stream)
+{
+  if (!x || !w || !y || nx <= 0 || ny <= 0 || nz <= 0 || (yType != FCB_F32 && yType != FCB_BF16))
+    return set_error(FCB_ERR_INVALID, "bad conv3d arguments");
+  if (((uintptr_t)x & 15) || ((uintptr_t)w & 15) || ((uintptr_t)y & 15))
+    return set_error(FCB_ERR_INVALID, "conv3d buffers must be 16-byte aligned");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  CUtensorMap map;
+  const uint64_t dims[4] = {16, (uint64_t)nx, (uint64_t)ny, (uint64_t)nz};
+  const uint64_t strides[3] = {32, 32ull * nx, 32ull * nx * ny};
+  const uint32_t box[4] = {8, CV_ROW, 1, 1};
+  FCB_TRY(encode_tmap(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box));
+  int* status = nullptr;
+  FCB_TRY(device_status_ptr(&status));
+  ConvParams P;
+  P.w = reinterpret_cast<const __nv_bfloat16*>(w);
+  P.bias = bias;
+  P.out = y;
+  P.out_f32 = yType == FCB_F32;
+  P.relu = relu;
+  P.nx = nx; P.ny = ny; P.nz = nz;
+  P.tiles_x = (nx + CV_TILE - 1) / CV_TILE;
+  P.status = status;
+  FCB_CUDA_TRY(cudaFuncSetAttribute(conv3d16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM));
+  const long long tiles = (long long)P.tiles_x * ny * nz;
+  conv3d16_kernel<<<(unsigned)tiles, 128, CV_SMEM, st>>>(map, P);
+  FCB_CUDA_TRY(cudaGetLastError());
+  return ok();
+}
+
+extern "C" int fcb_conv3d16_wgrad_device(const void* x, const void* dy, int dyType, float* dw, int nx, int ny,
+                                         int nz, void* stream)
+{
+  if (!x || !dy || !dw || nx <= 0 || ny <= 0 || nz <= 0 || (dyType != FCB_F32 && dyType != FCB_BF16))
+    return set_error(FCB_ERR_INVALID, "bad conv3d wgrad arguments");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  WgradParams P;
+  P.x = reinterpret_cast<const __nv_bfloat16*>(x);
+  P.dy = dy;
+  P.dy_f32 = dyType == FCB_F32;
+  P.dw = dw;
+  P.nx = nx; P.ny = ny; P.nz = nz;
+  P.tiles_x = (nx + WG_TILE - 1) / WG_TILE;
+  P.ntiles = P.tiles_x * ny * nz;
+  const int grid = std::min(P.ntiles, 148 * 4);
+  conv3d16_wgrad_kernel<<<grid, 256, 0, st>>>(P);
+  FCB_CUDA_TRY(cudaGetLastError());
+  return ok();
+}

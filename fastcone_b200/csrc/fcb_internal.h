@@ -74,6 +74,10 @@ int encode_tmap_3d(CUtensorMap* map, CUtensorMapDataType dtype, void* base, uint
                    uint64_t d1, uint64_t d2, uint64_t stride1_bytes, uint64_t stride2_bytes,
                    uint32_t b0, uint32_t b1, uint32_t b2);
 
+// Tiled tensor map of any rank (1..5), no swizzle, zero fill out of bounds.
+int encode_tmap(CUtensorMap* map, CUtensorMapDataType dtype, int rank, void* base,
+                const uint64_t* dims, const uint64_t* strides_bytes, const uint32_t* box);
+
 inline int dtype_size(int t) { return t == FCB_F32 ? 4 : 2; }
 
 }  // namespace fcb

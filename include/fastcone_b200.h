@@ -192,6 +192,20 @@ int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, 
                                 const float* angles, float D, float pw, float pitch, int nkappa,
                                 void* stream);
 
+/* 3x3x3 convolution, 16 -> 16 channels, stride 1, zero padding 1, on the tcgen05 tensor
+ * cores (BF16 inputs, FP32 accumulation).  x: BF16 [nz][ny][nx][16] (channels last), w: BF16
+ * [27 taps (dz,dy,dx) z-major][16 out][16 in], bias: 16 floats or NULL, y: [nz][ny][nx][16] of
+ * yType (FCB_F32 / FCB_BF16), ReLU applied when relu != 0.  Buffers 16-byte aligned.  The
+ * input gradient is the same call with dY as x and w'[t][ci][co] = w[26 - t][co][ci].
+ * No counterpart in the reference (the learned reconstruction is new). */
+int fcb_conv3d16_device(const void* x, const void* w, const float* bias, void* y, int yType, int nx,
+                        int ny, int nz, int relu, void* stream);
+
+/* Weight gradient of fcb_conv3d16_device: dw[t][co][ci] += sum_v dy[v][co] x[v + tap t][ci]
+ * (FP32, accumulated); dy of dyType (FCB_F32 / FCB_BF16), x BF16. */
+int fcb_conv3d16_wgrad_device(const void* x, const void* dy, int dyType, float* dw, int nx, int ny,
+                              int nz, void* stream);
+
 /* Ellipsoid phantom voxelisation: vol[z][y][x] = sum of densities of ellipsoids
  * containing the voxel centre (g - volDim/2).  params: n x 16 doubles (host):
  * centre(3), semi-axes(3), row-major rotation R (9, body = R^T (p - c)), density. */

@@ -1,0 +1,69 @@
+"""tcgen05 3x3x3 convolution vs torch.nn.functional.conv3d in FP32 on the same BF16-rounded
+inputs (FP32 accumulation both sides: rel-L2 <= 1e-5), input and weight gradients vs torch
+autograd (rel-L2 <= 1e-2 -- the gradient flowing in is rounded to BF16 by design)."""
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref(x_cl, w, b, relu):
+    import torch
+    import torch.nn.functional as F
+
+    x = x_cl.float().permute(3, 0, 1, 2).unsqueeze(0)          # [1, C, z, y, x]
+    y = F.conv3d(x, w.float(), b.float(), padding=1)
+    if relu:
+        y = torch.relu(y)
+    return y.squeeze(0).permute(1, 2, 3, 0)                      # [z, y, x, C]
+
+
+def _rel(a, b):
+    return float((a.float() - b.float()).norm() / b.float().norm())
+
+
+@pytest.mark.parametrize("shape", [(20, 17, 130), (8, 9, 256), (3, 5, 7)])
+@pytest.mark.parametrize("relu", [False, True])
+def test_conv_forward_vs_torch(shape, relu):
+    import torch
+
+    from fastcone_b200 import nn
+
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
+    w = (torch.randn(16, 16, 3, 3, 3, device="cuda", generator=g) * 0.1).to(torch.bfloat16).float()
+    b = torch.randn(16, device="cuda", generator=g)
+    y = nn.conv3d16(x, nn.to_kernel_weights(w).to(torch.bfloat16).contiguous(), b, relu=relu,
+                    out_dtype=torch.float32)
+    ref = _ref(x, w, b, relu)
+    assert _rel(y, ref) < 1e-5, _rel(y, ref)
+
+
+def test_conv_gradients_vs_torch():
+    import torch
+    import torch.nn.functional as F
+
+    from fastcone_b200 import nn
+
+    g = torch.Generator(device="cuda").manual_seed(1)
+    shape = (12, 10, 140)
+    x = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
+    w = (torch.randn(16, 16, 3, 3, 3, device="cuda", generator=g) * 0.1).to(torch.bfloat16).float()
+    b = torch.randn(16, device="cuda", generator=g) * 0.1
+    gy = torch.randn(shape + (16,), device="cuda", generator=g)
+
+    # ours: gradients through the custom function
+    xin = x.clone().requires_grad_(True)
+    w2 = w.clone().requires_grad_(True)
+    b2 = b.clone().requires_grad_(True)
+    y2 = nn.Conv3d16Function.apply(xin, w2, b2, True)
+    (y2.float() * gy).sum().backward()
+    # reference in FP32
+    xr = x.float().permute(3, 0, 1, 2).unsqueeze(0).clone().requires_grad_(True)
+    wr = w.clone().requires_grad_(True)
+    br = b.clone().requires_grad_(True)
+    yr = torch.relu(F.conv3d(xr, wr, br, padding=1)).squeeze(0).permute(1, 2, 3, 0)
+    (yr * gy).sum().backward()
+    gx_ref = xr.grad.squeeze(0).permute(1, 2, 3, 0)
+    assert _rel(xin.grad, gx_ref) < 1e-2
+    assert _rel(w2.grad, wr.grad) < 1e-2
+    assert _rel(b2.grad, br.grad) < 1e-2
