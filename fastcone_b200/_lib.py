@@ -43,6 +43,7 @@ EXPORTED_SYMBOLS = [
     "fcb_sync_status", "fcb_fdk_filter_device", "fcb_phantom_device",
     "fcb_backproject_device_noalloc", "fcb_katsevich_filter_device",
     "fcb_conv3d16_device", "fcb_conv3d16_wgrad_device",
+    "fcb_proj_plan_create", "fcb_proj_plan_execute", "fcb_proj_plan_destroy",
 ]
 
 
@@ -108,6 +109,9 @@ def lib():
                                                 ctypes.c_int, ctypes.c_float, c_float_p,
                                                 ctypes.c_int, ctypes.c_int, vp]
             L.fcb_phantom_device.argtypes = [vp, c_int_p, c_double_p, ctypes.c_int, vp]
+            L.fcb_proj_plan_create.argtypes = [gp, ctypes.c_int, ctypes.POINTER(vp)]
+            L.fcb_proj_plan_execute.argtypes = [vp, vp, vp, ctypes.c_int, vp]
+            L.fcb_proj_plan_destroy.argtypes = [vp]
             L.fcb_conv3d16_device.argtypes = [vp, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                               ctypes.c_int, ctypes.c_int, vp]
             L.fcb_conv3d16_wgrad_device.argtypes = [vp, vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int,

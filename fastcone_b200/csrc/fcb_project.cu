@@ -308,6 +308,100 @@ int project_launch(const Problem& pb, int method, const float* vol, float* proj,
 
 using namespace fcb;
 
+// Reusable projector: per-view parameters digested once; for the texture method a 3-D CUDA
+// array and its texture object live with the plan, so execute() only copies the volume in
+// (stream-ordered) and launches -- no allocation, no synchronisation.
+struct fcb_proj_plan {
+  Problem pb;
+  int method = FCB_PROJ_EXPLICIT;
+  int nx = 0, ny = 0, nz = 0;
+  cudaArray_t arr = nullptr;
+  cudaTextureObject_t tex = 0;
+  std::vector<PjParams> chunks;
+};
+
+extern "C" int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_plan** out)
+{
+  if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
+  *out = nullptr;
+  if (method != FCB_PROJ_TEXTURE && method != FCB_PROJ_EXPLICIT)
+    return set_error(FCB_ERR_INVALID, "unknown projector method");
+  auto* pl = new fcb_proj_plan();
+  int rc = make_problem(g, &pl->pb);
+  if (rc) { delete pl; return rc; }
+  const Problem& pb = pl->pb;
+  pl->method = method;
+  pl->nx = pb.volEnd[0] - pb.volStart[0];
+  pl->ny = pb.volEnd[1] - pb.volStart[1];
+  pl->nz = pb.volEnd[2] - pb.volStart[2];
+  if (method == FCB_PROJ_TEXTURE) {
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+    cudaError_t e = cudaMalloc3DArray(&pl->arr, &cd, make_cudaExtent(pl->nx, pl->ny, pl->nz));
+    if (e != cudaSuccess) { delete pl; return set_error(FCB_ERR_NOMEM, cudaGetErrorString(e)); }
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = pl->arr;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeElementType;
+    e = cudaCreateTextureObject(&pl->tex, &rd, &td, nullptr);
+    if (e != cudaSuccess) { cudaFreeArray(pl->arr); delete pl; return set_error(FCB_ERR_CUDA, cudaGetErrorString(e)); }
+  }
+  for (int v0 = 0; v0 < pb.nviews; v0 += PJ_MAXV) {
+    PjParams P;
+    memset(&P, 0, sizeof(P));
+    P.tex = pl->tex;
+    P.nx = pl->nx; P.ny = pl->ny; P.nz = pl->nz;
+    P.WH0 = pb.projWHSize[0]; P.WH1 = pb.projWHSize[1];
+    fill_pj_views(pb, v0, std::min(PJ_MAXV, pb.nviews - v0), &P);
+    pl->chunks.push_back(P);
+  }
+  *out = pl;
+  return ok();
+}
+
+// proj += norm * A vol (adjoint == 0), or vol += A^T (norm * proj) (adjoint != 0, explicit only).
+extern "C" int fcb_proj_plan_execute(fcb_proj_plan* pl, const float* volume, float* proj, int adjoint,
+                                     void* stream)
+{
+  if (!pl || !volume || !proj) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (adjoint && pl->method != FCB_PROJ_EXPLICIT)
+    return set_error(FCB_ERR_INVALID, "the adjoint belongs to the explicit projector");
+  if (pl->method == FCB_PROJ_TEXTURE) {
+    cudaMemcpy3DParms cp;
+    memset(&cp, 0, sizeof(cp));
+    cp.srcPtr = make_cudaPitchedPtr(const_cast<float*>(volume), pl->nx * sizeof(float), pl->nx, pl->ny);
+    cp.dstArray = pl->arr;
+    cp.extent = make_cudaExtent(pl->nx, pl->ny, pl->nz);
+    cp.kind = cudaMemcpyDeviceToDevice;
+    FCB_CUDA_TRY(cudaMemcpy3DAsync(&cp, st));
+  }
+  for (PjParams& P : pl->chunks) {
+    P.vol = volume;
+    P.proj = proj;
+    dim3 grid((P.WH0 + 15) / 16, (P.WH1 + 15) / 16, P.nviews);
+    if (adjoint) project_adjoint_kernel<<<grid, 256, 0, st>>>(P, const_cast<float*>(volume));
+    else if (pl->method == FCB_PROJ_TEXTURE) project_tex_kernel<<<grid, 256, 0, st>>>(P);
+    else project_explicit_kernel<<<grid, 256, 0, st>>>(P);
+    FCB_CUDA_TRY(cudaGetLastError());
+  }
+  return ok();
+}
+
+extern "C" int fcb_proj_plan_destroy(fcb_proj_plan* pl)
+{
+  if (pl) {
+    if (pl->tex) cudaDestroyTextureObject(pl->tex);
+    if (pl->arr) cudaFreeArray(pl->arr);
+    delete pl;
+  }
+  return ok();
+}
+
 extern "C" int fcb_project_device(const fcb_geometry* g, int method, const float* volume,
                                   float* proj, void* stream)
 {

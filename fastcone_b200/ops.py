@@ -101,6 +101,44 @@ def project(vol: torch.Tensor, geom: ConeGeometry, method: int = _lib.PROJ_EXPLI
     return proj
 
 
+class ProjectPlan:
+    """Reusable projector (and, for the explicit method, its exact adjoint); calls are
+    stream-ordered and allocate nothing."""
+
+    def __init__(self, geom: ConeGeometry, method: int = _lib.PROJ_EXPLICIT):
+        self.geom = geom
+        self.method = method
+        self._h = ctypes.c_void_p()
+        g = geom.struct()
+        check(lib().fcb_proj_plan_create(ctypes.byref(g), method, ctypes.byref(self._h)))
+
+    def __call__(self, vol: torch.Tensor, proj: torch.Tensor | None = None) -> torch.Tensor:
+        if tuple(vol.shape) != self.geom.vol_shape:
+            raise ValueError("volume shape does not match the plan")
+        if proj is None:
+            proj = torch.zeros(self.geom.proj_shape, device=vol.device, dtype=torch.float32)
+        check(lib().fcb_proj_plan_execute(self._h, _dev(vol, "vol", torch.float32), _dev(proj, "proj", torch.float32),
+                                          0, _stream()))
+        return proj
+
+    def adjoint(self, proj: torch.Tensor, vol: torch.Tensor | None = None) -> torch.Tensor:
+        if tuple(proj.shape) != self.geom.proj_shape:
+            raise ValueError("projection shape does not match the plan")
+        if vol is None:
+            vol = torch.zeros(self.geom.vol_shape, device=proj.device, dtype=torch.float32)
+        check(lib().fcb_proj_plan_execute(self._h, _dev(vol, "vol", torch.float32), _dev(proj, "proj", torch.float32),
+                                          1, _stream()))
+        return vol
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            try:
+                lib().fcb_proj_plan_destroy(self._h)
+            except Exception:
+                pass
+            self._h = ctypes.c_void_p()
+
+
 def project_adjoint(proj: torch.Tensor, geom: ConeGeometry, vol: torch.Tensor | None = None) -> torch.Tensor:
     """vol += A^T (norm * proj), the exact transpose of project(method=PROJ_EXPLICIT)."""
     if tuple(proj.shape) != geom.proj_shape:

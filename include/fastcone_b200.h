@@ -166,6 +166,17 @@ int fcb_bp_plan_destroy(fcb_bp_plan* plan);
 int fcb_backproject_device_noalloc(const fcb_geometry* g, int kernelMode, const void* proj,
                                    int projType, float* volume, void* stream);
 
+/* Reusable projector (per-view parameters digested once; the texture method keeps its 3-D
+ * CUDA array and texture object with the plan).  execute() is stream-ordered, allocates
+ * nothing and does not synchronise: adjoint == 0 adds norm * A volume into proj, adjoint != 0
+ * adds A^T (norm * proj) into volume (explicit method only).  A texture plan must not run
+ * on two streams at once (its array holds the volume being projected). */
+typedef struct fcb_proj_plan fcb_proj_plan;
+int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_plan** plan);
+int fcb_proj_plan_execute(fcb_proj_plan* plan, const float* volume, float* proj, int adjoint,
+                          void* stream);
+int fcb_proj_plan_destroy(fcb_proj_plan* plan);
+
 /* Waits for `stream` and returns FCB_ERR_TIMEOUT / FCB_ERR_RANGE if a kernel of this
  * library recorded a device-side failure since the previous check, else FCB_OK. */
 int fcb_sync_status(void* stream);
