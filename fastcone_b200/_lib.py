@@ -44,6 +44,7 @@ EXPORTED_SYMBOLS = [
     "fcb_backproject_device_noalloc", "fcb_katsevich_filter_device",
     "fcb_conv3d16_device", "fcb_conv3d16_wgrad_device",
     "fcb_proj_plan_create", "fcb_proj_plan_execute", "fcb_proj_plan_destroy",
+    "fcb_reference_windows",
 ]
 
 
@@ -64,6 +65,7 @@ class FcbGeometry(ctypes.Structure):
         ("misAlignments", c_float_p),
         ("helicalPitch", ctypes.c_float),
         ("piWindow", ctypes.c_int),
+        ("referenceWindows", ctypes.c_int),
     ]
 
 
@@ -119,6 +121,7 @@ def lib():
             L.fcb_katsevich_filter_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                       c_float_p, ctypes.c_float, ctypes.c_float,
                                                       ctypes.c_float, ctypes.c_int, vp]
+            L.fcb_reference_windows.argtypes = [gp] + [c_int_p] * 8
             _lib = L
     return _lib
 

@@ -19,6 +19,7 @@ OBJDIR = os.path.join(HERE, "_build")
 
 SOURCES = [
     "fcb_common.cpp",
+    "fcb_refgeom.cpp",
     "fcb_backproject.cu",
     "fcb_project.cu",
     "fcb_filter.cu",

@@ -208,8 +208,8 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
   return r;
 }
 
-template <typename T, int NZ, bool PIW, bool X2>
-__global__ void __launch_bounds__(FDK_THREADS) fdk_tma_kernel(const __grid_constant__ CUtensorMap tmap,
+template <typename T, int NZ, bool PIW, bool X2, int MINB = 1>
+__global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid_constant__ CUtensorMap tmap,
                                                               const __grid_constant__ FdkParams P)
 {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -425,6 +425,11 @@ struct GenParams {
   int wexp;
   int piwin;
   float td_a, td_r, td_sign, pw;
+  // reference-compatible windows (NULL: ideal operator).  win[tile * wviews + view] holds
+  // the first/last texel column and row of the sub-problem window, data-local; tiles are
+  // sv0 x sv1 x sv2 voxels from volStart, ntx x nty of them per z layer.
+  const int4* win;
+  int sv0, sv1, sv2, ntx, nty, wviews;
   GenView v[GEN_MAXV];
 };
 static_assert(sizeof(GenParams) < 32000, "kernel parameter space");
@@ -447,6 +452,11 @@ __global__ void __launch_bounds__(256) bp_generic_kernel(const __grid_constant__
   const int yi = (int)(r % P.ny), zi = (int)(r / P.ny);
   const float x = P.ox + xi, y = P.oy + yi, z = P.oz + zi;
   float acc = 0.0f;
+  const int4* wrow = nullptr;
+  if (P.win) {
+    const int tile = ((zi / P.sv2) * P.nty + yi / P.sv1) * P.ntx + xi / P.sv0;
+    wrow = P.win + (size_t)tile * P.wviews + P.view0;
+  }
   for (int v = 0; v < P.nviews; v++) {
     const GenView& V = P.v[v];
     const float uu = fmaf(V.m[0], x, fmaf(V.m[1], y, fmaf(V.m[2], z, V.m[3])));
@@ -457,6 +467,27 @@ __global__ void __launch_bounds__(256) bp_generic_kernel(const __grid_constant__
     float wt = V.wt;
     if (P.wexp >= 1) wt *= V.kappa * rs;
     if (P.wexp >= 2) wt *= V.kappa * rs;
+    if (wrow) {
+      // the reference's texture window: texel indices clamp to the window edge, texels
+      // outside the caller's data read zero (coneBeamGPU.cu:839-848, :1049-1088)
+      const int4 wb = wrow[v];
+      const float wc = fminf(fmaxf(wl, (float)wb.x - 2.0f), (float)wb.y + 2.0f);
+      const float hc = fminf(fmaxf(hl, (float)wb.z - 2.0f), (float)wb.w + 2.0f);
+      const float fw = floorf(wc), fh = floorf(hc);
+      const float a = wc - fw, b = hc - fh;
+      const int i0 = min(max((int)fw, wb.x), wb.y), i1 = min(max((int)fw + 1, wb.x), wb.y);
+      const int j0 = min(max((int)fh, wb.z), wb.w), j1 = min(max((int)fh + 1, wb.z), wb.w);
+      const size_t vb = (size_t)(P.view0 + v) * P.WH0 * P.WH1;
+      const bool ci0 = i0 >= 0 && i0 < P.WH0, ci1 = i1 >= 0 && i1 < P.WH0;
+      const bool cj0 = j0 >= 0 && j0 < P.WH1, cj1 = j1 >= 0 && j1 < P.WH1;
+      const float t00 = ci0 && cj0 ? gen_load(P.proj, P.ptype, vb + (size_t)j0 * P.WH0 + i0) : 0.f;
+      const float t10 = ci1 && cj0 ? gen_load(P.proj, P.ptype, vb + (size_t)j0 * P.WH0 + i1) : 0.f;
+      const float t01 = ci0 && cj1 ? gen_load(P.proj, P.ptype, vb + (size_t)j1 * P.WH0 + i0) : 0.f;
+      const float t11 = ci1 && cj1 ? gen_load(P.proj, P.ptype, vb + (size_t)j1 * P.WH0 + i1) : 0.f;
+      const float r0 = fmaf(a, t10 - t00, t00), r1 = fmaf(a, t11 - t01, t01);
+      acc = fmaf(wt, fmaf(b, r1 - r0, r0), acc);
+      continue;
+    }
     if (!(wl > -1.0f && wl < (float)P.WH0 && hl > -1.0f && hl < (float)P.WH1)) continue;
     const float fw0 = floorf(wl), fh0 = floorf(hl);
     const int iw = (int)fw0, ih = (int)fh0;
@@ -496,16 +527,21 @@ struct fcb_bp_plan {
   long long updates = 0;
   std::vector<FdkParams> fdk;  // one per view chunk
   std::vector<GenParams> gen;
+  int4* d_win = nullptr;  // reference-compatible window table (device), when in use
+  ~fcb_bp_plan()
+  {
+    if (d_win) cudaFree(d_win);
+  }
 };
 
 namespace {
 
-template <typename T, int NZ, bool PIW, bool X2>
+template <typename T, int NZ, bool PIW, bool X2, int MINB = 1>
 int launch_fdk(const fcb_bp_plan* pl, const CUtensorMap& map, int chunk, cudaStream_t st)
 {
   const size_t stage_bytes = ((size_t)pl->BW * pl->BH * sizeof(T) + 127) & ~(size_t)127;
   const size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int2));
-  auto kern = fdk_tma_kernel<T, NZ, PIW, X2>;
+  auto kern = fdk_tma_kernel<T, NZ, PIW, X2, MINB>;
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int c = 0; c < (int)pl->fdk.size(); c++) {
     if (chunk >= 0 && c != chunk) continue;
@@ -547,7 +583,7 @@ namespace fcb {
 // receives the kernels' status and the footprint pre-pass result; the pre-pass runs on
 // `st`.  scratch == NULL selects the library's per-device scratch word block.
 static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, int maxViewsPerLaunch,
-                         int* scratch_in, cudaStream_t st, fcb_bp_plan** out)
+                         int* scratch_in, cudaStream_t st, bool may_alloc, fcb_bp_plan** out)
 {
   if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
   *out = nullptr;
@@ -595,7 +631,44 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
   const double turn = pb.nviews > 1 ? pb.angle[pb.nviews - 1] - pb.angle[0] : 1.0;
   const float td_sign = (turn >= 0.0) == (pb.pitch >= 0.0) ? -1.0f : 1.0f;
 
-  if (aligned_geometry(pb)) {
+  // Reference-compatible windows: only when the reference's sub-problem windows cut off
+  // part of a footprint does the result differ from the ideal operator; then the generic
+  // kernel runs with the window table.
+  RefWindows rw;
+  bool compat = false;
+  if (pb.referenceWindows && !piwin) {
+    rc = ref_windows(pb, true, &rw);
+    if (rc) { delete pl; return rc; }
+    compat = rw.bp_matters;
+  }
+  if (compat) {
+    if (!may_alloc) {
+      delete pl;
+      return set_error(FCB_ERR_INVALID,
+                       "reference-compatible windows need a device table; this entry point allocates nothing");
+    }
+    const int ntile = rw.ntx * rw.nty * rw.ntz;
+    std::vector<int4> tab((size_t)ntile * pb.nviews);
+    for (int t = 0; t < ntile; t++)
+      for (int v = 0; v < pb.nviews; v++) {
+        const size_t o = (size_t)t * pb.nviews + v;
+        tab[o] = make_int4(rw.ws[o] - pb.woff[v], rw.ws[o] + rw.subProjDim[0] - 1 - pb.woff[v],
+                           rw.hs[o] - pb.hoff[v], rw.hs[o] + rw.subProjDim[1] - 1 - pb.hoff[v]);
+      }
+    if (cudaMalloc(&pl->d_win, tab.size() * sizeof(int4)) != cudaSuccess) {
+      cudaGetLastError();
+      pl->d_win = nullptr;
+      delete pl;
+      return set_error(FCB_ERR_NOMEM, "device allocation of the window table failed");
+    }
+    if (cudaMemcpy(pl->d_win, tab.data(), tab.size() * sizeof(int4), cudaMemcpyHostToDevice) !=
+        cudaSuccess) {
+      delete pl;
+      return set_error(FCB_ERR_CUDA, "copy of the window table failed");
+    }
+  }
+
+  if (aligned_geometry(pb) && !compat) {
     pl->path = 1;
     pl->wshift = projType == FCB_F32 ? 2 : 3;
     const int NZ = pl->nz_tile;
@@ -671,6 +744,12 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
         P.v[k].kappa = (float)kappa;
         P.v[k].wt = (float)pb.norm[v0 + k];
       }
+      if (compat) {
+        P.win = pl->d_win;
+        P.sv0 = rw.subVolDim[0]; P.sv1 = rw.subVolDim[1]; P.sv2 = rw.subVolDim[2];
+        P.ntx = rw.ntx; P.nty = rw.nty;
+        P.wviews = pb.nviews;
+      }
       pl->gen.push_back(P);
     }
   }
@@ -681,7 +760,7 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
 int bp_plan_create_ex(const fcb_geometry* g, int kernelMode, int projType, int maxViewsPerLaunch,
                       fcb_bp_plan** out)
 {
-  return bp_plan_build(g, kernelMode, projType, maxViewsPerLaunch, nullptr, 0, out);
+  return bp_plan_build(g, kernelMode, projType, maxViewsPerLaunch, nullptr, 0, true, out);
 }
 
 int bp_plan_chunks(const fcb_bp_plan* pl, std::vector<std::pair<int, int>>* ranges)
@@ -725,6 +804,10 @@ int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* v
     } else if (pl->ptype == FCB_F32 && pl->nz_tile == 64) {
       if (piw) FCB_TRY((launch_fdk<float, 64, true, true>(pl, map, chunk, st)));
       else FCB_TRY((launch_fdk<float, 64, false, true>(pl, map, chunk, st)));
+    } else if (pl->ptype == FCB_F32 && getenv("FCB_FDK_MINB4")) {
+      // register cap for 4 CTAs per SM (occupancy experiment)
+      if (piw) FCB_TRY((launch_fdk<float, 32, true, true, 4>(pl, map, chunk, st)));
+      else FCB_TRY((launch_fdk<float, 32, false, true, 4>(pl, map, chunk, st)));
     } else if (pl->ptype == FCB_F32) {
       if (piw) FCB_TRY((launch_fdk<float, 32, true, true>(pl, map, chunk, st)));
       else FCB_TRY((launch_fdk<float, 32, false, true>(pl, map, chunk, st)));
@@ -862,7 +945,7 @@ extern "C" int fcb_backproject_device_noalloc(const fcb_geometry* g, int kernelM
   // the array keeps the previous call's contents: clear the status word and the maxima
   FCB_CUDA_TRY(cudaMemsetAsync(scratch, 0, NOALLOC_NEEDED_INTS * sizeof(int), st));
   fcb_bp_plan* pl = nullptr;
-  FCB_TRY(bp_plan_build(g, kernelMode, projType, FDK_MAXV, scratch, st, &pl));
+  FCB_TRY(bp_plan_build(g, kernelMode, projType, FDK_MAXV, scratch, st, false, &pl));
   int rc = bp_plan_execute_chunk(pl, -1, proj, volume, st);
   fcb_bp_plan_destroy(pl);
   if (rc) return rc;

@@ -54,16 +54,6 @@ struct DeviceGuard {
   }
 };
 
-bool is_pinned(const void* p)
-{
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeHost;
-}
-
 // RAII bundle of device buffers/streams/events of one host-driver call.
 struct Scratch {
   std::vector<void*> dev;
@@ -126,7 +116,17 @@ extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kern
   if (kernelMode != 0) g.misAlignments = nullptr;
   const int W = g.projWHSize[0], H = g.projWHSize[1], n = g.projDim[2];
   if (W <= 0 || H <= 0 || n <= 0) return set_error(FCB_ERR_INVALID, "bad projection sizes");
-  const int wpad = (W + 3) & ~3;  // TMA row pitch must be a multiple of 16 bytes
+  if (g.referenceWindows) {
+    // the reference's windows depend on the data width: decide on the caller's geometry,
+    // and leave the rows unpadded when the windows change the result
+    Problem p0;
+    FCB_TRY(make_problem(&g, &p0));
+    RefWindows rw;
+    FCB_TRY(ref_windows(p0, true, &rw));
+    if (!rw.bp_matters) g.referenceWindows = 0;
+  }
+  // TMA row pitch must be a multiple of 16 bytes
+  const int wpad = g.referenceWindows ? W : (W + 3) & ~3;
   g.projWHSize[0] = wpad;         // zero columns beyond W change nothing (zero extension)
   const int chunk = 120;
   fcb_bp_plan* plan = nullptr;
@@ -232,6 +232,7 @@ fcb_geometry make_geom(float* angles, float* hMidPlane, float D, float pw, int v
   g.pixelWidth = pw;
   g.normalizationFactor = norm;
   g.misAlignments = mis;
+  g.referenceWindows = 1;  // drop-in: reproduce the reference's windows where they matter
   return g;
 }
 }  // namespace

@@ -132,6 +132,7 @@ int make_problem(const fcb_geometry* g, Problem* pb)
   }
   pb->pitch = g->helicalPitch;
   pb->piWindow = g->piWindow;
+  pb->referenceWindows = g->referenceWindows;
   pb->views.resize(n);
   const double D = pb->D, pw = pb->pw;
   const double* m = pb->mis;

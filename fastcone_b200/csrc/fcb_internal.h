@@ -58,6 +58,7 @@ struct Problem {
   double mis[6];
   double pitch;  // helical pitch (voxels per turn), Katsevich window
   int piWindow;
+  int referenceWindows;
   std::vector<ViewGeom> views;
 };
 
@@ -68,6 +69,19 @@ int make_problem(const fcb_geometry* g, Problem* pb);
 // (pixel g of the window centred at g).  For the aligned geometry s is proportional
 // to the source-voxel depth; kappa / s = U (= D / depth).
 void view_matrix(const Problem& pb, int t, double M[12], double* kappa);
+
+// The reference's sub-problem decomposition (fcb_refgeom.cpp): volume tiles (x fastest),
+// per (tile, view) detector-window starts (global detector indices) and projector sweeps,
+// the common window size, and whether they change the backprojection / the projection
+// compared with the ideal operator.
+struct RefWindows {
+  int subVolDim[3] = {0, 0, 0};
+  int subProjDim[2] = {0, 0};
+  int ntx = 0, nty = 0, ntz = 0;
+  std::vector<int> ws, hs, sweepStart, sweepSteps;  // [tile * nviews + view]
+  bool bp_matters = false, proj_matters = false;
+};
+int ref_windows(const Problem& pb, bool with_misalign, RefWindows* rw);
 
 // ------------------------------------------------------------------ TMA descriptors
 int encode_tmap_3d(CUtensorMap* map, CUtensorMapDataType dtype, void* base, uint64_t d0,

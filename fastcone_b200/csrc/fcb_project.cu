@@ -40,6 +40,10 @@ struct PjParams {
   int nx, ny, nz;               // local volume extents
   int WH0, WH1;                 // window size
   int nviews, view0;
+  // reference-compatible sub-problems (project_ref_kernel only): win[tile * wviews + view]
+  // = {first window column, first window row (data-local), sweep start, sweep steps}
+  const int4* win;
+  int sv0, sv1, sv2, ntx, nty, ntz, spd0, spd1, wviews;
   PjView v[PJ_MAXV];
 };
 static_assert(sizeof(PjParams) < 32000, "kernel parameter space");
@@ -180,6 +184,53 @@ __global__ void __launch_bounds__(256) project_explicit_kernel(const __grid_cons
   count_samples(P.samples, cnt);
 }
 
+// The reference's sub-problem projection (unit_coneBeamGPU.cu:88-171): every volume tile
+// of sv0 x sv1 x sv2 voxels is projected on its own, from a copy of the tile ringed by
+// zeros, onto the pixels of its detector window only, marching its own integer sweep of
+// sample distances.  Summed over tiles this is the ideal projection wherever the windows
+// and sweeps cover the tile's shadow; elsewhere it reproduces what the reference loses.
+// Used only when the restated windows show a difference (exact FP32 weights).
+__global__ void __launch_bounds__(256) project_ref_kernel(const __grid_constant__ PjParams P)
+{
+  const int wl = blockIdx.x * 16 + (threadIdx.x & 15);
+  const int hl = blockIdx.y * 16 + (threadIdx.x >> 4);
+  const int v = blockIdx.z;
+  if (wl >= P.WH0 || hl >= P.WH1) return;
+  const PjView& V = P.v[v];
+  float s[3], d[3];
+  ray_of(V, wl, hl, s, d);
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  float acc = 0.0f;
+  for (int tk = 0; tk < P.ntz; tk++)
+    for (int tj = 0; tj < P.nty; tj++)
+      for (int ti = 0; ti < P.ntx; ti++) {
+        const int tile = (tk * P.nty + tj) * P.ntx + ti;
+        const int4 wb = P.win[(size_t)tile * P.wviews + P.view0 + v];
+        if (wl < wb.x || wl >= wb.x + P.spd0 || hl < wb.y || hl >= wb.y + P.spd1) continue;
+        const int ox = ti * P.sv0, oy = tj * P.sv1, oz = tk * P.sv2;
+        const int ex = min(ox + P.sv0, nx), ey = min(oy + P.sv1, ny), ez = min(oz + P.sv2, nz);
+        const float st[3] = {s[0] - ox, s[1] - oy, s[2] - oz};
+        int m0, m1;
+        if (!ray_clip(st, d, ex - ox, ey - oy, ez - oz, m0, m1)) continue;
+        m0 = max(m0, wb.z);
+        m1 = min(m1, wb.z + wb.w - 1);
+        for (int m = m0; m <= m1; m++) {
+          const float mf = (float)m;
+          const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            const int X = t.i + (q & 1), Y = t.j + ((q >> 1) & 1), Z = t.k + ((q >> 2) & 1);
+            if (X < ox || Y < oy || Z < oz || X >= ex || Y >= ey || Z >= ez) continue;
+            const float w = ((q & 1) ? t.a : 1.0f - t.a) * (((q >> 1) & 1) ? t.b : 1.0f - t.b) *
+                            (((q >> 2) & 1) ? t.c : 1.0f - t.c);
+            acc = fmaf(w, __ldg(P.vol + X + Y * sy + Z * sz), acc);
+          }
+        }
+      }
+  P.proj[((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl] += V.wt * acc;
+}
+
 // Exact transpose of project_explicit_kernel: vol += A^T (norm * proj).
 __global__ void __launch_bounds__(256) project_adjoint_kernel(const __grid_constant__ PjParams P,
                                                               float* vol)
@@ -241,9 +292,35 @@ int project_launch(const Problem& pb, int method, const float* vol, float* proj,
 {
   const int nx = pb.volEnd[0] - pb.volStart[0], ny = pb.volEnd[1] - pb.volStart[1],
             nz = pb.volEnd[2] - pb.volStart[2];
+  // reference-compatible sub-problems, when they change the projection
+  RefWindows rw;
+  bool compat = false;
+  if (pb.referenceWindows && !adj_vol) {
+    FCB_TRY(ref_windows(pb, true, &rw));
+    compat = rw.proj_matters;
+  }
+  int4* d_win = nullptr;
+  if (compat) {
+    const int ntile = rw.ntx * rw.nty * rw.ntz;
+    std::vector<int4> tab((size_t)ntile * pb.nviews);
+    for (int t = 0; t < ntile; t++)
+      for (int v = 0; v < pb.nviews; v++) {
+        const size_t o = (size_t)t * pb.nviews + v;
+        tab[o] = make_int4(rw.ws[o] - pb.woff[v], rw.hs[o] - pb.hoff[v], rw.sweepStart[o],
+                           rw.sweepSteps[o]);
+      }
+    FCB_CUDA_TRY(cudaMallocAsync((void**)&d_win, tab.size() * sizeof(int4), st));
+    cudaError_t e = cudaMemcpyAsync(d_win, tab.data(), tab.size() * sizeof(int4),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the table is a local vector
+    if (e != cudaSuccess) {
+      cudaFreeAsync(d_win, st);
+      return set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
+    }
+  }
   cudaArray_t arr = nullptr;
   cudaTextureObject_t tex = 0;
-  if (method == FCB_PROJ_TEXTURE && !adj_vol) {
+  if (method == FCB_PROJ_TEXTURE && !adj_vol && !compat) {
     cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
     FCB_CUDA_TRY(cudaMalloc3DArray(&arr, &cd, make_cudaExtent(nx, ny, nz)));
     cudaMemcpy3DParms cp;
@@ -284,12 +361,20 @@ int project_launch(const Problem& pb, int method, const float* vol, float* proj,
     P.nx = nx; P.ny = ny; P.nz = nz;
     P.WH0 = pb.projWHSize[0]; P.WH1 = pb.projWHSize[1];
     fill_pj_views(pb, v0, std::min(PJ_MAXV, pb.nviews - v0), &P);
+    if (compat) {
+      P.win = d_win;
+      P.sv0 = rw.subVolDim[0]; P.sv1 = rw.subVolDim[1]; P.sv2 = rw.subVolDim[2];
+      P.ntx = rw.ntx; P.nty = rw.nty; P.ntz = rw.ntz;
+      P.spd0 = rw.subProjDim[0]; P.spd1 = rw.subProjDim[1];
+      P.wviews = pb.nviews;
+    }
     chunks.push_back(P);
   }
   int rc = FCB_OK;
   for (const PjParams& P : chunks) {
     dim3 grid((P.WH0 + 15) / 16, (P.WH1 + 15) / 16, P.nviews);
-    if (adj_vol) project_adjoint_kernel<<<grid, 256, 0, st>>>(P, adj_vol);
+    if (compat) project_ref_kernel<<<grid, 256, 0, st>>>(P);
+    else if (adj_vol) project_adjoint_kernel<<<grid, 256, 0, st>>>(P, adj_vol);
     else if (method == FCB_PROJ_TEXTURE) project_tex_kernel<<<grid, 256, 0, st>>>(P);
     else project_explicit_kernel<<<grid, 256, 0, st>>>(P);
     cudaError_t e = cudaGetLastError();
@@ -301,6 +386,7 @@ int project_launch(const Problem& pb, int method, const float* vol, float* proj,
     cudaDestroyTextureObject(tex);
     cudaFreeArray(arr);
   }
+  if (d_win) cudaFreeAsync(d_win, st);
   return rc;
 }
 
@@ -330,6 +416,17 @@ extern "C" int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_
   int rc = make_problem(g, &pl->pb);
   if (rc) { delete pl; return rc; }
   const Problem& pb = pl->pb;
+  if (pb.referenceWindows) {
+    RefWindows rw;
+    rc = ref_windows(pb, true, &rw);
+    if (rc) { delete pl; return rc; }
+    if (rw.proj_matters) {
+      delete pl;
+      return set_error(FCB_ERR_INVALID,
+                       "the reference's sub-problem windows change this projection; plans do not "
+                       "reproduce them (use fcb_project_device)");
+    }
+  }
   pl->method = method;
   pl->nx = pb.volEnd[0] - pb.volStart[0];
   pl->ny = pb.volEnd[1] - pb.volStart[1];

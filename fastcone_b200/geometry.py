@@ -36,6 +36,7 @@ class ConeGeometry:
     misalignments: Optional[np.ndarray] = None  # Dw, Dh, Dl (pixels), Dphi, Dtheta, Dpsi (rad)
     helical_pitch: float = 0.0     # source z advance per turn, voxels (Katsevich window)
     pi_window: bool = False
+    reference_windows: bool = False  # reproduce the reference's sub-problem windows/sweeps
 
     def __post_init__(self):
         self.angles = arr_f32(self.angles)
@@ -99,6 +100,7 @@ class ConeGeometry:
                            else ctypes.cast(None, c_float_p))
         g.helicalPitch = float(self.helical_pitch)
         g.piWindow = 1 if self.pi_window else 0
+        g.referenceWindows = 1 if self.reference_windows else 0
         g._keep = (self.woff, self.hoff, self.angles, self.hmid, self.norm, self.misalignments)
         return g
 

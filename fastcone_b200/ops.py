@@ -214,3 +214,22 @@ def phantom(vol_xyz, params: np.ndarray, device="cuda", out: torch.Tensor | None
 def sync_status():
     """Synchronise the current stream; raise if a kernel recorded a device-side failure."""
     check(lib().fcb_sync_status(_stream()))
+
+
+def reference_windows(geom: ConeGeometry) -> dict:
+    """The reference's sub-problem decomposition of ``geom`` (host computation): tile and
+    window sizes, per [tile, view] window starts and projector sweeps, and whether the
+    windows change the backprojection / projection (``bp_matters`` / ``proj_matters``)."""
+    L = lib()
+    g = geom.struct()
+    sv, sp, tiles, m = (np.zeros(k, np.int32) for k in (3, 2, 3, 2))
+    ip = lambda a: a.ctypes.data_as(_lib.c_int_p)  # noqa: E731
+    null = ctypes.cast(None, _lib.c_int_p)
+    check(L.fcb_reference_windows(ctypes.byref(g), ip(sv), ip(sp), ip(tiles), null, null, null, null, ip(m)))
+    n = int(np.prod(tiles)) * geom.nviews
+    ws, hs, s0, sn = (np.zeros(n, np.int32) for _ in range(4))
+    check(L.fcb_reference_windows(ctypes.byref(g), null, null, null, ip(ws), ip(hs), ip(s0), ip(sn), null))
+    shp = (int(np.prod(tiles)), geom.nviews)
+    return dict(subVolDim=sv, subProjDim=sp, tiles=tiles, ws=ws.reshape(shp), hs=hs.reshape(shp),
+                sweepStart=s0.reshape(shp), sweepSteps=sn.reshape(shp), bp_matters=bool(m[0]),
+                proj_matters=bool(m[1]))

@@ -119,6 +119,10 @@ typedef struct fcb_geometry {
   const float* misAlignments;
   float helicalPitch; /* source z advance per 2*pi rad (voxels); Katsevich PI window only */
   int piWindow;       /* Katsevich: 1 = apply the Tam-Danielsson window, 0 = dense */
+  /* 1 = reproduce the reference's sub-problem detector windows and projector sweeps
+   * (coneBeamGPU.cu:1509-1609, :1757-1786) where they change a result -- the GPU_CB_*
+   * entry points always do; 0 = the ideal operator (zero-extended data, full support). */
+  int referenceWindows;
 } fcb_geometry;
 
 /* Host-buffer versions of GPU_CB_K_backproject / GPU_CB_misalign_project that return
@@ -222,6 +226,17 @@ int fcb_conv3d16_wgrad_device(const void* x, const void* dy, int dyType, float* 
  * centre(3), semi-axes(3), row-major rotation R (9, body = R^T (p - c)), density. */
 int fcb_phantom_device(float* vol, const int volDim[3], const double* params, int n,
                        void* stream);
+
+/* The reference's sub-problem decomposition of a geometry, as restated here for
+ * referenceWindows = 1 (coneBeamGeometry::_setupSubProblem and ::_calculateSweep,
+ * coneBeamGPU.cu:1509-1609, :1757-1786): tile size subVolDim[3], window size subProjDim[2],
+ * tile counts tiles[3] (x, y, z), and per [tile][view] (tile = (z * ty + y) * tx + x) the
+ * window's first detector column / row and the projector's sweep start / steps; matters[0]
+ * / [1] = 1 when the windows change the backprojection / the projection.  Host only (no
+ * device work); any output may be NULL -- call with NULL arrays first to learn the tile
+ * counts.  No counterpart in the reference, whose windows are internal. */
+int fcb_reference_windows(const fcb_geometry* g, int* subVolDim, int* subProjDim, int* tiles,
+                          int* ws, int* hs, int* sweepStart, int* sweepSteps, int* matters);
 
 #ifdef __cplusplus
 }

@@ -126,7 +126,8 @@ def test_reference_abi_project_zeroes_column0():
     vol = _phantom(pb)
     proj = np.full(pb.proj_shape, 0.5, np.float32)
     fc.project(vol, proj, pb.angles, pb.D, pb.hMid, norm=pb.norm, pixelWidth=pb.pw)
-    want = 0.5 + O.project_f64(pb, vol)
+    # reference-compatible: the sub-problem windows of this geometry drop detector rows
+    want = 0.5 + O.ref_project(pb, vol, texq=0)
     want[:, :, 0] = 0.0
     assert np.all(proj[:, :, 0] == 0.0)
     assert O.rel_l2(proj, want) < 1e-3

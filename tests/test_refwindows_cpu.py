@@ -1,0 +1,100 @@
+"""The library's restatement of the reference's sub-problem windows (used when
+referenceWindows = 1) against the oracle's, which is pinned bit-exact to the reference's
+own coneBeamGeometry (test_oracle_cpu).  Host computation only -- no GPU."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.test_oracle_cpu import GEOMETRY_CASES, _helical_case
+
+
+def _geom(pb, mis=None):
+    from fastcone_b200.geometry import ConeGeometry
+
+    return ConeGeometry(tuple(int(v) for v in pb.volDim), (int(pb.projDim[0]), int(pb.projDim[1])), pb.angles,
+                        pb.D, pb.pw, hmid=pb.hMid, norm=pb.norm, vol_start=tuple(int(v) for v in pb.volStart),
+                        vol_end=tuple(int(v) for v in pb.volEnd), woff=pb.projWOffset, hoff=pb.projHOffset,
+                        window_wh=(int(pb.projWHSize[0]), int(pb.projWHSize[1])), misalignments=mis,
+                        reference_windows=True)
+
+
+def _cases():
+    out = [(O.make_problem(**kw), None) for kw in GEOMETRY_CASES]
+    out.append((_helical_case(), None))
+    out.append((O.make_problem((48, 48, 48), (64, 64), 20, D=150, pw=0.8),
+                np.array([1.5, -0.5, 2.0, 0.02, -0.01, 0.03], np.float32)))
+    # several tiles in x and z, two view chunks
+    out.append((O.make_problem((1100, 40, 600), (1200, 700), 300, D=3000, pw=1.0,
+                               volStart=(20, 0, 30), volEnd=(1090, 40, 590)), None))
+    # the 48^3 / 72-pixel case whose windows cut the detector
+    out.append((O.make_problem((48, 48, 48), (72, 48), 36, D=200.0, pw=0.5), None))
+    return out
+
+
+CASES = _cases()
+
+
+@pytest.mark.parametrize("idx", range(len(CASES)))
+def test_windows_match_oracle(idx):
+    from fastcone_b200 import ops
+
+    pb, mis = CASES[idx]
+    a = O.ref_geometry(pb, mis)
+    b = ops.reference_windows(_geom(pb, mis))
+    assert np.array_equal(b["subVolDim"], a["subVolDim"])
+    assert np.array_equal(b["subProjDim"], a["subProjDim"][:2])
+    spd2 = int(a["subProjDim"][2])
+    nsx, nsy, nsz = (int(v) for v in b["tiles"])
+    nsp = a["numSubProblems"] // (nsx * nsy * nsz)
+    n = pb.projDim[2]
+    tg = np.arange(n)
+    pp, t = tg // spd2, tg % spd2
+    for kk in range(nsz):
+        for jj in range(nsy):
+            for ii in range(nsx):
+                tile = (kk * nsy + jj) * nsx + ii
+                idx_ss = ((kk * nsy + jj) * nsx + ii) * nsp + pp
+                o = idx_ss * spd2 + t
+                assert np.array_equal(b["ws"][tile], a["wwStart"][o]), (tile, "ws")
+                assert np.array_equal(b["hs"][tile], a["hhStart"][o]), (tile, "hs")
+                assert np.array_equal(b["sweepStart"][tile], a["sweepStart"][o]), (tile, "sweep")
+                assert np.array_equal(b["sweepSteps"][tile], a["sweepNumSteps"][o]), (tile, "steps")
+
+
+@pytest.mark.parametrize("name,kw", [
+    ("quirk", dict(vol_xyz=(48, 48, 48), det_wh=(72, 48), nviews=36, D=200.0, pw=0.5)),
+    ("clean", dict(vol_xyz=(48, 48, 48), det_wh=(64, 48), nviews=36, D=200.0, pw=0.5)),
+    ("windows", dict(vol_xyz=(64, 56, 40), det_wh=(80, 64), nviews=30, D=180.0, pw=0.7,
+                     volStart=(6, 4, 3), volEnd=(58, 50, 37), whsize=(60, 48),
+                     woff=np.arange(30) % 5 + 6, hoff=np.arange(30) % 4 + 7)),
+])
+def test_bp_matters_flag_agrees_with_oracle_difference(name, kw):
+    """bp_matters is set exactly when the reference's windowed backprojection (exact
+    weights) differs from the ideal one on a random detector."""
+    from fastcone_b200 import ops
+
+    pb = O.make_problem(**kw)
+    proj = np.random.default_rng(3).random(pb.proj_shape, dtype=np.float32)
+    flags = ops.reference_windows(_geom(pb))
+    for mode in (2, 0):
+        diff = O.rel_l2(O.ref_backproject(pb, proj, kernel_mode=mode, texq=0),
+                        O.backproject_f64(pb, proj, kernel_mode=mode))
+        assert (diff > 1e-5) == flags["bp_matters"], (mode, diff, flags["bp_matters"])
+
+
+@pytest.mark.parametrize("kw", [
+    dict(vol_xyz=(48, 48, 48), det_wh=(72, 48), nviews=36, D=200.0, pw=0.5),
+    dict(vol_xyz=(48, 48, 48), det_wh=(64, 48), nviews=36, D=200.0, pw=0.5),
+    dict(vol_xyz=(40, 40, 24), det_wh=(90, 40), nviews=20, D=120.0, pw=0.5),
+])
+def test_proj_matters_flag_covers_every_difference(kw):
+    """proj_matters may be conservative but never misses a case where the reference's
+    windows or sweeps change the projection."""
+    from fastcone_b200 import ops
+
+    pb = O.make_problem(**kw)
+    s, e = pb.volStart, pb.volEnd
+    vol = np.random.default_rng(1).random((e[2] - s[2], e[1] - s[1], e[0] - s[0]), dtype=np.float32)
+    diff = O.rel_l2(O.ref_project(pb, vol, texq=0), O.project_f64(pb, vol))
+    if diff > 1e-5:
+        assert ops.reference_windows(_geom(pb))["proj_matters"], diff
