@@ -167,20 +167,34 @@ def ssim3d(x, ref, mask, sigma=1.5):
     return float(s[mask].mean())
 
 
+def step_weights(steps: int = STEPS, final: float = 2.0):
+    """Loss weight of each unrolled step's output: every step is supervised (so each
+    intermediate x_k is already a good reconstruction and the chain can stop early), the
+    final output counts `final` times; normalised to sum 1."""
+    w = [1.0] * (steps - 1) + [final]
+    t = sum(w)
+    return [v / t for v in w]
+
+
 def train(net: UnrolledNet, geom: ConeGeometry, n_phantoms: int = 2000, lr: float = 1e-3, seed0: int = 1000,
-          log_every: int = 50, checkpoint: str | None = None, log=print):
-    """Trains on seeded phantoms generated (and projected) on the GPU, one per step."""
+          log_every: int = 50, checkpoint: str | None = None, log=print, deep: bool = True):
+    """Trains on seeded phantoms generated (and projected) on the GPU, one per step.
+    deep=True supervises every step's output (step_weights), else only the last."""
     ops_ = Operators(geom)
     mask = fov_mask(ops_.g)
     opt = torch.optim.Adam(net.parameters(), lr=lr)
     sched = torch.optim.lr_scheduler.CosineAnnealingLR(opt, n_phantoms)
+    wk = step_weights(net.steps) if deep else [0.0] * (net.steps - 1) + [1.0]
     t0 = time.time()
     for i in range(n_phantoms):
         mu, y = make_sample(ops_, seed0 + i)
         with torch.no_grad():
             x0 = ops_.fdk(y)
-        x = net(x0, y, ops_)
-        loss = torch.mean((x[mask] - mu[mask]) ** 2) / MU_PER_VOXEL ** 2
+        outs = []
+        x = net(x0, y, ops_, callback=lambda k, xk: outs.append(xk))
+        m = mu[mask]
+        loss = sum(w * torch.mean((xk[mask] - m) ** 2) for w, xk in zip(wk, outs) if w > 0)
+        loss = loss / MU_PER_VOXEL ** 2
         opt.zero_grad(set_to_none=True)
         loss.backward()
         opt.step()
@@ -190,7 +204,7 @@ def train(net: UnrolledNet, geom: ConeGeometry, n_phantoms: int = 2000, lr: floa
                 f"t {time.time() - t0:.0f}s")
         if checkpoint and (i + 1) % 500 == 0:
             torch.save({"model": net.state_dict(), "optim": opt.state_dict(), "phantoms_seen": i + 1,
-                        "seed0": seed0}, checkpoint)
+                        "seed0": seed0, "deep": deep}, checkpoint)
     return net
 
 
@@ -257,6 +271,7 @@ def main():
     ap.add_argument("--weights", default=None, help="load weights from / save weights to this file")
     ap.add_argument("--eval", type=int, default=0, help="number of held-out phantoms to evaluate")
     ap.add_argument("--out", default=None, help="write the evaluation JSON here")
+    ap.add_argument("--final-only", action="store_true", help="supervise only the last step")
     a = ap.parse_args()
     torch.manual_seed(0)
     geom = configs.learned_sparse()
@@ -264,9 +279,10 @@ def main():
     if a.weights and a.train == 0:
         net.load_state_dict(torch.load(a.weights, map_location="cuda")["model"])
     if a.train:
-        train(net, geom, a.train, a.lr, checkpoint=a.weights)
+        train(net, geom, a.train, a.lr, checkpoint=a.weights, deep=not a.final_only)
         if a.weights:
-            torch.save({"model": net.state_dict(), "phantoms_seen": a.train}, a.weights)
+            torch.save({"model": net.state_dict(), "phantoms_seen": a.train, "deep": not a.final_only},
+                       a.weights)
     if a.eval:
         r = evaluate(net, geom, list(range(1, a.eval + 1)))
         s = json.dumps(r)
