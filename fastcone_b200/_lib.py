@@ -28,7 +28,7 @@ FCB_ERR_RANGE = 6
 
 FCB_F32, FCB_F16, FCB_BF16 = 0, 1, 2
 MODE_UNWEIGHTED, MODE_KATSEVICH, MODE_FDK = 0, 1, 2
-PROJ_TEXTURE, PROJ_EXPLICIT = 0, 1
+PROJ_TEXTURE, PROJ_EXPLICIT, PROJ_EXPLICIT_GLOBAL = 0, 1, 2
 FILTER_RAMLAK, FILTER_SHEPPLOGAN = 0, 1
 
 # Every symbol include/fastcone_b200.h declares (checked by the CPU test suite).
@@ -44,7 +44,7 @@ EXPORTED_SYMBOLS = [
     "fcb_backproject_device_noalloc", "fcb_katsevich_filter_device",
     "fcb_conv3d16_device", "fcb_conv3d16_wgrad_device",
     "fcb_proj_plan_create", "fcb_proj_plan_execute", "fcb_proj_plan_destroy",
-    "fcb_reference_windows",
+    "fcb_reference_windows", "fcb_proj_plan_info",
 ]
 
 
@@ -122,6 +122,7 @@ def lib():
                                                       c_float_p, ctypes.c_float, ctypes.c_float,
                                                       ctypes.c_float, ctypes.c_int, vp]
             L.fcb_reference_windows.argtypes = [gp] + [c_int_p] * 8
+            L.fcb_proj_plan_info.argtypes = [vp] + [c_int_p] * 4
             _lib = L
     return _lib
 

@@ -44,9 +44,13 @@ struct PjParams {
   // = {first window column, first window row (data-local), sweep start, sweep steps}
   const int4* win;
   int sv0, sv1, sv2, ntx, nty, ntz, spd0, spd1, wviews;
+  // TMA-brick projector (project_brick_kernel only): brick cross / z extents, stages,
+  // bytes per stage (128-byte multiple), status word
+  int BC, BZ, stages, stage_bytes;
+  int* status;
   PjView v[PJ_MAXV];
 };
-static_assert(sizeof(PjParams) < 32000, "kernel parameter space");
+static_assert(sizeof(PjParams) + 2 * sizeof(CUtensorMap) < 32000, "kernel parameter space");
 
 // Integer sample range [m0, m1] of S + m d inside the open box (-1, n) per axis.
 __device__ __forceinline__ bool ray_clip(const float s[3], const float d[3], int nx, int ny,
@@ -182,6 +186,344 @@ __global__ void __launch_bounds__(256) project_explicit_kernel(const __grid_cons
     P.proj[((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl] += V.wt * acc;
   }
   count_samples(P.samples, cnt);
+}
+
+// ------------------------------------------------------------------ TMA-brick projector
+// Explicit FP32 trilinear sampling from volume bricks staged in shared memory by TMA.
+// A CTA owns a bundle of 32 x 8 rays (detector pixels) of one view.  Its rays share the
+// source, so the bundle is a thin frustum; the CTA walks it along the dominant axis of its
+// central ray (x or y) in slabs of PB_T planes, and a producer warp stages, per slab, the
+// brick of voxels the frustum can touch there -- PB_T + 1 dominant planes x BC cross
+// voxels x BZ z-planes -- with one 3-D TMA load (zero fill outside the volume) into a ring
+// of `stages` buffers.  Eight consumer warps (one detector row each, lanes along the row)
+// then take every sample of their ray inside the slab from shared memory.  For x-dominant
+// bundles the bricks come from a y-fastest copy of the volume, so that in both cases the
+// lanes of a warp walk along the brick's contiguous axis (no bank conflicts).
+//
+// Sample positions, weights and the order of the FP32 operations are those of
+// project_explicit_kernel (tri_of / tri_fetch), so the two kernels agree bit for bit: a
+// sample whose taps are not all inside the volume, or not inside the staged brick, is
+// taken from global memory by tri_fetch itself.
+constexpr int PB_W = 32, PB_H = 8;              // rays per CTA: 32 pixels x 8 rows
+constexpr int PB_CWARPS = PB_H;                 // one consumer warp per detector row
+constexpr int PB_THREADS = (PB_CWARPS + 1) * 32;
+constexpr int PB_T = 12;                        // dominant planes per slab
+constexpr int PB_BD = PB_T + 1;                 // dominant planes per brick
+
+struct Bundle {
+  float s[3];     // source (local voxel-index coordinates)
+  float d[4][3];  // unit directions of the bundle's four corner rays
+  int xdom;       // 1: x is the dominant axis, bricks from the y-fastest copy
+  int sgn;        // direction of travel along the dominant axis (+1 / -1)
+};
+
+__device__ __forceinline__ void bundle_of(const PjView& V, int bw0, int bh0, Bundle& B)
+{
+  float c[3] = {0.0f, 0.0f, 0.0f};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    float s[3], d[3];
+    ray_of(V, bw0 + (q & 1) * (PB_W - 1), bh0 + (q >> 1) * (PB_H - 1), s, d);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      B.d[q][a] = d[a];
+      B.s[a] = s[a];
+      c[a] += d[a];
+    }
+  }
+  B.xdom = fabsf(c[0]) >= fabsf(c[1]) ? 1 : 0;
+  B.sgn = (B.xdom ? c[0] : c[1]) > 0.0f ? 1 : -1;
+}
+
+// Brick of the slab whose samples have floor(dominant) in [a, a + PB_T - 1]: the frustum's
+// cross / z range between the dominant planes a and a + PB_T (clipped to [lo, hi]), plus
+// the +1 trilinear neighbour; the cross origin is aligned down to 4 voxels (16-byte TMA rule).
+__device__ __forceinline__ void brick_extent(const Bundle& B, int a, float lo, float hi, int& c0,
+                                             int& z0, int& needc, int& needz)
+{
+  // (selects instead of runtime array indices keep everything in registers)
+  const bool xd = B.xdom != 0;
+  const float sD = xd ? B.s[0] : B.s[1], sC = xd ? B.s[1] : B.s[0];
+  float cmin = 3.0e38f, cmax = -3.0e38f, zmin = 3.0e38f, zmax = -3.0e38f;
+  const float p0 = fmaxf((float)a, lo), p1 = fminf((float)(a + PB_T), hi);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const float dD = xd ? B.d[q][0] : B.d[q][1], dC = xd ? B.d[q][1] : B.d[q][0];
+    const float inv = 1.0f / dD;
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      const float t = ((e ? p1 : p0) - sD) * inv;
+      const float c = fmaf(t, dC, sC), z = fmaf(t, B.d[q][2], B.s[2]);
+      cmin = fminf(cmin, c); cmax = fmaxf(cmax, c);
+      zmin = fminf(zmin, z); zmax = fmaxf(zmax, z);
+    }
+  }
+  cmin = fminf(fmaxf(cmin, -1.0e6f), 1.0e6f); cmax = fminf(fmaxf(cmax, -1.0e6f), 1.0e6f);
+  zmin = fminf(fmaxf(zmin, -1.0e6f), 1.0e6f); zmax = fminf(fmaxf(zmax, -1.0e6f), 1.0e6f);
+  c0 = __float2int_rd(cmin) & ~3;
+  z0 = __float2int_rd(zmin);
+  needc = __float2int_rd(cmax) + 2 - c0;
+  needz = __float2int_rd(zmax) + 2 - z0;
+}
+
+// Pre-pass: the largest brick over every (view, bundle, slab start) sizes the staged box.
+__global__ void project_brick_extent_kernel(const __grid_constant__ PjParams P, int bx, int by,
+                                            int* out)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long total = (long long)P.nviews * bx * by;
+  int mc = 0, mz = 0;
+  if (i < total) {
+    const int v = (int)(i / ((long long)bx * by));
+    const int b = (int)(i % ((long long)bx * by));
+    Bundle B;
+    bundle_of(P.v[v], (b % bx) * PB_W, (b / bx) * PB_H, B);
+    const int ndom = B.xdom ? P.nx : P.ny;
+    for (int a = -PB_T; a <= ndom; a++) {
+      int c0, z0, nc, nz;
+      brick_extent(B, a, -1.0f, (float)ndom, c0, z0, nc, nz);
+      mc = max(mc, nc);
+      mz = max(mz, nz);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mc = max(mc, __shfl_xor_sync(0xffffffffu, mc, o));
+    mz = max(mz, __shfl_xor_sync(0xffffffffu, mz, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(out, mc);
+    atomicMax(out + 1, mz);
+  }
+}
+
+__device__ __forceinline__ float lds32(uint32_t a)
+{
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+
+__global__ void __launch_bounds__(PB_THREADS, 1) project_brick_kernel(
+    const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmT,
+    const __grid_constant__ PjParams P)
+{
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)P.stages * P.stage_bytes);
+  uint64_t* empty = full + P.stages;
+  int4* origin = reinterpret_cast<int4*>(empty + P.stages);
+  int* range = reinterpret_cast<int*>(origin + P.stages);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int v = blockIdx.z;
+  const PjView& V = P.v[v];
+  const int bw0 = blockIdx.x * PB_W, bh0 = blockIdx.y * PB_H;
+  Bundle B;
+  bundle_of(V, bw0, bh0, B);
+  const bool xd = B.xdom != 0;
+  const int ndom = xd ? P.nx : P.ny;
+
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < P.stages; st++) {
+      dev::mbar_init(&full[st], 1);
+      dev::mbar_init(&empty[st], PB_CWARPS);
+    }
+    range[0] = 0x7fffffff;
+    range[1] = -0x7fffffff;
+    dev::fence_mbar_init();
+  }
+  __syncthreads();
+
+  // each consumer thread: its ray, clipped to the interpolant's support
+  float s[3], d[3];
+  int m0 = 1, m1 = 0;
+  const int wl = bw0 + lane, hl = bh0 + warp;
+  const bool pix = warp < PB_CWARPS && wl < P.WH0 && hl < P.WH1;
+  if (pix) {
+    ray_of(V, wl, hl, s, d);
+    if (ray_clip(s, d, P.nx, P.ny, P.nz, m0, m1)) {
+      const float sD = xd ? s[0] : s[1], dD = xd ? d[0] : d[1];
+      const int f0 = (int)floorf(fmaf((float)m0, dD, sD));
+      const int f1 = (int)floorf(fmaf((float)m1, dD, sD));
+      atomicMin(&range[0], min(f0, f1));
+      atomicMax(&range[1], max(f0, f1));
+    } else {
+      m0 = 1;
+      m1 = 0;
+    }
+  }
+  __syncthreads();
+  const int fmin = range[0], fmax = range[1];
+  const int nsl = fmax >= fmin ? (fmax - fmin) / PB_T + 1 : 0;
+
+  if (warp == PB_CWARPS) {
+    // ------------------------------------------------------------- producer warp
+    if (lane != 0) return;
+    const CUtensorMap* tm = B.xdom ? &tmT : &tmV;
+    dev::tma_prefetch(tm);
+    const uint32_t bytes = (uint32_t)(P.BC * PB_BD * P.BZ * 4);
+    int issued = 0;
+    bool failed = false;
+    for (int k = 0; k < nsl; k++) {
+      const int st = k % P.stages;
+      if (k >= P.stages && !dev::mbar_wait(&empty[st], ((k / P.stages) - 1) & 1)) {
+        failed = true;
+        break;
+      }
+      const int a = B.sgn > 0 ? fmin + k * PB_T : fmax - PB_T + 1 - k * PB_T;
+      int c0, z0, nc, nz;
+      brick_extent(B, a, -1.0f, (float)ndom, c0, z0, nc, nz);
+      origin[st] = make_int4(c0, a, z0, 0);
+      dev::mbar_arrive_expect_tx(&full[st], bytes);
+      dev::tma_load_3d(smem_raw + (size_t)st * P.stage_bytes, tm, &full[st], c0, a, z0);
+      issued = k + 1;
+    }
+    if (failed) {
+      dev::record_status(P.status, DEV_TIMEOUT);
+      for (int k = max(0, issued - P.stages); k < issued; k++)
+        dev::mbar_wait(&full[k % P.stages], (k / P.stages) & 1, 100000000ull);
+    }
+    return;
+  }
+
+  // --------------------------------------------------------------- consumer warps
+  const uint32_t sbase = dev::smem_u32(smem_raw);
+  const uint32_t rowb = (uint32_t)P.BC * 4u, planeb = rowb * (uint32_t)PB_BD;
+  const uint32_t ox = B.xdom ? rowb : 4u, oy = B.xdom ? 4u : rowb;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  float acc = 0.0f;
+  int m = m0;
+  for (int k = 0; k < nsl; k++) {
+    const int st = k % P.stages;
+    // warp-uniform outcome, so the warp-wide operations below stay converged
+    if (!__all_sync(0xffffffffu, dev::mbar_wait(&full[st], (k / P.stages) & 1))) {
+      dev::record_status(P.status, DEV_TIMEOUT);
+      return;
+    }
+    const int4 o = origin[st];
+    const int alo = o.y, ahi = o.y + PB_T - 1;
+    const uint32_t stb = sbase + (uint32_t)st * (uint32_t)P.stage_bytes;
+    while (m <= m1) {
+      const float mf = (float)m;
+      const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
+      const int idom = B.xdom ? t.i : t.j;
+      if (B.sgn > 0 ? idom > ahi : idom < alo) break;
+      const int ic = (B.xdom ? t.j : t.i) - o.x, id = idom - alo, iz = t.k - o.z;
+      const bool inside = t.i >= 0 && t.j >= 0 && t.k >= 0 && t.i + 1 < nx && t.j + 1 < ny &&
+                          t.k + 1 < nz;
+      float val;
+      if (inside && (unsigned)ic < (unsigned)(P.BC - 1) && (unsigned)id < (unsigned)PB_T &&
+          (unsigned)iz < (unsigned)(P.BZ - 1)) {
+        const uint32_t p = stb + (uint32_t)iz * planeb + (uint32_t)id * rowb + (uint32_t)ic * 4u;
+        const float v000 = lds32(p), v100 = lds32(p + ox), v010 = lds32(p + oy),
+                    v110 = lds32(p + ox + oy);
+        const float v001 = lds32(p + planeb), v101 = lds32(p + planeb + ox),
+                    v011 = lds32(p + planeb + oy), v111 = lds32(p + planeb + ox + oy);
+        const float x00 = fmaf(t.a, v100 - v000, v000), x10 = fmaf(t.a, v110 - v010, v010);
+        const float x01 = fmaf(t.a, v101 - v001, v001), x11 = fmaf(t.a, v111 - v011, v011);
+        const float y0 = fmaf(t.b, x10 - x00, x00), y1 = fmaf(t.b, x11 - x01, x01);
+        val = fmaf(t.c, y1 - y0, y0);
+      } else {
+        val = tri_fetch(P.vol, nx, ny, nz, t);
+      }
+      acc += val;
+      m++;
+    }
+    __syncwarp();
+    if (lane == 0) dev::mbar_arrive(&empty[st]);
+  }
+  if (pix) P.proj[((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl] += V.wt * acc;
+  count_samples(P.samples, m1 - m0 + 1);
+}
+
+// y-fastest copy of the volume: vt[z][x][y] = vol[z][y][x] (bricks of x-dominant bundles).
+__global__ void transpose_xy_kernel(const float* __restrict__ vol, float* __restrict__ vt, int nx,
+                                    int ny)
+{
+  __shared__ float tile[32][33];
+  const int z = blockIdx.z;
+  const size_t plane = (size_t)nx * ny;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int x = x0 + threadIdx.x, y = y0 + r;
+    if (x < nx && y < ny) tile[r][threadIdx.x] = vol[z * plane + (size_t)y * nx + x];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int y = y0 + threadIdx.x, x = x0 + r;
+    if (x < nx && y < ny) vt[z * plane + (size_t)x * ny + y] = tile[threadIdx.x][r];
+  }
+}
+
+// Host side of the brick projector: box sizing (pre-pass), the y-fastest copy, tensor maps.
+struct BrickSetup {
+  bool ok = false;
+  int BC = 0, BZ = 0, stages = 0, stage_bytes = 0;
+  size_t smem = 0;
+};
+
+// Sizes the bricks for the views of `chunks` (pre-pass on `st`, synchronises `st`).
+// ok == false when the volume rows are not 16-byte multiples or the bricks do not fit.
+int brick_setup(const std::vector<PjParams>& chunks, int nx, int ny, cudaStream_t st, BrickSetup* bs)
+{
+  bs->ok = false;
+  if (nx % 4 != 0 || ny % 4 != 0 || getenv("FCB_PROJ_NOBRICK")) return FCB_OK;
+  int* scratch = nullptr;
+  FCB_TRY(device_status_ptr(&scratch));
+  int* need = scratch + 3;  // [3..4]: brick extents ([1..2] belong to the backprojector)
+  FCB_CUDA_TRY(cudaMemsetAsync(need, 0, 2 * sizeof(int), st));
+  for (const PjParams& P : chunks) {
+    const int bx = (P.WH0 + PB_W - 1) / PB_W, by = (P.WH1 + PB_H - 1) / PB_H;
+    const long long total = (long long)P.nviews * bx * by;
+    project_brick_extent_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(P, bx, by, need);
+    FCB_CUDA_TRY(cudaGetLastError());
+  }
+  int h[2] = {0, 0};
+  FCB_CUDA_TRY(cudaMemcpyAsync(h, need, sizeof h, cudaMemcpyDeviceToHost, st));
+  FCB_CUDA_TRY(cudaStreamSynchronize(st));
+  const int BC = std::max(4, (h[0] + 3) & ~3), BZ = std::max(2, h[1]);
+  if (BC > 128 || BZ > 64) return FCB_OK;  // a wide cone: bricks would not pay
+  const int box = BC * PB_BD * BZ * 4;
+  const int stage_bytes = (box + 127) & ~127;
+  const int stages = std::max(2, std::min(4, (96 * 1024) / stage_bytes));
+  const size_t smem = (size_t)stages * stage_bytes + stages * (2 * sizeof(uint64_t) + sizeof(int4)) + 16;
+  if (smem > 200 * 1024) return FCB_OK;
+  bs->ok = true;
+  bs->BC = BC;
+  bs->BZ = BZ;
+  bs->stages = stages;
+  bs->stage_bytes = stage_bytes;
+  bs->smem = smem;
+  return FCB_OK;
+}
+
+// Launches the brick projector over `chunks` (the volume and its y-fastest copy `vt`).
+int brick_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, const float* vol, float* vt,
+                 int nx, int ny, int nz, cudaStream_t st)
+{
+  if ((uintptr_t)vol % 16 || (uintptr_t)vt % 16)
+    return set_error(FCB_ERR_INVALID, "volume buffers must be 16-byte aligned");
+  dim3 tg((nx + 31) / 32, (ny + 31) / 32, nz);
+  transpose_xy_kernel<<<tg, dim3(32, 8), 0, st>>>(vol, vt, nx, ny);
+  FCB_CUDA_TRY(cudaGetLastError());
+  CUtensorMap mv, mt;
+  FCB_TRY(encode_tmap_3d(&mv, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, const_cast<float*>(vol), nx, ny, nz,
+                         (uint64_t)nx * 4, (uint64_t)nx * ny * 4, bs.BC, PB_BD, bs.BZ));
+  FCB_TRY(encode_tmap_3d(&mt, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vt, ny, nx, nz, (uint64_t)ny * 4,
+                         (uint64_t)nx * ny * 4, bs.BC, PB_BD, bs.BZ));
+  int* status = nullptr;
+  FCB_TRY(device_status_ptr(&status));
+  FCB_CUDA_TRY(cudaFuncSetAttribute(project_brick_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)bs.smem));
+  for (PjParams& P : chunks) {
+    P.BC = bs.BC;
+    P.BZ = bs.BZ;
+    P.stages = bs.stages;
+    P.stage_bytes = bs.stage_bytes;
+    P.status = status;
+    dim3 grid((P.WH0 + PB_W - 1) / PB_W, (P.WH1 + PB_H - 1) / PB_H, P.nviews);
+    project_brick_kernel<<<grid, PB_THREADS, bs.smem, st>>>(mv, mt, P);
+    FCB_CUDA_TRY(cudaGetLastError());
+  }
+  return FCB_OK;
 }
 
 // The reference's sub-problem projection (unit_coneBeamGPU.cu:88-171): every volume tile
@@ -371,6 +713,17 @@ int project_launch(const Problem& pb, int method, const float* vol, float* proj,
     chunks.push_back(P);
   }
   int rc = FCB_OK;
+  if (method == FCB_PROJ_EXPLICIT && !adj_vol && !compat) {
+    BrickSetup bs;
+    FCB_TRY(brick_setup(chunks, nx, ny, st, &bs));
+    if (bs.ok) {
+      float* vt = nullptr;
+      FCB_CUDA_TRY(cudaMallocAsync((void**)&vt, (size_t)nx * ny * nz * sizeof(float), st));
+      rc = brick_launch(chunks, bs, vol, vt, nx, ny, nz, st);
+      cudaFreeAsync(vt, st);
+      return rc;
+    }
+  }
   for (const PjParams& P : chunks) {
     dim3 grid((P.WH0 + 15) / 16, (P.WH1 + 15) / 16, P.nviews);
     if (compat) project_ref_kernel<<<grid, 256, 0, st>>>(P);
@@ -404,13 +757,15 @@ struct fcb_proj_plan {
   cudaArray_t arr = nullptr;
   cudaTextureObject_t tex = 0;
   std::vector<PjParams> chunks;
+  BrickSetup bricks;     // explicit method: staged-brick projector, when it applies
+  float* vt = nullptr;   // its y-fastest volume copy
 };
 
 extern "C" int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_plan** out)
 {
   if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
   *out = nullptr;
-  if (method != FCB_PROJ_TEXTURE && method != FCB_PROJ_EXPLICIT)
+  if (method != FCB_PROJ_TEXTURE && method != FCB_PROJ_EXPLICIT && method != FCB_PROJ_EXPLICIT_GLOBAL)
     return set_error(FCB_ERR_INVALID, "unknown projector method");
   auto* pl = new fcb_proj_plan();
   int rc = make_problem(g, &pl->pb);
@@ -456,6 +811,18 @@ extern "C" int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_
     fill_pj_views(pb, v0, std::min(PJ_MAXV, pb.nviews - v0), &P);
     pl->chunks.push_back(P);
   }
+  if (method == FCB_PROJ_EXPLICIT) {
+    rc = brick_setup(pl->chunks, pl->nx, pl->ny, 0, &pl->bricks);
+    if (rc == FCB_OK && pl->bricks.ok &&
+        cudaMalloc((void**)&pl->vt, (size_t)pl->nx * pl->ny * pl->nz * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      rc = set_error(FCB_ERR_NOMEM, "device allocation of the brick projector's volume copy failed");
+    }
+    if (rc) {
+      fcb_proj_plan_destroy(pl);
+      return rc;
+    }
+  }
   *out = pl;
   return ok();
 }
@@ -466,8 +833,16 @@ extern "C" int fcb_proj_plan_execute(fcb_proj_plan* pl, const float* volume, flo
 {
   if (!pl || !volume || !proj) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  if (adjoint && pl->method != FCB_PROJ_EXPLICIT)
+  if (adjoint && pl->method == FCB_PROJ_TEXTURE)
     return set_error(FCB_ERR_INVALID, "the adjoint belongs to the explicit projector");
+  if (!adjoint && pl->bricks.ok) {
+    for (PjParams& P : pl->chunks) {
+      P.vol = volume;
+      P.proj = proj;
+    }
+    FCB_TRY(brick_launch(pl->chunks, pl->bricks, volume, pl->vt, pl->nx, pl->ny, pl->nz, st));
+    return ok();
+  }
   if (pl->method == FCB_PROJ_TEXTURE) {
     cudaMemcpy3DParms cp;
     memset(&cp, 0, sizeof(cp));
@@ -489,11 +864,23 @@ extern "C" int fcb_proj_plan_execute(fcb_proj_plan* pl, const float* volume, flo
   return ok();
 }
 
+extern "C" int fcb_proj_plan_info(const fcb_proj_plan* pl, int* staged, int* brickC, int* brickZ,
+                                  int* stages)
+{
+  if (!pl) return set_error(FCB_ERR_INVALID, "NULL plan");
+  if (staged) *staged = pl->bricks.ok ? 1 : 0;
+  if (brickC) *brickC = pl->bricks.BC;
+  if (brickZ) *brickZ = pl->bricks.BZ;
+  if (stages) *stages = pl->bricks.stages;
+  return ok();
+}
+
 extern "C" int fcb_proj_plan_destroy(fcb_proj_plan* pl)
 {
   if (pl) {
     if (pl->tex) cudaDestroyTextureObject(pl->tex);
     if (pl->arr) cudaFreeArray(pl->arr);
+    if (pl->vt) cudaFree(pl->vt);
     delete pl;
   }
   return ok();
@@ -503,7 +890,7 @@ extern "C" int fcb_project_device(const fcb_geometry* g, int method, const float
                                   float* proj, void* stream)
 {
   if (!volume || !proj) return set_error(FCB_ERR_INVALID, "NULL buffer");
-  if (method != FCB_PROJ_TEXTURE && method != FCB_PROJ_EXPLICIT)
+  if (method != FCB_PROJ_TEXTURE && method != FCB_PROJ_EXPLICIT && method != FCB_PROJ_EXPLICIT_GLOBAL)
     return set_error(FCB_ERR_INVALID, "unknown projector method");
   Problem pb;
   FCB_TRY(make_problem(g, &pb));

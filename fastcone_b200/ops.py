@@ -121,6 +121,13 @@ class ProjectPlan:
                                           0, _stream()))
         return proj
 
+    def info(self) -> dict:
+        """Whether the explicit projector runs on TMA-staged bricks, and their shape."""
+        v = [ctypes.c_int() for _ in range(4)]
+        check(lib().fcb_proj_plan_info(self._h, *[ctypes.byref(x) for x in v]))
+        return {"staged": bool(v[0].value), "brick_c": v[1].value, "brick_z": v[2].value,
+                "stages": v[3].value}
+
     def adjoint(self, proj: torch.Tensor, vol: torch.Tensor | None = None) -> torch.Tensor:
         if tuple(proj.shape) != self.geom.proj_shape:
             raise ValueError("projection shape does not match the plan")

@@ -47,7 +47,11 @@ extern "C" {
 
 /* forward projector variants */
 #define FCB_PROJ_TEXTURE 0   /* hardware texture trilinear (8-bit weights, like the reference) */
-#define FCB_PROJ_EXPLICIT 1  /* explicit FP32 trilinear; exact transpose is fcb_project_adjoint_device */
+#define FCB_PROJ_EXPLICIT 1  /* explicit FP32 trilinear from TMA-staged volume bricks (global-memory
+                                reads where a brick does not apply); exact transpose is
+                                fcb_project_adjoint_device */
+#define FCB_PROJ_EXPLICIT_GLOBAL 2 /* the same samples and arithmetic (bit-identical results), every
+                                      tap read from global memory: the unstaged comparison */
 
 /* ramp-filter windows for fcb_fdk_filter_device */
 #define FCB_FILTER_RAMLAK 0
@@ -180,6 +184,10 @@ int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_plan** plan
 int fcb_proj_plan_execute(fcb_proj_plan* plan, const float* volume, float* proj, int adjoint,
                           void* stream);
 int fcb_proj_plan_destroy(fcb_proj_plan* plan);
+/* staged = 1 when the plan's explicit projector runs on TMA-staged bricks of brickC (cross,
+ * contiguous) x 13 (along the ray) x brickZ voxels in `stages` shared-memory buffers. */
+int fcb_proj_plan_info(const fcb_proj_plan* plan, int* staged, int* brickC, int* brickZ,
+                       int* stages);
 
 /* Waits for `stream` and returns FCB_ERR_TIMEOUT / FCB_ERR_RANGE if a kernel of this
  * library recorded a device-side failure since the previous check, else FCB_OK. */
