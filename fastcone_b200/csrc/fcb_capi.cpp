@@ -10,7 +10,10 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <stdlib.h>
+
 #include <algorithm>
+#include <chrono>
 #include <vector>
 
 #include "fcb_internal.h"
@@ -106,16 +109,36 @@ int copy_proj_h2d(float* d, const float* h, int v0, int v1, int W, int H, int wp
 
 }  // namespace
 
+// Phase times of one host-driver call, printed to stderr when FCB_HOST_TRACE is set.
+struct HostTrace {
+  bool on = getenv("FCB_HOST_TRACE") != nullptr;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  double ms() const
+  {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
+// Host-buffer backprojection, pipelined over z-slabs of the volume:
+//   copy-in stream : volume slab 0, the projections in view chunks, then volume slab s+1
+//   compute stream : slab 0 chunk by chunk as the projections arrive, then whole slabs
+//   copy-out stream: slab s back to the host as soon as its backprojection is done
+// so the PCIe traffic (projections once, the volume in and out) hides behind the kernels
+// except for the first chunk and the last slab.  Reference-compatible windows that change
+// the result need the whole volume as one problem (their tiling starts at volStart).
 extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kernelMode,
                                     const float* projections, float* volume)
 {
   if (!g0 || !projections || !volume) return set_error(FCB_ERR_INVALID, "NULL argument");
+  HostTrace tr;
   DeviceGuard guard(device);
   if (guard.rc) return guard.rc;
   fcb_geometry g = *g0;
   if (kernelMode != 0) g.misAlignments = nullptr;
   const int W = g.projWHSize[0], H = g.projWHSize[1], n = g.projDim[2];
   if (W <= 0 || H <= 0 || n <= 0) return set_error(FCB_ERR_INVALID, "bad projection sizes");
+  for (int a = 0; a < 3; a++)
+    if (g.volEnd[a] <= g.volStart[a]) return set_error(FCB_ERR_INVALID, "empty volume range");
   if (g.referenceWindows) {
     // the reference's windows depend on the data width: decide on the caller's geometry,
     // and leave the rows unpadded when the windows change the result
@@ -127,44 +150,105 @@ extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kern
   }
   // TMA row pitch must be a multiple of 16 bytes
   const int wpad = g.referenceWindows ? W : (W + 3) & ~3;
-  g.projWHSize[0] = wpad;         // zero columns beyond W change nothing (zero extension)
-  const int chunk = 120;
-  fcb_bp_plan* plan = nullptr;
-  FCB_TRY(bp_plan_create_ex(&g, kernelMode, FCB_F32, chunk, &plan));
-  struct PlanGuard {
-    fcb_bp_plan* p;
-    ~PlanGuard() { fcb_bp_plan_destroy(p); }
-  } pg{plan};
-  std::vector<std::pair<int, int>> ranges;
-  FCB_TRY(bp_plan_chunks(plan, &ranges));
+  g.projWHSize[0] = wpad;  // zero columns beyond W change nothing (zero extension)
 
-  const size_t nvox = (size_t)(g.volEnd[0] - g.volStart[0]) * (g.volEnd[1] - g.volStart[1]) *
-                      (g.volEnd[2] - g.volStart[2]);
+  // z-slabs: multiples of 32 planes (the kernel's z tile), at least 64 deep, at most 8
+  const int nx = g.volEnd[0] - g.volStart[0], ny = g.volEnd[1] - g.volStart[1],
+            nz = g.volEnd[2] - g.volStart[2];
+  int nslab = g.referenceWindows ? 1 : std::max(1, std::min(8, nz / 64));
+  const int slab = ((nz + nslab - 1) / nslab + 31) / 32 * 32;
+  nslab = (nz + slab - 1) / slab;
+  const int chunk = 120;  // views per upload chunk (slab 0 follows the upload chunk by chunk)
+
+  struct PlanSet {
+    std::vector<fcb_bp_plan*> p;
+    ~PlanSet()
+    {
+      for (fcb_bp_plan* q : p) fcb_bp_plan_destroy(q);
+    }
+  } plans;
+  std::vector<int> z0(nslab), z1(nslab);
+  for (int s = 0; s < nslab; s++) {
+    z0[s] = g.volStart[2] + s * slab;
+    z1[s] = std::min(g.volEnd[2], z0[s] + slab);
+    fcb_geometry gs = g;
+    gs.volStart[2] = z0[s];
+    gs.volEnd[2] = z1[s];
+    fcb_bp_plan* pl = nullptr;
+    FCB_TRY(bp_plan_create_ex(&gs, kernelMode, FCB_F32, s == 0 ? chunk : 1 << 30, &pl));
+    plans.p.push_back(pl);
+  }
+  std::vector<std::pair<int, int>> ranges;
+  FCB_TRY(bp_plan_chunks(plans.p[0], &ranges));
+  const double t_plan = tr.ms();
+
+  const size_t plane = (size_t)nx * ny;
+  const size_t nvox = plane * nz;
   Scratch sc;
   float *dvol = nullptr, *dproj = nullptr;
   FCB_TRY(sc.alloc((void**)&dvol, nvox * sizeof(float)));
   FCB_TRY(sc.alloc((void**)&dproj, (size_t)n * H * wpad * sizeof(float)));
-  if (wpad != W)
-    FCB_CUDA_TRY(cudaMemset(dproj, 0, (size_t)n * H * wpad * sizeof(float)));
-  cudaStream_t cs, xs;
+  const double t_alloc = tr.ms();
+  cudaStream_t cs, xs, os;
   FCB_TRY(sc.stream(&cs));
   FCB_TRY(sc.stream(&xs));
-  cudaEvent_t evVol;
-  FCB_TRY(sc.event(&evVol));
-  FCB_CUDA_TRY(cudaMemcpyAsync(dvol, volume, nvox * sizeof(float), cudaMemcpyHostToDevice, xs));
-  FCB_CUDA_TRY(cudaEventRecord(evVol, xs));
-  FCB_CUDA_TRY(cudaStreamWaitEvent(cs, evVol, 0));
+  FCB_TRY(sc.stream(&os));
+  if (wpad != W) FCB_CUDA_TRY(cudaMemsetAsync(dproj, 0, (size_t)n * H * wpad * sizeof(float), xs));
+  auto slab_ptr = [&](float* base, int s) { return base + (size_t)(z0[s] - g.volStart[2]) * plane; };
+  auto slab_bytes = [&](int s) { return (size_t)(z1[s] - z0[s]) * plane * sizeof(float); };
+  cudaEvent_t ev;
+  std::vector<cudaEvent_t> done(nslab);
+  for (int s = 0; s < nslab; s++) FCB_TRY(sc.event(&done[s]));
+  cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (tr.on)
+    for (cudaEvent_t& e : tev) FCB_CUDA_TRY(cudaEventCreate(&e));
+  if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[0], xs));
+
+  // slab 0 and the projections
+  FCB_CUDA_TRY(cudaMemcpyAsync(slab_ptr(dvol, 0), slab_ptr(volume, 0), slab_bytes(0),
+                               cudaMemcpyHostToDevice, xs));
   for (size_t c = 0; c < ranges.size(); c++) {
-    cudaEvent_t ev;
-    FCB_TRY(sc.event(&ev));
     FCB_TRY(copy_proj_h2d(dproj, projections, ranges[c].first, ranges[c].second, W, H, wpad, xs));
+    FCB_TRY(sc.event(&ev));
     FCB_CUDA_TRY(cudaEventRecord(ev, xs));
     FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
-    FCB_TRY(bp_plan_execute_chunk(plan, (int)c, dproj, dvol, cs));
+    if (c == 0 && tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[1], cs));
+    FCB_TRY(bp_plan_execute_chunk(plans.p[0], (int)c, dproj, slab_ptr(dvol, 0), cs));
   }
-  FCB_CUDA_TRY(cudaMemcpyAsync(volume, dvol, nvox * sizeof(float), cudaMemcpyDeviceToHost, cs));
+  FCB_CUDA_TRY(cudaEventRecord(done[0], cs));
+  // the other slabs: volume in (copy-in stream), backprojection, volume out (copy-out)
+  for (int s = 1; s < nslab; s++) {
+    FCB_CUDA_TRY(cudaMemcpyAsync(slab_ptr(dvol, s), slab_ptr(volume, s), slab_bytes(s),
+                                 cudaMemcpyHostToDevice, xs));
+    FCB_TRY(sc.event(&ev));
+    FCB_CUDA_TRY(cudaEventRecord(ev, xs));
+    FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
+    FCB_TRY(bp_plan_execute_chunk(plans.p[s], -1, dproj, slab_ptr(dvol, s), cs));
+    FCB_CUDA_TRY(cudaEventRecord(done[s], cs));
+    FCB_CUDA_TRY(cudaStreamWaitEvent(os, done[s - 1], 0));
+    FCB_CUDA_TRY(cudaMemcpyAsync(slab_ptr(volume, s - 1), slab_ptr(dvol, s - 1), slab_bytes(s - 1),
+                                 cudaMemcpyDeviceToHost, os));
+  }
+  if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[2], cs));
+  FCB_CUDA_TRY(cudaStreamWaitEvent(os, done[nslab - 1], 0));
+  FCB_CUDA_TRY(cudaMemcpyAsync(slab_ptr(volume, nslab - 1), slab_ptr(dvol, nslab - 1),
+                               slab_bytes(nslab - 1), cudaMemcpyDeviceToHost, os));
+  if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[3], os));
+  FCB_CUDA_TRY(cudaStreamSynchronize(os));
   FCB_CUDA_TRY(cudaStreamSynchronize(cs));
   FCB_TRY(collect_device_status(cs));
+  if (tr.on) {
+    float a = 0, b = 0, c = 0;
+    cudaEventElapsedTime(&a, tev[0], tev[1]);
+    cudaEventElapsedTime(&b, tev[0], tev[2]);
+    cudaEventElapsedTime(&c, tev[0], tev[3]);
+    fprintf(stderr,
+            "fcb_backproject_host: %d slab(s) of %d planes, %zu view chunks; plans %.1f ms, "
+            "alloc %.1f ms; first kernel at %.1f ms, kernels done %.1f ms, volume home %.1f ms "
+            "(GPU clock from the first copy); call %.1f ms\n",
+            nslab, slab, ranges.size(), t_plan, t_alloc - t_plan, a, b, c, tr.ms());
+    for (cudaEvent_t e : tev) cudaEventDestroy(e);
+  }
   return ok();
 }
 
