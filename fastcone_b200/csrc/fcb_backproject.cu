@@ -208,7 +208,12 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
   return r;
 }
 
-template <typename T, int NZ, bool PIW, bool X2, int MINB = 1>
+// Resident CTAs per SM the register allocation must allow: 3 (the default 64 KB staging
+// budget fits 3 CTAs) unless NZ = 64 needs the registers of 2.
+template <int NZ>
+constexpr int fdk_min_blocks() { return NZ >= 64 ? 2 : 3; }
+
+template <typename T, int NZ, bool PIW, bool X2, int MINB = fdk_min_blocks<NZ>()>
 __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid_constant__ CUtensorMap tmap,
                                                               const __grid_constant__ FdkParams P)
 {
@@ -536,7 +541,7 @@ struct fcb_bp_plan {
 
 namespace {
 
-template <typename T, int NZ, bool PIW, bool X2, int MINB = 1>
+template <typename T, int NZ, bool PIW, bool X2, int MINB = fdk_min_blocks<NZ>()>
 int launch_fdk(const fcb_bp_plan* pl, const CUtensorMap& map, int chunk, cudaStream_t st)
 {
   const size_t stage_bytes = ((size_t)pl->BW * pl->BH * sizeof(T) + 127) & ~(size_t)127;
