@@ -39,6 +39,24 @@ VOXEL_MM, PITCH_MM, SOD_MM, SDD_MM = 0.25, 0.4, 500.0, 1000.0
 FDK_BYTES_PER_UPDATE = {"f32": 16, "bf16": 8}  # bilinear gather: 4 detector samples
 
 
+# DRAM bytes per FDK launch (1024^3, <= 900 views): ncu dram__bytes_read.sum +
+# dram__bytes_write.sum of the 128-plane / 64-view slab capture
+# (profiles/fdk_tma_kernel_fdk-slab.md), scaled per component: the volume read-modify-write
+# with the voxels (x8), the staged detector rows with voxels x views (x8 x 720 / 64 for the
+# mean launch of 720 views).
+FDK_TRAFFIC_PER_LAUNCH = round((2 * 0.540e9) * 8 + 0.123e9 * 8 * 720 / 64)
+FDK_TRAFFIC_NOTE = "scaled from the ncu slab capture (volume x8, detector rows x8 x 720/64 views)"
+
+
+def smem_roofline(gather_gbs, clocks):
+    """The binding ceiling of the FDK kernel: 4 ld.shared per voxel-view update, one 128-byte
+    wavefront per warp instruction -> 128 B/clk/SM of gather bytes on 148 SMs."""
+    mhz = clocks.get("sm_mhz") or 1965.0
+    peak = 128.0 * 148 * mhz * 1e6 / 1e9
+    return {"bound": "smem", "achieved": gather_gbs, "peak": peak, "unit": "GB/s", "frac": gather_gbs / peak,
+            "clock_mhz": mhz, "note": "peak = 128 B/clk/SM x 148 SMs x median sampled SM clock"}
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -47,7 +65,11 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--case", default=None, choices=["fdk-slab", "fdk-slab-bf16", "proj-512"],
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--shard", default="replicas", choices=["replicas", "z"],
+                    help="N>1: independent volumes per rank (weak scaling) or one volume in z-slabs "
+                         "(strong scaling)")
+    ap.add_argument("--case", default=None, choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "conv-256"],
                     help="profiling case: run only this kernel on a reduced workload (no JSON line)")
     return ap.parse_args()
 
@@ -56,7 +78,10 @@ def run_case(args):
     """Reduced single-kernel workloads for ncu captures (a few GB on the device):
     fdk-slab[-bf16]: the 1024^3 geometry restricted to a 1024x1024x128 z-slab (z 448..575),
     64 views (0.5 GB volume + 0.4 GB projections);
-    proj-512: both projectors on 512^3, 90 views, 768x512 detector (0.5 GB volume)."""
+    proj-512: the staged, unstaged and texture projectors on 512^3, 90 views, 768x512
+    detector (0.5 GB volume);
+    conv-256: one unrolled step's convolutions at 256^3 x 16 BF16 channels (0.54 GB per
+    activation): forward, input gradient (tensor cores) and weight gradient."""
     import numpy as np
     import torch
 
@@ -87,24 +112,51 @@ def run_case(args):
         ms = e0.elapsed_time(e1) / args.steps
         upd = 1024 * 1024 * 128 * n
         print(json.dumps({"case": args.case, "ms": ms, "GUPS": upd / ms / 1e6, "box": plan.info()}))
+    elif args.case == "conv-256":
+        from fastcone_b200 import nn
+
+        gen = torch.Generator(device=dev).manual_seed(0)
+        x = torch.randn((256, 256, 256, 16), device=dev, generator=gen).to(torch.bfloat16)
+        wk = (0.05 * torch.randn((27, 16, 16), device=dev, generator=gen)).to(torch.bfloat16)
+        b = torch.zeros(16, device=dev)
+        res = {}
+        for name, fn in (("fwd", lambda: nn.conv3d16(x, wk, b, relu=True)),
+                         ("wgrad", lambda: nn.conv3d16_wgrad(x, x))):
+            for _ in range(args.warmup):
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / args.steps
+            flop = 2.0 * 16 * 27 * 16 * 256 ** 3
+            res[name] = {"ms": ms, "TFLOP/s": flop / ms / 1e9}
+        print(json.dumps({"case": args.case, **res}))
     else:
         g = ConeGeometry.circular((512, 512, 512), 1.0, (768, 512), 1.0, 1000.0, 2000.0, 90)
         from fastcone_b200.phantom import random_ellipsoids
 
         v = ops.phantom(g.vol_xyz, random_ellipsoids(10, g.vol_xyz, 1), device=dev)
-        for _ in range(args.warmup + args.steps):
-            ops.project(v, g, method=_lib.PROJ_EXPLICIT)
-            ops.project(v, g, method=_lib.PROJ_TEXTURE)
+        res = {}
+        for name, meth in (("explicit", _lib.PROJ_EXPLICIT), ("explicit_unstaged", _lib.PROJ_EXPLICIT_GLOBAL),
+                           ("texture", _lib.PROJ_TEXTURE)):
+            plan = ops.ProjectPlan(g, meth)
+            p = plan(v)
+            for _ in range(args.warmup):
+                plan(v, p)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(args.steps):
+                plan(v, p)
+            e1.record()
+            torch.cuda.synchronize()
+            res[name] = {"ms": e0.elapsed_time(e1) / args.steps, **(plan.info() if meth == _lib.PROJ_EXPLICIT else {})}
+        print(json.dumps({"case": args.case, **res}))
     ops.sync_status()
     torch.cuda.synchronize()
     print("case", args.case, "done")
-
-
-def dist_env():
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return rank, world, local
 
 
 def measured_peaks():
@@ -225,7 +277,9 @@ def run_reference(args, rank, world):
 
 def main():
     args = parse()
-    rank, world, local = dist_env()
+    from fastcone_b200.dist import env_ranks
+
+    rank, world, local = env_ranks()
     if args.case:
         run_case(args)
         return
@@ -238,33 +292,29 @@ def main():
     from fastcone_b200 import _lib, ops
     from fastcone_b200.geometry import ConeGeometry
 
+    from fastcone_b200 import dist as fd
+
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+    fd.init("nccl", device=dev)
 
     def barrier_max(x):
-        if world == 1:
-            return x
-        import torch.distributed as dist
+        return fd.max_over_ranks(x, dev)
 
-        t = torch.tensor([x], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
+    barrier = fd.barrier
 
     g = geometry()
+    if args.shard == "z":
+        # one volume split into z-slabs, one per rank (strong scaling): each rank owns the
+        # planes [z0, z1) and backprojects them from all projections
+        import dataclasses
+
+        z0, z1 = fd.z_slab(VOL[2], world, rank)
+        g = dataclasses.replace(g, vol_start=(0, 0, z0), vol_end=(VOL[0], VOL[1], max(z1, z0 + 1)))
+    # work of the whole job per step: every rank's volume (replicas) or the one volume (z)
     updates = VOL[0] * VOL[1] * VOL[2] * NVIEWS
+    job_updates = updates * (world if args.shard == "replicas" else 1)
+    updates = g.vol_shape[0] * g.vol_shape[1] * g.vol_shape[2] * NVIEWS  # this rank's
     gen = torch.Generator(device=dev)
     gen.manual_seed(1234 + rank)
     proj = torch.randn((NVIEWS, DET[1], DET[0]), device=dev, dtype=torch.float32, generator=gen)
@@ -290,12 +340,14 @@ def main():
         torch.cuda.synchronize()
         barrier()
     ops.sync_status()
+    clk_summary = clk.summary()
     ms = e0.elapsed_time(e1)
     ms = barrier_max(ms)
     ms_step = ms / args.steps
-    value = world * updates / (ms_step / 1e3) / 1e9
+    value = job_updates / (ms_step / 1e3) / 1e9
 
     hbm, peak_kind = measured_peaks()
+    # per launch: the step's launches split the views; bytes and time both scale with views
     achieved = FDK_BYTES_PER_UPDATE["f32"] * updates / (ms_step / 1e3) / 1e9
 
     # BF16-stored filtered projections (same kernel family, 2-byte gathers)
@@ -326,7 +378,8 @@ def main():
     torch.cuda.synchronize()
     nsamp = int(ctr.item())
     proj_res = {}
-    for name, meth in (("explicit", _lib.PROJ_EXPLICIT), ("texture", _lib.PROJ_TEXTURE)):
+    for name, meth in (("explicit", _lib.PROJ_EXPLICIT), ("explicit_unstaged", _lib.PROJ_EXPLICIT_GLOBAL),
+                       ("texture", _lib.PROJ_TEXTURE)):
         for _ in range(2):
             pp.zero_()
             ops.project(pv, gp, method=meth, proj=pp)
@@ -339,6 +392,29 @@ def main():
         proj_res[name] = nsamp / (e0.elapsed_time(e1) / 3 / 1e3) / 1e9
     del pv, pp
 
+    # learned unrolled reconstruction vs SIRT-100 (committed weights), two held-out phantoms
+    learned_res = None
+    wpath = os.path.join(ROOT, "fastcone_b200", "weights", "unrolled8.pt")
+    if not args.no_learned and rank == 0 and os.path.exists(wpath):
+        from fastcone_b200 import learned
+
+        net = learned.UnrolledNet().to(dev)
+        net.load_state_dict(torch.load(wpath, map_location=dev)["model"])
+        r = learned.evaluate(net, configs.learned_sparse(), seeds=[1, 2], sirt_iters=100)
+        mean = lambda k: sum(x[k] for x in r) / len(r)  # noqa: E731
+        sp = [x["speedup_to_sirt_psnr"] for x in r]
+        learned_res = {
+            "workload": "256^3, 90 views, 384x256, Poisson I0=1e4; 8 unrolled steps vs SIRT-100 from zero",
+            "sirt100_psnr": mean("sirt_psnr"), "sirt100_ssim": mean("sirt_ssim"), "sirt100_s": mean("sirt_time_s"),
+            "learned_psnr": mean("learned_psnr"), "learned_ssim": mean("learned_ssim"),
+            "learned_s": mean("learned_time_s"), "fdk_psnr": mean("fdk_psnr"),
+            "fallback_psnr": mean("no_net_psnr"),
+            "time_to_sirt100_psnr_s": [x["time_to_sirt_psnr_s"] for x in r],
+            "speedup_to_sirt100_psnr": sp,
+        }
+        del net
+        torch.cuda.empty_cache()
+
     # end to end through the reference-facing C entry point, pinned host buffers
     e2e = None
     if not args.no_e2e:
@@ -349,7 +425,7 @@ def main():
         hvol = torch.zeros(g.vol_shape, dtype=torch.float32, pin_memory=True)
         L = _lib.lib()
         i32 = lambda a: np.ascontiguousarray(np.asarray(a, np.int32))
-        volDim, volStart, volEnd = i32(VOL), i32([0, 0, 0]), i32(VOL)
+        volDim, volStart, volEnd = i32(VOL), i32(g.vol_start), i32(g.vol_end)
         projDim, whs = i32([DET[0], DET[1], NVIEWS]), i32(DET)
         woff = i32(np.zeros(NVIEWS)); hoff = i32(np.zeros(NVIEWS))
         fp = lambda a: a.ctypes.data_as(_lib.c_float_p)
@@ -369,7 +445,7 @@ def main():
         for _ in range(ke):
             call()
         dt = barrier_max(time.perf_counter() - t0) / ke
-        e2e = {"value": world * updates / dt / 1e9, "unit": UNIT,
+        e2e = {"value": job_updates / dt / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": hproj.numel() * 4 + hvol.numel() * 4,
                "d2h_bytes_per_step": hvol.numel() * 4, "ms_per_step": dt * 1e3,
                "path": "GPU_CB_K_backproject (C ABI), pinned host buffers"}
@@ -384,25 +460,31 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    scaling = "weak" if args.shard == "replicas" else "strong"
+    parallelism = f"replicas x{world}" if args.shard == "replicas" else f"z-slabs x{world}"
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": scaling,
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "circular FDK backprojection 1024^3 voxels, 1440 views, 1536x1024 detector, "
                                "FP32 filtered projections in HBM",
                    "voxel_view_updates_per_step": updates, "D_voxels": g.D, "pw_voxels": g.pw,
                    "l2": "inputs (13.4 GB) larger than L2; no flush", "box": [info["box_w"], info["box_h"]],
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": parallelism},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
-                     "note": f"achieved = 16 B/update bilinear gather bytes / kernel time; peak {peak_kind} "
-                             f"HBM copy bandwidth; the gathers are served from shared memory"},
-        "bf16_storage": {"value": world * updates / (ms16 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms16},
+                     "frac": achieved / hbm, "traffic": FDK_TRAFFIC_PER_LAUNCH,
+                     "note": f"achieved = 16 B/update bilinear gather bytes per launch / launch time "
+                             f"(CUDA events); peak = {peak_kind} HBM copy bandwidth. frac > 1: the gathers "
+                             f"are served from shared memory (TMA-staged boxes), see smem_roofline; "
+                             f"traffic = DRAM bytes per launch, {FDK_TRAFFIC_NOTE}"},
+        "smem_roofline": smem_roofline(achieved, clk_summary),
+        "bf16_storage": {"value": job_updates / (ms16 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms16},
         "fwd_proj": {"unit": "Gsamples/s", "samples_per_pass": nsamp,
                      "workload": "256^3, 360 views, 384x256 detector",
                      **{k: v for k, v in proj_res.items()}},
-        "clocks": clk.summary(),
+        "clocks": clk_summary,
+        "learned": learned_res,
         "e2e": e2e,
         "cpu_baseline": cpu,
     }
