@@ -48,6 +48,31 @@ FDK_TRAFFIC_PER_LAUNCH = round((2 * 0.540e9) * 8 + 0.123e9 * 8 * 720 / 64)
 FDK_TRAFFIC_NOTE = "scaled from the ncu slab capture (volume x8, detector rows x8 x 720/64 views)"
 
 
+def pi_window_fraction(g, nvox=4096, seed=0):
+    """Fraction of voxel-view pairs inside the Tam-Danielsson window, estimated on random
+    voxels with the window test of the FP64 Katsevich reference (u = sign * w / D, bounds
+    q (pi/2 -+ atan u), q = P / (2 pi) (1 + u^2), lengths in voxels)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = g.vol_shape
+    xyz = rng.integers(0, [nx, ny, nz], size=(nvox, 3)).astype(np.float64)
+    x = xyz[:, 0:1] - g.vol_xyz[0] // 2
+    y = xyz[:, 1:2] - g.vol_xyz[1] // 2
+    z = xyz[:, 2:3] - g.vol_xyz[2] // 2
+    a = g.angles.astype(np.float64)[None, :]
+    hm = g.hmid.astype(np.float64)[None, :] - g.vol_xyz[2] // 2
+    U = g.D / (g.D + x * np.cos(a) + y * np.sin(a))
+    w = (y * np.cos(a) - x * np.sin(a)) * U
+    h = (z - hm) * U
+    turn = float(g.angles[-1]) - float(g.angles[0])
+    sgn = -1.0 if (turn >= 0) == (g.helical_pitch >= 0) else 1.0
+    u = sgn * w / g.D
+    q = g.helical_pitch / (2 * np.pi) * (1 + u * u)
+    inside = (h <= q * (np.pi / 2 - np.arctan(u))) & (h >= -q * (np.pi / 2 + np.arctan(u)))
+    return float(inside.mean())
+
+
 def smem_roofline(gather_gbs, clocks):
     """The binding ceiling of the FDK kernel: 4 ld.shared per voxel-view update, one 128-byte
     wavefront per warp instruction -> 128 B/clk/SM of gather bytes on 148 SMs."""
@@ -120,7 +145,16 @@ def run_case(args):
         wk = (0.05 * torch.randn((27, 16, 16), device=dev, generator=gen)).to(torch.bfloat16)
         b = torch.zeros(16, device=dev)
         res = {}
+
+        def fwd_simple():
+            os.environ["FCB_CONV_SIMPLE"] = "1"
+            try:
+                return nn.conv3d16(x, wk, b, relu=True)
+            finally:
+                os.environ.pop("FCB_CONV_SIMPLE", None)
+
         for name, fn in (("fwd", lambda: nn.conv3d16(x, wk, b, relu=True)),
+                         ("fwd_one_tile_per_cta", fwd_simple),
                          ("wgrad", lambda: nn.conv3d16_wgrad(x, x))):
             for _ in range(args.warmup):
                 fn()
@@ -380,17 +414,42 @@ def main():
     proj_res = {}
     for name, meth in (("explicit", _lib.PROJ_EXPLICIT), ("explicit_unstaged", _lib.PROJ_EXPLICIT_GLOBAL),
                        ("texture", _lib.PROJ_TEXTURE)):
+        pplan = ops.ProjectPlan(gp, meth)  # geometry, brick sizing, buffers: once
         for _ in range(2):
-            pp.zero_()
-            ops.project(pv, gp, method=meth, proj=pp)
+            pplan(pv, pp)
         torch.cuda.synchronize()
         e0.record(st)
         for _ in range(3):
-            ops.project(pv, gp, method=meth, proj=pp)
+            pplan(pv, pp)
         e1.record(st)
         torch.cuda.synchronize()
         proj_res[name] = nsamp / (e0.elapsed_time(e1) / 3 / 1e3) / 1e9
+        del pplan
     del pv, pp
+
+    # helical Katsevich backprojection with the PI window (512x512x384, 4 turns x 1160 views)
+    gk = configs.helical_katsevich(pi_window=True)
+    pk = torch.randn(gk.proj_shape, device=dev, generator=gen)
+    vk = torch.zeros(gk.vol_shape, device=dev)
+    kplan = ops.BackprojectPlan(gk, mode=_lib.MODE_KATSEVICH, dtype=torch.float32)
+    for _ in range(2):
+        kplan(pk, vk)
+    torch.cuda.synchronize()
+    e0.record(st)
+    kk = 3
+    for _ in range(kk):
+        kplan(pk, vk)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ops.sync_status()
+    ms_k = barrier_max(e0.elapsed_time(e1)) / kk
+    dense = gk.vol_shape[0] * gk.vol_shape[1] * gk.vol_shape[2] * gk.nviews
+    frac = pi_window_fraction(gk)
+    katsevich = {"workload": "helical 512x512x384, 4 turns x 1160 views, 736x64 detector, PI window",
+                 "ms_per_pass": ms_k, "dense_GUPS": dense / (ms_k / 1e3) / 1e9,
+                 "pi_window_pairs_fraction": frac, "pi_window_GUPS": frac * dense / (ms_k / 1e3) / 1e9,
+                 "launches": kplan.info()["launches"]}
+    del pk, vk, kplan
 
     # learned unrolled reconstruction vs SIRT-100 (committed weights), two held-out phantoms
     learned_res = None
@@ -484,6 +543,7 @@ def main():
                      "workload": "256^3, 360 views, 384x256 detector",
                      **{k: v for k, v in proj_res.items()}},
         "clocks": clk_summary,
+        "katsevich": katsevich,
         "learned": learned_res,
         "e2e": e2e,
         "cpu_baseline": cpu,

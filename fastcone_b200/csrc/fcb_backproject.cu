@@ -93,12 +93,13 @@ __device__ __forceinline__ void fdk_tile(const FdkParams& P, int tile, int& tx, 
 // to the TMA 16-byte rule.
 __device__ __forceinline__ void fdk_box_origin(const FdkParams& P, const FdkView& V, int tx,
                                                int ty, int tz, int nzt, int& w0, int& h0,
-                                               int& needw, int& needh)
+                                               int& needw, int& needh, float* fp = nullptr)
 {
   const float x0 = P.ox + tx * FDK_TX, y0 = P.oy + ty * FDK_TY, z0 = P.oz + tz * nzt;
   float wmin, wmax, hmin, hmax;
   fdk_footprint(P, V, x0, x0 + (FDK_TX - 1), y0, y0 + (FDK_TY - 1), z0, z0 + (nzt - 1), wmin,
                 wmax, hmin, hmax);
+  if (fp) { fp[0] = wmin; fp[1] = wmax; fp[2] = hmin; fp[3] = hmax; }
   // clamp far-away footprints so the integer math below stays defined
   wmin = fminf(fmaxf(wmin, -1.0e6f), 1.0e6f); wmax = fminf(fmaxf(wmax, -1.0e6f), 1.0e6f);
   hmin = fminf(fmaxf(hmin, -1.0e6f), 1.0e6f); hmax = fminf(fmaxf(hmax, -1.0e6f), 1.0e6f);
@@ -107,6 +108,27 @@ __device__ __forceinline__ void fdk_box_origin(const FdkParams& P, const FdkView
   h0 = __float2int_rd(hmin) - 1;
   needw = __float2int_rd(wmax) + 3 - w0;
   needh = __float2int_rd(hmax) + 3 - h0;
+}
+
+// Katsevich PI window: true when no voxel of the tile can lie inside the Tam-Danielsson
+// window of the view, so the view is skipped for the tile.  The window bounds are smooth in
+// the detector column; over a tile's few columns their extremes are those at the ends and
+// the middle to well under the 1-pixel margin kept here.
+__device__ __forceinline__ bool fdk_tile_outside_window(const FdkParams& P, const FdkView& V,
+                                                        float wmin, float wmax, float hmin,
+                                                        float hmax)
+{
+  float lo = 3.0e38f, hi = -3.0e38f;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const float w = c == 0 ? wmin : (c == 1 ? 0.5f * (wmin + wmax) : wmax);
+    const float u = (w - V.wc) * P.td_sign / P.td_r;
+    const float q = P.td_a * (1.0f + u * u);
+    const float at = atanf(u);
+    hi = fmaxf(hi, V.hc + q * (1.5707963267948966f - at));
+    lo = fminf(lo, V.hc - q * (1.5707963267948966f + at));
+  }
+  return hmin > hi + 1.0f || hmax < lo - 1.0f;
 }
 
 // Pre-pass: the largest footprint over all (tile, view) pairs sizes the staging box.
@@ -223,7 +245,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   const int stage_bytes = ((stage_elems * ES) + 127) & ~127;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)P.stages * stage_bytes);
   uint64_t* empty = full + P.stages;
-  int2* origin = reinterpret_cast<int2*>(empty + P.stages);
+  int4* origin = reinterpret_cast<int4*>(empty + P.stages);  // box origin w, h; view (-1: end)
   const uint32_t smem_base = dev::smem_u32(smem_raw);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -244,29 +266,42 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
     if (lane != 0) return;
     dev::tma_prefetch(&tmap);
     const uint32_t bytes = (uint32_t)(stage_elems * ES);
-    int issued = 0;
+    int issued = 0;  // staged views so far (= ring position)
     bool failed = false;
     for (int v = 0; v < P.nviews; v++) {
-      const int s = v % P.stages;
-      if (v >= P.stages) {
-        if (!dev::mbar_wait(&empty[s], ((v / P.stages) - 1) & 1)) {
+      int w0, h0, nw, nh;
+      float fp[4];
+      fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, w0, h0, nw, nh, fp);
+      // with the PI window, views that cannot reach the tile are not staged at all
+      if (PIW && fdk_tile_outside_window(P, P.v[v], fp[0], fp[1], fp[2], fp[3])) continue;
+      const int s = issued % P.stages;
+      if (issued >= P.stages) {
+        if (!dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
           failed = true;
           break;
         }
       }
-      int w0, h0, nw, nh;
-      fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, w0, h0, nw, nh);
       if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
-      origin[s] = make_int2(w0, h0);
+      origin[s] = make_int4(w0, h0, v, 0);
       dev::mbar_arrive_expect_tx(&full[s], bytes);
       dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + v);
-      issued = v + 1;
+      issued++;
+    }
+    if (PIW && !failed) {
+      // end of the view list: a slot whose phase completes without data, view -1
+      const int s = issued % P.stages;
+      if (issued < P.stages || dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
+        origin[s] = make_int4(0, 0, -1, 0);
+        dev::mbar_arrive(&full[s]);
+      } else {
+        failed = true;
+      }
     }
     if (failed) {
       dev::record_status(P.status, DEV_TIMEOUT);
       // drain: wait (bounded) for the copies still in flight before leaving
-      for (int v = max(0, issued - P.stages); v < issued; v++)
-        dev::mbar_wait(&full[v % P.stages], (v / P.stages) & 1, 100000000ull);
+      for (int j = max(0, issued - P.stages); j < issued; j++)
+        dev::mbar_wait(&full[j % P.stages], (j / P.stages) & 1, 100000000ull);
     }
     return;
   }
@@ -290,14 +325,18 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
     else acc[k] = 0.0f;
   }
 
-  for (int v = 0; v < P.nviews; v++) {
-    const int s = v % P.stages;
-    if (!dev::mbar_wait(&full[s], (v / P.stages) & 1)) {
+  // ring position j carries view j (all views staged) or the view the producer chose (PI
+  // window: only views that reach the tile, then an end marker)
+  for (int j = 0; PIW || j < P.nviews; j++) {
+    const int s = j % P.stages;
+    if (!dev::mbar_wait(&full[s], (j / P.stages) & 1)) {
       dev::record_status(P.status, DEV_TIMEOUT);
       return;
     }
+    const int4 org = origin[s];
+    const int v = PIW ? org.z : j;
+    if (PIW && v < 0) break;
     const FdkView& V = P.v[v];
-    const int2 org = origin[s];
 
     const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
     const float U = __frcp_rn(den);
@@ -545,7 +584,7 @@ template <typename T, int NZ, bool PIW, bool X2, int MINB = fdk_min_blocks<NZ>()
 int launch_fdk(const fcb_bp_plan* pl, const CUtensorMap& map, int chunk, cudaStream_t st)
 {
   const size_t stage_bytes = ((size_t)pl->BW * pl->BH * sizeof(T) + 127) & ~(size_t)127;
-  const size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int2));
+  const size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int4));
   auto kern = fdk_tma_kernel<T, NZ, PIW, X2, MINB>;
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int c = 0; c < (int)pl->fdk.size(); c++) {

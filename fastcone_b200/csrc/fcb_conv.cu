@@ -12,9 +12,10 @@
 // warps read their TMEM lane quadrant back (tcgen05.ld 32x32b.x16), add the bias, apply
 // ReLU and store.
 //
-// The same kernel computes the input gradient (transposed, tap-flipped weights, prepared by
-// the caller).  The weight gradient, a 6912-entry reduction over all voxels, runs on the
+// The same kernels compute the input gradient (transposed, tap-flipped weights, prepared by
+// the caller).  conv3d16p_kernel is the persistent, pipelined form used by default.  The weight gradient, a 6912-entry reduction over all voxels, runs on the
 // CUDA cores (fcb_conv3d16_wgrad_device).
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -227,6 +228,180 @@ __global__ void __launch_bounds__(128) conv3d16_kernel(const __grid_constant__ C
   if (warp == 0) tc::tmem_dealloc(taddr, 32);
 }
 
+// Persistent, pipelined form of the same convolution: one CTA per SM walks the row tiles
+// (tile = blockIdx.x + i * gridDim.x) with warp-specialised roles --
+//   warp 4 (one lane): TMA producer, 18 row boxes per tile into a ring of CVP_STAGES buffers;
+//   warp 5 (one lane): MMA issuer, 27 tcgen05.mma per tile into one of two TMEM
+//                       accumulators (16 columns each), commits to the ring's empty barrier
+//                       and to the accumulator's full barrier;
+//   warps 0-3:         epilogue, each reads its 32-lane TMEM quadrant of the finished
+//                       accumulator, releases it, adds bias / ReLU and stores.
+// The weights are staged once per CTA, TMEM is allocated once, and the loads of the next
+// tiles, the MMAs of this one and the stores of the previous one overlap.  Every wait is
+// bounded; a role that times out records the status and stops, and the others stop at their
+// next (bounded) wait.
+constexpr int CVP_STAGES = 4;
+constexpr int CVP_THREADS = 192;
+constexpr int CVP_SMEM = CVP_STAGES * CV_A_BYTES + CV_W_BYTES + 64 + 8 * (2 * CVP_STAGES + 4) + 16;
+
+__global__ void __launch_bounds__(CVP_THREADS, 1) conv3d16p_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                                  const __grid_constant__ ConvParams P,
+                                                                  int ntiles)
+{
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* A = smem;
+  unsigned char* Wsm = smem + CVP_STAGES * CV_A_BYTES;
+  float* bias = reinterpret_cast<float*>(Wsm + CV_W_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(Wsm + CV_W_BYTES + 64);
+  uint64_t* empty = full + CVP_STAGES;
+  uint64_t* accf = empty + CVP_STAGES;  // [2] accumulator written (MMA commit)
+  uint64_t* acce = accf + 2;            // [2] accumulator read (4 epilogue warps)
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nmine = blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < CVP_STAGES; s++) {
+      dev::mbar_init(&full[s], 1);
+      dev::mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      dev::mbar_init(&accf[b], 1);
+      dev::mbar_init(&acce[b], 4);
+    }
+    dev::fence_mbar_init();
+  }
+  if (warp == 5) {
+    tc::tmem_alloc(tslot, 32);
+    tc::tmem_relinquish();
+  }
+  const uint4* wg = reinterpret_cast<const uint4*>(P.w);
+  for (int i = threadIdx.x; i < 27 * 16 * 2; i += blockDim.x) {
+    const int t = i / 32, n = (i / 2) % 16, kh = i % 2;
+    reinterpret_cast<uint4*>(Wsm + t * 512 + kh * 256 + n * 16)[0] = wg[(t * 16 + n) * 2 + kh];
+  }
+  if (threadIdx.x < 16) bias[threadIdx.x] = P.bias ? P.bias[threadIdx.x] : 0.0f;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t taddr = *tslot;
+
+  if (warp == 4) {
+    // ---------------------------------------------------------------- TMA producer
+    if (lane == 0) {
+      dev::tma_prefetch(&xmap);
+      int issued = 0;
+      for (int i = 0; i < nmine; i++) {
+        const int s = i % CVP_STAGES;
+        if (i >= CVP_STAGES && !dev::mbar_wait(&empty[s], ((i / CVP_STAGES) - 1) & 1)) {
+          dev::record_status(P.status, DEV_TIMEOUT);
+          break;
+        }
+        issued = i + 1;
+        const int tile = blockIdx.x + i * gridDim.x;
+        const int x0 = (tile % P.tiles_x) * CV_TILE;
+        const int yz = tile / P.tiles_x;
+        const int y = yz % P.ny, z = yz / P.ny;
+        unsigned char* As = A + s * CV_A_BYTES;
+        dev::mbar_arrive_expect_tx(&full[s], 18u * CV_BOX_BYTES);
+        for (int r = 0; r < 9; r++) {
+          const int dz = r / 3, dy = r % 3;
+          for (int kh = 0; kh < 2; kh++)
+            tc::tma_load_4d(As + (r * 2 + kh) * CV_RB, &xmap, &full[s], kh * 8, x0 - 1, y + dy - 1, z + dz - 1);
+        }
+      }
+      // no copy may still be landing in shared memory when the CTA leaves (bounded waits;
+      // immediate unless another role stopped early)
+      for (int j = max(0, issued - CVP_STAGES); j < issued; j++)
+        dev::mbar_wait(&full[j % CVP_STAGES], (j / CVP_STAGES) & 1, 100000000ull);
+    }
+  } else if (warp == 5) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t wbase = dev::smem_u32(Wsm);
+      constexpr uint32_t IDESC = tc::idesc_bf16(CV_TILE, 16);
+      for (int i = 0; i < nmine; i++) {
+        const int s = i % CVP_STAGES, b = i & 1;
+        if (!dev::mbar_wait(&full[s], (i / CVP_STAGES) & 1) ||
+            (i >= 2 && !dev::mbar_wait(&acce[b], ((i >> 1) - 1) & 1))) {
+          dev::record_status(P.status, DEV_TIMEOUT);
+          break;
+        }
+        tc::fence_after();
+        const uint32_t abase = dev::smem_u32(A + s * CV_A_BYTES);
+        for (int t = 0; t < 27; t++) {
+          const int r = t / 3, dx = t % 3;
+          const uint64_t ad = tc::smem_desc(abase + r * 2 * CV_RB + dx * 16, CV_RB, 128);
+          const uint64_t bd = tc::smem_desc(wbase + t * 512, 256, 128);
+          tc::mma_bf16(taddr + (uint32_t)(b * 16), ad, bd, IDESC, t > 0 ? 1u : 0u);
+        }
+        tc::mma_commit(&empty[s]);
+        tc::mma_commit(&accf[b]);
+      }
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue (warps 0-3)
+    for (int i = 0; i < nmine; i++) {
+      const int b = i & 1;
+      // warp-uniform: tcgen05.ld below is a warp-collective instruction
+      if (!__all_sync(0xffffffffu, dev::mbar_wait(&accf[b], (i >> 1) & 1))) {
+        if (lane == 0) dev::record_status(P.status, DEV_TIMEOUT);
+        break;
+      }
+      tc::fence_after();
+      uint32_t r[16];
+      tc::tmem_ld16(taddr + (uint32_t)(b * 16) + ((uint32_t)(warp * 32) << 16), r);
+      tc::fence_before();
+      __syncwarp();
+      if (lane == 0) dev::mbar_arrive(&acce[b]);
+      const int tile = blockIdx.x + i * gridDim.x;
+      const int x0 = (tile % P.tiles_x) * CV_TILE;
+      const int yz = tile / P.tiles_x;
+      const int y = yz % P.ny, z = yz / P.ny;
+      const int xv = x0 + warp * 32 + lane;
+      if (xv < P.nx) {
+        float v[16];
+#pragma unroll
+        for (int c = 0; c < 16; c++) {
+          v[c] = __uint_as_float(r[c]) + bias[c];
+          if (P.relu) v[c] = fmaxf(v[c], 0.0f);
+        }
+        const size_t vox = ((size_t)z * P.ny + y) * P.nx + xv;
+        if (P.out_f32) {
+          float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + vox * 16);
+#pragma unroll
+          for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        } else {
+          uint32_t pk[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            __nv_bfloat162 bb = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+            pk[q] = *reinterpret_cast<uint32_t*>(&bb);
+          }
+          uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(P.out) + vox * 16);
+          o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        }
+      }
+    }
+  }
+  // all MMAs this CTA issued must be complete before the columns are released: the
+  // epilogue waited for every accumulator commit, and the issuer waits (bounded) for its last
+  // one in case the epilogue stopped early
+  if (warp == 5 && lane == 0 && nmine > 0) {
+    const int last = nmine - 1;
+    dev::mbar_wait(&accf[last & 1], (last >> 1) & 1, 100000000ull);
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    tc::fence_after();
+    tc::tmem_dealloc(taddr, 32);
+  }
+}
+
 // Weight gradient on the CUDA cores: dW[t][co][ci] += sum_v dY[v][co] * X[v + off(t)][ci].
 // Thread (co, ci) slides along a row of 128 voxels keeping the three x-neighbours of each of
 // the 9 tap rows in registers; CTAs loop over tiles and add their 27 partial sums once.
@@ -319,9 +494,22 @@ extern "C" int fcb_conv3d16_device(const void* x, const void* w, const float* bi
   P.nx = nx; P.ny = ny; P.nz = nz;
   P.tiles_x = (nx + CV_TILE - 1) / CV_TILE;
   P.status = status;
-  FCB_CUDA_TRY(cudaFuncSetAttribute(conv3d16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM));
   const long long tiles = (long long)P.tiles_x * ny * nz;
-  conv3d16_kernel<<<(unsigned)tiles, 128, CV_SMEM, st>>>(map, P);
+  if (tiles > 0x7fffffffll) return set_error(FCB_ERR_RANGE, "conv3d volume too large");
+  // FCB_CONV_SIMPLE=1: one CTA per tile without the pipeline (for comparison)
+  const char* env = getenv("FCB_CONV_SIMPLE");
+  const bool simple = env && env[0] == '1';
+  if (simple) {
+    FCB_CUDA_TRY(cudaFuncSetAttribute(conv3d16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM));
+    conv3d16_kernel<<<(unsigned)tiles, 128, CV_SMEM, st>>>(map, P);
+  } else {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    FCB_CUDA_TRY(cudaFuncSetAttribute(conv3d16p_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CVP_SMEM));
+    const int grid = (int)std::min<long long>(tiles, sms);
+    conv3d16p_kernel<<<grid, CVP_THREADS, CVP_SMEM, st>>>(map, P, (int)tiles);
+  }
   FCB_CUDA_TRY(cudaGetLastError());
   return ok();
 }

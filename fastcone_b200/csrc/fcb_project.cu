@@ -137,30 +137,35 @@ __device__ __forceinline__ Tri tri_of(float x, float y, float z)
   return t;
 }
 
+// Trilinear interpolation with zero outside the volume, always in the same FP32 lerp order
+// (x, then y, then z) so that every kernel that takes a sample computes it identically.
+__device__ __forceinline__ float tri_lerp(const Tri& t, float v000, float v100, float v010,
+                                          float v110, float v001, float v101, float v011,
+                                          float v111)
+{
+  const float x00 = fmaf(t.a, v100 - v000, v000), x10 = fmaf(t.a, v110 - v010, v010);
+  const float x01 = fmaf(t.a, v101 - v001, v001), x11 = fmaf(t.a, v111 - v011, v011);
+  const float y0 = fmaf(t.b, x10 - x00, x00), y1 = fmaf(t.b, x11 - x01, x01);
+  return fmaf(t.c, y1 - y0, y0);
+}
+
 __device__ __forceinline__ float tri_fetch(const float* __restrict__ vol, int nx, int ny, int nz,
                                            const Tri& t)
 {
   const size_t sx = 1, sy = nx, sz = (size_t)nx * ny;
   if (t.i >= 0 && t.j >= 0 && t.k >= 0 && t.i + 1 < nx && t.j + 1 < ny && t.k + 1 < nz) {
     const float* p = vol + t.i * sx + t.j * sy + t.k * sz;
-    const float v000 = __ldg(p), v100 = __ldg(p + sx), v010 = __ldg(p + sy), v110 = __ldg(p + sx + sy);
-    const float v001 = __ldg(p + sz), v101 = __ldg(p + sx + sz), v011 = __ldg(p + sy + sz),
-                v111 = __ldg(p + sx + sy + sz);
-    const float x00 = fmaf(t.a, v100 - v000, v000), x10 = fmaf(t.a, v110 - v010, v010);
-    const float x01 = fmaf(t.a, v101 - v001, v001), x11 = fmaf(t.a, v111 - v011, v011);
-    const float y0 = fmaf(t.b, x10 - x00, x00), y1 = fmaf(t.b, x11 - x01, x01);
-    return fmaf(t.c, y1 - y0, y0);
+    return tri_lerp(t, __ldg(p), __ldg(p + sx), __ldg(p + sy), __ldg(p + sx + sy), __ldg(p + sz),
+                    __ldg(p + sx + sz), __ldg(p + sy + sz), __ldg(p + sx + sy + sz));
   }
-  float r = 0.0f;
+  float v[8];
 #pragma unroll
   for (int q = 0; q < 8; q++) {
     const int X = t.i + (q & 1), Y = t.j + ((q >> 1) & 1), Z = t.k + ((q >> 2) & 1);
-    if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
-    const float w = ((q & 1) ? t.a : 1.0f - t.a) * (((q >> 1) & 1) ? t.b : 1.0f - t.b) *
-                    (((q >> 2) & 1) ? t.c : 1.0f - t.c);
-    r = fmaf(w, __ldg(vol + X * sx + Y * sy + Z * sz), r);
+    const bool in = X >= 0 && Y >= 0 && Z >= 0 && X < nx && Y < ny && Z < nz;
+    v[q] = in ? __ldg(vol + X * sx + Y * sy + Z * sz) : 0.0f;
   }
-  return r;
+  return tri_lerp(t, v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]);
 }
 
 __global__ void __launch_bounds__(256) project_explicit_kernel(const __grid_constant__ PjParams P)
@@ -201,9 +206,10 @@ __global__ void __launch_bounds__(256) project_explicit_kernel(const __grid_cons
 // lanes of a warp walk along the brick's contiguous axis (no bank conflicts).
 //
 // Sample positions, weights and the order of the FP32 operations are those of
-// project_explicit_kernel (tri_of / tri_fetch), so the two kernels agree bit for bit: a
-// sample whose taps are not all inside the volume, or not inside the staged brick, is
-// taken from global memory by tri_fetch itself.
+// project_explicit_kernel (tri_of / tri_lerp), so the two kernels agree bit for bit: taps
+// outside the volume are the bricks' zero fill (tri_fetch reads zeros there too), and a
+// sample whose taps are not inside the staged brick is taken from global memory by
+// tri_fetch itself.
 constexpr int PB_W = 32, PB_H = 8;              // rays per CTA: 32 pixels x 8 rows
 constexpr int PB_CWARPS = PB_H;                 // one consumer warp per detector row
 constexpr int PB_THREADS = (PB_CWARPS + 1) * 32;
@@ -303,6 +309,58 @@ __device__ __forceinline__ float lds32(uint32_t a)
   return v;
 }
 
+// The consumer side of one bundle: every sample of this thread's ray, slab by slab, from the
+// staged bricks.  XD: x is the dominant axis (bricks of the y-fastest copy: the brick's
+// contiguous axis is y, its middle axis x).  Returns the ray sum; a timed-out wait records
+// the status and returns what was summed (the caller's store then carries a partial sum
+// that the status flags).
+template <bool XD>
+__device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char* smem_raw,
+                                               uint64_t* full, uint64_t* empty, const int4* origin,
+                                               int nsl, int sgn, const float s[3], const float d[3],
+                                               int m0, int m1)
+{
+  const int lane = threadIdx.x & 31;
+  const uint32_t sbase = dev::smem_u32(smem_raw);
+  const uint32_t rowb = (uint32_t)P.BC * 4u, planeb = rowb * (uint32_t)PB_BD;
+  const uint32_t ox = XD ? rowb : 4u, oy = XD ? 4u : rowb;
+  const int BC1 = P.BC - 1, BZ1 = P.BZ - 1;
+  float acc = 0.0f;
+  int m = m0;
+  for (int k = 0; k < nsl; k++) {
+    const int st = k % P.stages;
+    // warp-uniform outcome, so the warp-wide operations below stay converged
+    if (!__all_sync(0xffffffffu, dev::mbar_wait(&full[st], (k / P.stages) & 1))) {
+      dev::record_status(P.status, DEV_TIMEOUT);
+      return acc;
+    }
+    const int4 o = origin[st];
+    const int alo = o.y, ahi = o.y + PB_T - 1;
+    const uint32_t stb = sbase + (uint32_t)st * (uint32_t)P.stage_bytes;
+    while (m <= m1) {
+      const float mf = (float)m;
+      const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
+      const int idom = XD ? t.i : t.j;
+      if (sgn > 0 ? idom > ahi : idom < alo) break;
+      const int ic = (XD ? t.j : t.i) - o.x, id = idom - alo, iz = t.k - o.z;
+      float val;
+      if ((unsigned)ic < (unsigned)BC1 && (unsigned)id < (unsigned)PB_T && (unsigned)iz < (unsigned)BZ1) {
+        // taps outside the volume are the brick's zero fill
+        const uint32_t p = stb + (uint32_t)iz * planeb + (uint32_t)id * rowb + (uint32_t)ic * 4u;
+        val = tri_lerp(t, lds32(p), lds32(p + ox), lds32(p + oy), lds32(p + ox + oy), lds32(p + planeb),
+                       lds32(p + planeb + ox), lds32(p + planeb + oy), lds32(p + planeb + ox + oy));
+      } else {
+        val = tri_fetch(P.vol, P.nx, P.ny, P.nz, t);
+      }
+      acc += val;
+      m++;
+    }
+    __syncwarp();
+    if (lane == 0) dev::mbar_arrive(&empty[st]);
+  }
+  return acc;
+}
+
 __global__ void __launch_bounds__(PB_THREADS, 1) project_brick_kernel(
     const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmT,
     const __grid_constant__ PjParams P)
@@ -385,51 +443,8 @@ __global__ void __launch_bounds__(PB_THREADS, 1) project_brick_kernel(
   }
 
   // --------------------------------------------------------------- consumer warps
-  const uint32_t sbase = dev::smem_u32(smem_raw);
-  const uint32_t rowb = (uint32_t)P.BC * 4u, planeb = rowb * (uint32_t)PB_BD;
-  const uint32_t ox = B.xdom ? rowb : 4u, oy = B.xdom ? 4u : rowb;
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  float acc = 0.0f;
-  int m = m0;
-  for (int k = 0; k < nsl; k++) {
-    const int st = k % P.stages;
-    // warp-uniform outcome, so the warp-wide operations below stay converged
-    if (!__all_sync(0xffffffffu, dev::mbar_wait(&full[st], (k / P.stages) & 1))) {
-      dev::record_status(P.status, DEV_TIMEOUT);
-      return;
-    }
-    const int4 o = origin[st];
-    const int alo = o.y, ahi = o.y + PB_T - 1;
-    const uint32_t stb = sbase + (uint32_t)st * (uint32_t)P.stage_bytes;
-    while (m <= m1) {
-      const float mf = (float)m;
-      const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
-      const int idom = B.xdom ? t.i : t.j;
-      if (B.sgn > 0 ? idom > ahi : idom < alo) break;
-      const int ic = (B.xdom ? t.j : t.i) - o.x, id = idom - alo, iz = t.k - o.z;
-      const bool inside = t.i >= 0 && t.j >= 0 && t.k >= 0 && t.i + 1 < nx && t.j + 1 < ny &&
-                          t.k + 1 < nz;
-      float val;
-      if (inside && (unsigned)ic < (unsigned)(P.BC - 1) && (unsigned)id < (unsigned)PB_T &&
-          (unsigned)iz < (unsigned)(P.BZ - 1)) {
-        const uint32_t p = stb + (uint32_t)iz * planeb + (uint32_t)id * rowb + (uint32_t)ic * 4u;
-        const float v000 = lds32(p), v100 = lds32(p + ox), v010 = lds32(p + oy),
-                    v110 = lds32(p + ox + oy);
-        const float v001 = lds32(p + planeb), v101 = lds32(p + planeb + ox),
-                    v011 = lds32(p + planeb + oy), v111 = lds32(p + planeb + ox + oy);
-        const float x00 = fmaf(t.a, v100 - v000, v000), x10 = fmaf(t.a, v110 - v010, v010);
-        const float x01 = fmaf(t.a, v101 - v001, v001), x11 = fmaf(t.a, v111 - v011, v011);
-        const float y0 = fmaf(t.b, x10 - x00, x00), y1 = fmaf(t.b, x11 - x01, x01);
-        val = fmaf(t.c, y1 - y0, y0);
-      } else {
-        val = tri_fetch(P.vol, nx, ny, nz, t);
-      }
-      acc += val;
-      m++;
-    }
-    __syncwarp();
-    if (lane == 0) dev::mbar_arrive(&empty[st]);
-  }
+  const float acc = xd ? brick_consume<true>(P, smem_raw, full, empty, origin, nsl, B.sgn, s, d, m0, m1)
+                       : brick_consume<false>(P, smem_raw, full, empty, origin, nsl, B.sgn, s, d, m0, m1);
   if (pix) P.proj[((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl] += V.wt * acc;
   count_samples(P.samples, m1 - m0 + 1);
 }

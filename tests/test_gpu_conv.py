@@ -67,3 +67,24 @@ def test_conv_gradients_vs_torch():
     assert _rel(xin.grad, gx_ref) < 1e-2
     assert _rel(w2.grad, wr.grad) < 1e-2
     assert _rel(b2.grad, br.grad) < 1e-2
+
+
+@pytest.mark.parametrize("shape", [(20, 17, 130), (4, 3, 512), (1, 1, 5), (37, 41, 300)])
+def test_persistent_conv_equals_one_tile_per_cta(shape, monkeypatch):
+    """The persistent pipelined kernel (default) and the one-tile-per-CTA kernel issue the
+    same MMAs in the same order: identical outputs, including when a CTA owns many tiles
+    and when tiles are fewer than SMs."""
+    import torch
+
+    from fastcone_b200 import nn
+
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
+    wk = (torch.randn(27, 16, 16, device="cuda", generator=g) * 0.1).to(torch.bfloat16)
+    b = torch.randn(16, device="cuda", generator=g)
+    monkeypatch.delenv("FCB_CONV_SIMPLE", raising=False)
+    y1 = nn.conv3d16(x, wk, b, relu=True, out_dtype=torch.float32)
+    monkeypatch.setenv("FCB_CONV_SIMPLE", "1")
+    y2 = nn.conv3d16(x, wk, b, relu=True, out_dtype=torch.float32)
+    torch.cuda.synchronize()
+    assert torch.equal(y1, y2)
