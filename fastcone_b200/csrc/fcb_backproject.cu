@@ -49,6 +49,7 @@ struct FdkParams {
   int* status;
   int nx, ny, nz;               // local sub-volume extents (x fastest)
   int tiles_x, tiles_y, tiles_z;
+  int tile0;                    // first tile of this launch (launches may cover z-ranges)
   float ox, oy, oz;             // coordinate of local voxel (0,0,0) relative to volDim/2
   int nviews, view0;
   int BW, BH, stages, wshift;
@@ -250,7 +251,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int tx, ty, tz;
-  fdk_tile(P, blockIdx.x, tx, ty, tz);
+  fdk_tile(P, P.tile0 + blockIdx.x, tx, ty, tz);
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < P.stages; s++) {
@@ -263,29 +264,68 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
 
   if (warp == FDK_CWARPS) {
     // ------------------------------------------------------------- producer warp
-    if (lane != 0) return;
-    dev::tma_prefetch(&tmap);
     const uint32_t bytes = (uint32_t)(stage_elems * ES);
     int issued = 0;  // staged views so far (= ring position)
     bool failed = false;
-    for (int v = 0; v < P.nviews; v++) {
-      int w0, h0, nw, nh;
-      float fp[4];
-      fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, w0, h0, nw, nh, fp);
-      // with the PI window, views that cannot reach the tile are not staged at all
-      if (PIW && fdk_tile_outside_window(P, P.v[v], fp[0], fp[1], fp[2], fp[3])) continue;
-      const int s = issued % P.stages;
-      if (issued >= P.stages) {
-        if (!dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
-          failed = true;
-          break;
+    if constexpr (PIW) {
+      // the whole warp tests 32 views at a time against the PI window (most views miss a
+      // tile of a helical scan); lane 0 stages the ones that reach it, in view order
+      if (lane == 0) dev::tma_prefetch(&tmap);
+      for (int vb = 0; vb < P.nviews && !failed; vb += 32) {
+        const int v = vb + lane;
+        int w0 = 0, h0 = 0, nw = 0, nh = 0;
+        bool need = false;
+        if (v < P.nviews) {
+          float fp[4];
+          fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, w0, h0, nw, nh, fp);
+          need = !fdk_tile_outside_window(P, P.v[v], fp[0], fp[1], fp[2], fp[3]);
+        }
+        unsigned mask = __ballot_sync(0xffffffffu, need);
+        while (mask) {
+          const int l = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const int sw0 = __shfl_sync(0xffffffffu, w0, l), sh0 = __shfl_sync(0xffffffffu, h0, l);
+          const int snw = __shfl_sync(0xffffffffu, nw, l), snh = __shfl_sync(0xffffffffu, nh, l);
+          int ok = 1;
+          if (lane == 0) {
+            const int s = issued % P.stages;
+            if (issued >= P.stages && !dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
+              ok = 0;
+            } else {
+              if (snw > P.BW || snh > P.BH) dev::record_status(P.status, DEV_RANGE);
+              origin[s] = make_int4(sw0, sh0, vb + l, 0);
+              dev::mbar_arrive_expect_tx(&full[s], bytes);
+              dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], sw0, sh0,
+                               P.view0 + vb + l);
+            }
+          }
+          if (!__shfl_sync(0xffffffffu, ok, 0)) {
+            failed = true;
+            break;
+          }
+          issued++;
         }
       }
-      if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
-      origin[s] = make_int4(w0, h0, v, 0);
-      dev::mbar_arrive_expect_tx(&full[s], bytes);
-      dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + v);
-      issued++;
+      if (lane != 0) return;
+    } else {
+      if (lane != 0) return;
+      dev::tma_prefetch(&tmap);
+      for (int v = 0; v < P.nviews; v++) {
+        int w0, h0, nw, nh;
+        fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, w0, h0, nw, nh);
+        const int s = issued % P.stages;
+        if (issued >= P.stages) {
+          if (!dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
+            failed = true;
+            break;
+          }
+        }
+        if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
+        origin[s] = make_int4(w0, h0, v, 0);
+        dev::mbar_arrive_expect_tx(&full[s], bytes);
+        dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + v);
+        issued++;
+      }
     }
     if (PIW && !failed) {
       // end of the view list: a slot whose phase completes without data, view -1
@@ -474,6 +514,7 @@ struct GenParams {
   // sv0 x sv1 x sv2 voxels from volStart, ntx x nty of them per z layer.
   const int4* win;
   int sv0, sv1, sv2, ntx, nty, wviews;
+  long long vox0, nvox;  // voxel range of this launch (launches may cover z-ranges)
   GenView v[GEN_MAXV];
 };
 static_assert(sizeof(GenParams) < 32000, "kernel parameter space");
@@ -488,9 +529,8 @@ __device__ __forceinline__ float gen_load(const void* base, int ptype, size_t i)
 
 __global__ void __launch_bounds__(256) bp_generic_kernel(const __grid_constant__ GenParams P)
 {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nvox = (long long)P.nx * P.ny * P.nz;
-  if (i >= nvox) return;
+  const long long i = P.vox0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= P.vox0 + P.nvox) return;
   const int xi = (int)(i % P.nx);
   const long long r = i / P.nx;
   const int yi = (int)(r % P.ny), zi = (int)(r / P.ny);
@@ -580,8 +620,9 @@ struct fcb_bp_plan {
 
 namespace {
 
+// Launches chunk `chunk` (-1: all) over the z-tile layers [tz0, tz1) of the plan.
 template <typename T, int NZ, bool PIW, bool X2, int MINB = fdk_min_blocks<NZ>()>
-int launch_fdk(const fcb_bp_plan* pl, const CUtensorMap& map, int chunk, cudaStream_t st)
+int launch_fdk(fcb_bp_plan* pl, const CUtensorMap& map, int chunk, int tz0, int tz1, cudaStream_t st)
 {
   const size_t stage_bytes = ((size_t)pl->BW * pl->BH * sizeof(T) + 127) & ~(size_t)127;
   const size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int4));
@@ -589,8 +630,11 @@ int launch_fdk(const fcb_bp_plan* pl, const CUtensorMap& map, int chunk, cudaStr
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int c = 0; c < (int)pl->fdk.size(); c++) {
     if (chunk >= 0 && c != chunk) continue;
-    const FdkParams& P = pl->fdk[c];
-    const int ntiles = P.tiles_x * P.tiles_y * P.tiles_z;
+    FdkParams& P = pl->fdk[c];
+    const int layer = P.tiles_x * P.tiles_y;
+    P.tile0 = tz0 * layer;
+    const int ntiles = (tz1 - tz0) * layer;
+    if (ntiles <= 0) continue;
     kern<<<ntiles, FDK_THREADS, smem, st>>>(map, P);
     FCB_CUDA_TRY(cudaGetLastError());
   }
@@ -818,12 +862,18 @@ int bp_plan_chunks(const fcb_bp_plan* pl, std::vector<std::pair<int, int>>* rang
   return FCB_OK;
 }
 
-// Launch chunk `chunk` of the plan (-1: all chunks).
-int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* volume,
-                          cudaStream_t st)
+// Launch chunk `chunk` of the plan (-1: all chunks) over the volume planes [z0, z1) of the
+// plan's sub-volume (z0, z1 multiples of the plan's z tile, or the volume's end; -1: all).
+int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void* proj,
+                          float* volume, cudaStream_t st)
 {
   if (!pl || !proj || !volume) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
   const Problem& pb = pl->pb;
+  const int nzv = pb.volEnd[2] - pb.volStart[2];
+  if (z0 < 0) { z0 = 0; z1 = nzv; }
+  if (z0 > z1 || z1 > nzv || (z0 % pl->nz_tile) || (z1 % pl->nz_tile && z1 != nzv))
+    return set_error(FCB_ERR_INVALID, "plane range must follow the plan's z tiles");
+  const int tz0 = z0 / pl->nz_tile, tz1 = (z1 + pl->nz_tile - 1) / pl->nz_tile;
   const size_t es = dtype_size(pl->ptype);
   bool tma_ok = pl->path == 1 && ((uintptr_t)proj % 16 == 0) &&
                 ((size_t)pb.projWHSize[0] * es) % 16 == 0;
@@ -840,27 +890,27 @@ int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* v
     // FCB_FDK_SCALAR=1 selects the one-voxel-per-instruction FP32 path (for comparison)
     static const bool scalar = getenv("FCB_FDK_SCALAR") && getenv("FCB_FDK_SCALAR")[0] == '1';
     if (pl->ptype == FCB_F32 && scalar) {
-      if (piw) FCB_TRY((launch_fdk<float, 32, true, false>(pl, map, chunk, st)));
-      else FCB_TRY((launch_fdk<float, 32, false, false>(pl, map, chunk, st)));
+      if (piw) FCB_TRY((launch_fdk<float, 32, true, false>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<float, 32, false, false>(pl, map, chunk, tz0, tz1, st)));
     } else if (pl->ptype == FCB_F32 && pl->nz_tile == 16) {
-      if (piw) FCB_TRY((launch_fdk<float, 16, true, true>(pl, map, chunk, st)));
-      else FCB_TRY((launch_fdk<float, 16, false, true>(pl, map, chunk, st)));
+      if (piw) FCB_TRY((launch_fdk<float, 16, true, true>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<float, 16, false, true>(pl, map, chunk, tz0, tz1, st)));
     } else if (pl->ptype == FCB_F32 && pl->nz_tile == 64) {
-      if (piw) FCB_TRY((launch_fdk<float, 64, true, true>(pl, map, chunk, st)));
-      else FCB_TRY((launch_fdk<float, 64, false, true>(pl, map, chunk, st)));
+      if (piw) FCB_TRY((launch_fdk<float, 64, true, true>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<float, 64, false, true>(pl, map, chunk, tz0, tz1, st)));
     } else if (pl->ptype == FCB_F32 && getenv("FCB_FDK_MINB4")) {
       // register cap for 4 CTAs per SM (occupancy experiment)
-      if (piw) FCB_TRY((launch_fdk<float, 32, true, true, 4>(pl, map, chunk, st)));
-      else FCB_TRY((launch_fdk<float, 32, false, true, 4>(pl, map, chunk, st)));
+      if (piw) FCB_TRY((launch_fdk<float, 32, true, true, 4>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<float, 32, false, true, 4>(pl, map, chunk, tz0, tz1, st)));
     } else if (pl->ptype == FCB_F32) {
-      if (piw) FCB_TRY((launch_fdk<float, 32, true, true>(pl, map, chunk, st)));
-      else FCB_TRY((launch_fdk<float, 32, false, true>(pl, map, chunk, st)));
+      if (piw) FCB_TRY((launch_fdk<float, 32, true, true>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<float, 32, false, true>(pl, map, chunk, tz0, tz1, st)));
     } else if (pl->ptype == FCB_F16) {
-      if (piw) FCB_TRY((launch_fdk<__half, 32, true, false>(pl, map, chunk, st)));
-      else FCB_TRY((launch_fdk<__half, 32, false, false>(pl, map, chunk, st)));
+      if (piw) FCB_TRY((launch_fdk<__half, 32, true, false>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<__half, 32, false, false>(pl, map, chunk, tz0, tz1, st)));
     } else {
-      if (piw) FCB_TRY((launch_fdk<__nv_bfloat16, 32, true, false>(pl, map, chunk, st)));
-      else FCB_TRY((launch_fdk<__nv_bfloat16, 32, false, false>(pl, map, chunk, st)));
+      if (piw) FCB_TRY((launch_fdk<__nv_bfloat16, 32, true, false>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<__nv_bfloat16, 32, false, false>(pl, map, chunk, tz0, tz1, st)));
     }
     return ok();
   }
@@ -893,12 +943,23 @@ int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* v
     GenParams& P = pl->gen[c];
     P.vol = volume;
     P.proj = proj;
-    const long long nvox = (long long)P.nx * P.ny * P.nz;
-    bp_generic_kernel<<<(unsigned)((nvox + 255) / 256), 256, 0, st>>>(P);
+    const long long plane = (long long)P.nx * P.ny;
+    P.vox0 = plane * z0;
+    P.nvox = plane * (z1 - z0);
+    if (P.nvox <= 0) continue;
+    bp_generic_kernel<<<(unsigned)((P.nvox + 255) / 256), 256, 0, st>>>(P);
     FCB_CUDA_TRY(cudaGetLastError());
   }
   return ok();
 }
+
+int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* volume,
+                          cudaStream_t st)
+{
+  return bp_plan_execute_range(pl, chunk, -1, -1, proj, volume, st);
+}
+
+int bp_plan_z_tile(const fcb_bp_plan* pl) { return pl->nz_tile; }
 
 }  // namespace fcb
 

@@ -26,6 +26,9 @@ int bp_plan_create_ex(const fcb_geometry* g, int kernelMode, int projType, int m
 int bp_plan_chunks(const fcb_bp_plan* pl, std::vector<std::pair<int, int>>* ranges);
 int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* volume,
                           cudaStream_t st);
+int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void* proj,
+                          float* volume, cudaStream_t st);
+int bp_plan_z_tile(const fcb_bp_plan* pl);
 }  // namespace fcb
 
 using namespace fcb;
@@ -119,13 +122,15 @@ struct HostTrace {
   }
 };
 
-// Host-buffer backprojection, pipelined over z-slabs of the volume:
-//   copy-in stream : volume slab 0, the projections in view chunks, then volume slab s+1
-//   compute stream : slab 0 chunk by chunk as the projections arrive, then whole slabs
-//   copy-out stream: slab s back to the host as soon as its backprojection is done
+// Host-buffer backprojection, pipelined over view chunks and z-slabs of the volume:
+//   copy-in stream : the first view chunk, the volume slab by slab, then the other chunks
+//   compute stream : chunk by chunk as they arrive, each over all slabs (slab s of the first
+//                    chunk as soon as slab s is in)
+//   copy-out stream: slab s back to the host as soon as the last chunk has passed over it
 // so the PCIe traffic (projections once, the volume in and out) hides behind the kernels
-// except for the first chunk and the last slab.  Reference-compatible windows that change
-// the result need the whole volume as one problem (their tiling starts at volStart).
+// except for the first chunk with the first slab, and the last slab.  One plan (one staging
+// pre-pass) serves every slab: a slab is a range of the plan's z tiles.  Reference-compatible
+// windows that change the result run as one slab (their tiling starts at volStart).
 extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kernelMode,
                                     const float* projections, float* volume)
 {
@@ -152,35 +157,29 @@ extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kern
   const int wpad = g.referenceWindows ? W : (W + 3) & ~3;
   g.projWHSize[0] = wpad;  // zero columns beyond W change nothing (zero extension)
 
-  // z-slabs: multiples of 32 planes (the kernel's z tile), at least 64 deep, at most 8
+  const int chunk = 120;  // views per upload chunk
+  fcb_bp_plan* plan = nullptr;
+  FCB_TRY(bp_plan_create_ex(&g, kernelMode, FCB_F32, chunk, &plan));
+  struct PlanGuard {
+    fcb_bp_plan* p;
+    ~PlanGuard() { fcb_bp_plan_destroy(p); }
+  } pg{plan};
+  std::vector<std::pair<int, int>> ranges;
+  FCB_TRY(bp_plan_chunks(plan, &ranges));
+  const double t_plan = tr.ms();
+
+  // z-slabs: multiples of the plan's z tile, at least 64 planes, at most 8
   const int nx = g.volEnd[0] - g.volStart[0], ny = g.volEnd[1] - g.volStart[1],
             nz = g.volEnd[2] - g.volStart[2];
+  const int zt = bp_plan_z_tile(plan);
   int nslab = g.referenceWindows ? 1 : std::max(1, std::min(8, nz / 64));
-  const int slab = ((nz + nslab - 1) / nslab + 31) / 32 * 32;
+  const int slab = ((nz + nslab - 1) / nslab + zt - 1) / zt * zt;
   nslab = (nz + slab - 1) / slab;
-  const int chunk = 120;  // views per upload chunk (slab 0 follows the upload chunk by chunk)
-
-  struct PlanSet {
-    std::vector<fcb_bp_plan*> p;
-    ~PlanSet()
-    {
-      for (fcb_bp_plan* q : p) fcb_bp_plan_destroy(q);
-    }
-  } plans;
   std::vector<int> z0(nslab), z1(nslab);
   for (int s = 0; s < nslab; s++) {
-    z0[s] = g.volStart[2] + s * slab;
-    z1[s] = std::min(g.volEnd[2], z0[s] + slab);
-    fcb_geometry gs = g;
-    gs.volStart[2] = z0[s];
-    gs.volEnd[2] = z1[s];
-    fcb_bp_plan* pl = nullptr;
-    FCB_TRY(bp_plan_create_ex(&gs, kernelMode, FCB_F32, s == 0 ? chunk : 1 << 30, &pl));
-    plans.p.push_back(pl);
+    z0[s] = s * slab;
+    z1[s] = std::min(nz, z0[s] + slab);
   }
-  std::vector<std::pair<int, int>> ranges;
-  FCB_TRY(bp_plan_chunks(plans.p[0], &ranges));
-  const double t_plan = tr.ms();
 
   const size_t plane = (size_t)nx * ny;
   const size_t nvox = plane * nz;
@@ -194,45 +193,40 @@ extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kern
   FCB_TRY(sc.stream(&xs));
   FCB_TRY(sc.stream(&os));
   if (wpad != W) FCB_CUDA_TRY(cudaMemsetAsync(dproj, 0, (size_t)n * H * wpad * sizeof(float), xs));
-  auto slab_ptr = [&](float* base, int s) { return base + (size_t)(z0[s] - g.volStart[2]) * plane; };
+  auto zoff = [&](int s) { return (size_t)z0[s] * plane; };
   auto slab_bytes = [&](int s) { return (size_t)(z1[s] - z0[s]) * plane * sizeof(float); };
   cudaEvent_t ev;
-  std::vector<cudaEvent_t> done(nslab);
-  for (int s = 0; s < nslab; s++) FCB_TRY(sc.event(&done[s]));
   cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};
   if (tr.on)
     for (cudaEvent_t& e : tev) FCB_CUDA_TRY(cudaEventCreate(&e));
   if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[0], xs));
 
-  // slab 0 and the projections
-  FCB_CUDA_TRY(cudaMemcpyAsync(slab_ptr(dvol, 0), slab_ptr(volume, 0), slab_bytes(0),
-                               cudaMemcpyHostToDevice, xs));
-  for (size_t c = 0; c < ranges.size(); c++) {
+  const int nch = (int)ranges.size();
+  for (int c = 0; c < nch; c++) {
     FCB_TRY(copy_proj_h2d(dproj, projections, ranges[c].first, ranges[c].second, W, H, wpad, xs));
     FCB_TRY(sc.event(&ev));
     FCB_CUDA_TRY(cudaEventRecord(ev, xs));
     FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
-    if (c == 0 && tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[1], cs));
-    FCB_TRY(bp_plan_execute_chunk(plans.p[0], (int)c, dproj, slab_ptr(dvol, 0), cs));
-  }
-  FCB_CUDA_TRY(cudaEventRecord(done[0], cs));
-  // the other slabs: volume in (copy-in stream), backprojection, volume out (copy-out)
-  for (int s = 1; s < nslab; s++) {
-    FCB_CUDA_TRY(cudaMemcpyAsync(slab_ptr(dvol, s), slab_ptr(volume, s), slab_bytes(s),
-                                 cudaMemcpyHostToDevice, xs));
-    FCB_TRY(sc.event(&ev));
-    FCB_CUDA_TRY(cudaEventRecord(ev, xs));
-    FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
-    FCB_TRY(bp_plan_execute_chunk(plans.p[s], -1, dproj, slab_ptr(dvol, s), cs));
-    FCB_CUDA_TRY(cudaEventRecord(done[s], cs));
-    FCB_CUDA_TRY(cudaStreamWaitEvent(os, done[s - 1], 0));
-    FCB_CUDA_TRY(cudaMemcpyAsync(slab_ptr(volume, s - 1), slab_ptr(dvol, s - 1), slab_bytes(s - 1),
-                                 cudaMemcpyDeviceToHost, os));
+    for (int s = 0; s < nslab; s++) {
+      if (c == 0) {
+        FCB_CUDA_TRY(cudaMemcpyAsync(dvol + zoff(s), volume + zoff(s), slab_bytes(s),
+                                     cudaMemcpyHostToDevice, xs));
+        FCB_TRY(sc.event(&ev));
+        FCB_CUDA_TRY(cudaEventRecord(ev, xs));
+        FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
+        if (s == 0 && tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[1], cs));
+      }
+      FCB_TRY(bp_plan_execute_range(plan, c, z0[s], z1[s], dproj, dvol, cs));
+      if (c == nch - 1) {
+        FCB_TRY(sc.event(&ev));
+        FCB_CUDA_TRY(cudaEventRecord(ev, cs));
+        FCB_CUDA_TRY(cudaStreamWaitEvent(os, ev, 0));
+        FCB_CUDA_TRY(cudaMemcpyAsync(volume + zoff(s), dvol + zoff(s), slab_bytes(s),
+                                     cudaMemcpyDeviceToHost, os));
+      }
+    }
   }
   if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[2], cs));
-  FCB_CUDA_TRY(cudaStreamWaitEvent(os, done[nslab - 1], 0));
-  FCB_CUDA_TRY(cudaMemcpyAsync(slab_ptr(volume, nslab - 1), slab_ptr(dvol, nslab - 1),
-                               slab_bytes(nslab - 1), cudaMemcpyDeviceToHost, os));
   if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[3], os));
   FCB_CUDA_TRY(cudaStreamSynchronize(os));
   FCB_CUDA_TRY(cudaStreamSynchronize(cs));
@@ -243,10 +237,10 @@ extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kern
     cudaEventElapsedTime(&b, tev[0], tev[2]);
     cudaEventElapsedTime(&c, tev[0], tev[3]);
     fprintf(stderr,
-            "fcb_backproject_host: %d slab(s) of %d planes, %zu view chunks; plans %.1f ms, "
+            "fcb_backproject_host: %d slab(s) of %d planes, %d view chunks; plan %.1f ms, "
             "alloc %.1f ms; first kernel at %.1f ms, kernels done %.1f ms, volume home %.1f ms "
             "(GPU clock from the first copy); call %.1f ms\n",
-            nslab, slab, ranges.size(), t_plan, t_alloc - t_plan, a, b, c, tr.ms());
+            nslab, slab, nch, t_plan, t_alloc - t_plan, a, b, c, tr.ms());
     for (cudaEvent_t e : tev) cudaEventDestroy(e);
   }
   return ok();

@@ -11,10 +11,14 @@
 //
 //  * FCB_PROJ_TEXTURE: trilinear sampling by the texture unit from a 3-D CUDA array with
 //    border (zero) addressing -- the reference's interpolation, 8-bit weights included;
-//  * FCB_PROJ_EXPLICIT: FP32 trilinear from global memory (read-only path), exact weights;
-//    project_adjoint_kernel scatters with the very same weights, so the pair satisfies
-//    <A x, y> = <x, A^T y> to rounding.
+//  * FCB_PROJ_EXPLICIT: FP32 trilinear with exact weights from volume bricks staged in
+//    shared memory by TMA (project_brick_kernel); its transpose project_adjoint_brick_kernel
+//    accumulates in shared-memory bricks; <A x, y> = <x, A^T y> to rounding;
+//  * FCB_PROJ_EXPLICIT_GLOBAL: the same samples and arithmetic with every tap read from
+//    global memory (project_explicit_kernel; transpose project_adjoint_kernel, a direct
+//    scatter), the unstaged comparison and the fallback where bricks do not apply.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -449,6 +453,135 @@ __global__ void __launch_bounds__(PB_THREADS, 1) project_brick_kernel(
   count_samples(P.samples, m1 - m0 + 1);
 }
 
+// Transpose of the brick projector, A^T: the same bundles, slabs and samples; each sample's
+// eight weighted taps are added into a shared-memory brick (shared atomics, many rays meet
+// in a voxel) and the brick is then added to global memory once per slab (only its nonzero
+// voxels, contiguous along the brick's inner axis).  x-dominant bundles accumulate into a
+// y-fastest buffer `volT` that transpose_add_kernel folds into the volume afterwards, so
+// both orientations flush coalesced.  Samples whose taps leave the brick scatter straight
+// to global memory.  Weights are those of project_adjoint_kernel; the pair with the brick
+// projector passes the dot-product test to rounding.
+__global__ void __launch_bounds__(256) project_adjoint_brick_kernel(const __grid_constant__ PjParams P,
+                                                                    float* vol, float* volT)
+{
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* brick = reinterpret_cast<float*>(smem_raw);
+  const int nb = P.BC * PB_BD * P.BZ;
+  int* range = reinterpret_cast<int*>(smem_raw + (size_t)nb * 4);
+  int4* org = reinterpret_cast<int4*>(range + 4);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int v = blockIdx.z;
+  const PjView& V = P.v[v];
+  const int bw0 = blockIdx.x * PB_W, bh0 = blockIdx.y * PB_H;
+  Bundle B;
+  bundle_of(V, bw0, bh0, B);
+  const bool xd = B.xdom != 0;
+  const int ndom = xd ? P.nx : P.ny;
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  for (int e = threadIdx.x; e < nb; e += blockDim.x) brick[e] = 0.0f;
+  if (threadIdx.x == 0) {
+    range[0] = 0x7fffffff;
+    range[1] = -0x7fffffff;
+  }
+  __syncthreads();
+
+  float s[3], d[3];
+  int m0 = 1, m1 = 0;
+  float y = 0.0f;
+  const int wl = bw0 + lane, hl = bh0 + warp;
+  if (wl < P.WH0 && hl < P.WH1) {
+    y = V.wt * __ldg(P.proj + ((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl);
+    ray_of(V, wl, hl, s, d);
+    if (y != 0.0f && ray_clip(s, d, nx, ny, nz, m0, m1)) {
+      const float sD = xd ? s[0] : s[1], dD = xd ? d[0] : d[1];
+      const int f0 = (int)floorf(fmaf((float)m0, dD, sD));
+      const int f1 = (int)floorf(fmaf((float)m1, dD, sD));
+      atomicMin(&range[0], min(f0, f1));
+      atomicMax(&range[1], max(f0, f1));
+    } else {
+      m0 = 1;
+      m1 = 0;
+    }
+  }
+  __syncthreads();
+  const int fmin = range[0], fmax = range[1];
+  const int nsl = fmax >= fmin ? (fmax - fmin) / PB_T + 1 : 0;
+  const size_t sy = nx, sz = (size_t)nx * ny;
+  int m = m0;
+  for (int k = 0; k < nsl; k++) {
+    const int a = B.sgn > 0 ? fmin + k * PB_T : fmax - PB_T + 1 - k * PB_T;
+    if (threadIdx.x == 0) {
+      int c0, z0, nc, nzz;
+      brick_extent(B, a, -1.0f, (float)ndom, c0, z0, nc, nzz);
+      org[0] = make_int4(c0, a, z0, 0);
+    }
+    __syncthreads();
+    const int4 o = org[0];
+    const int alo = a, ahi = a + PB_T - 1;
+    while (m <= m1) {
+      const float mf = (float)m;
+      const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
+      const int idom = xd ? t.i : t.j;
+      if (B.sgn > 0 ? idom > ahi : idom < alo) break;
+      const int ic = (xd ? t.j : t.i) - o.x, id = idom - alo, iz = t.k - o.z;
+      const float ab[2] = {1.0f - t.a, t.a}, bb[2] = {1.0f - t.b, t.b}, cb[2] = {1.0f - t.c, t.c};
+      if ((unsigned)ic < (unsigned)(P.BC - 1) && (unsigned)id < (unsigned)PB_T &&
+          (unsigned)iz < (unsigned)(P.BZ - 1)) {
+        float* b0 = brick + ((size_t)iz * PB_BD + id) * P.BC + ic;
+        const int ox = xd ? P.BC : 1, oy = xd ? 1 : P.BC, oz = P.BC * PB_BD;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const float w = ab[q & 1] * bb[(q >> 1) & 1] * cb[(q >> 2) & 1];
+          atomicAdd(b0 + (q & 1) * ox + ((q >> 1) & 1) * oy + ((q >> 2) & 1) * oz, w * y);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+          const int X = t.i + (q & 1), Y = t.j + ((q >> 1) & 1), Z = t.k + ((q >> 2) & 1);
+          if (X < 0 || Y < 0 || Z < 0 || X >= nx || Y >= ny || Z >= nz) continue;
+          const float w = ab[q & 1] * bb[(q >> 1) & 1] * cb[(q >> 2) & 1];
+          atomicAdd(vol + X + Y * sy + Z * sz, w * y);
+        }
+      }
+      m++;
+    }
+    __syncthreads();
+    // flush: brick element (c, dd, zz) -> voxel; y-fastest buffer for x-dominant bundles
+    for (int e = threadIdx.x; e < nb; e += blockDim.x) {
+      const float val = brick[e];
+      if (val == 0.0f) continue;
+      brick[e] = 0.0f;
+      const int c = e % P.BC, r = e / P.BC;
+      const int dd = r % PB_BD, zz = r / PB_BD;
+      const int gc = o.x + c, gd = a + dd, gz = o.z + zz;
+      const int X = xd ? gd : gc, Y = xd ? gc : gd;
+      if (X < 0 || Y < 0 || gz < 0 || X >= nx || Y >= ny || gz >= nz) continue;
+      if (xd) atomicAdd(volT + (size_t)gz * sz + (size_t)X * ny + Y, val);
+      else atomicAdd(vol + (size_t)gz * sz + (size_t)Y * nx + X, val);
+    }
+    __syncthreads();
+  }
+}
+
+// vol[z][y][x] += vt[z][x][y]
+__global__ void transpose_add_kernel(const float* __restrict__ vt, float* __restrict__ vol, int nx,
+                                     int ny)
+{
+  __shared__ float tile[32][33];
+  const int z = blockIdx.z;
+  const size_t plane = (size_t)nx * ny;
+  const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int y = y0 + threadIdx.x, x = x0 + r;
+    if (x < nx && y < ny) tile[r][threadIdx.x] = vt[z * plane + (size_t)x * ny + y];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int x = x0 + threadIdx.x, y = y0 + r;
+    if (x < nx && y < ny) vol[z * plane + (size_t)y * nx + x] += tile[threadIdx.x][r];
+  }
+}
+
 // y-fastest copy of the volume: vt[z][x][y] = vol[z][y][x] (bricks of x-dominant bundles).
 __global__ void transpose_xy_kernel(const float* __restrict__ vol, float* __restrict__ vt, int nx,
                                     int ny)
@@ -498,7 +631,9 @@ int brick_setup(const std::vector<PjParams>& chunks, int nx, int ny, cudaStream_
   if (BC > 128 || BZ > 64) return FCB_OK;  // a wide cone: bricks would not pay
   const int box = BC * PB_BD * BZ * 4;
   const int stage_bytes = (box + 127) & ~127;
-  const int stages = std::max(2, std::min(4, (96 * 1024) / stage_bytes));
+  int stages = std::max(2, std::min(4, (96 * 1024) / stage_bytes));
+  // tuning knob: FCB_PROJ_STAGES=2..6 buffers (fewer buffers, more resident CTAs)
+  if (const char* e = getenv("FCB_PROJ_STAGES")) stages = std::max(2, std::min(6, atoi(e)));
   const size_t smem = (size_t)stages * stage_bytes + stages * (2 * sizeof(uint64_t) + sizeof(int4)) + 16;
   if (smem > 200 * 1024) return FCB_OK;
   bs->ok = true;
@@ -538,6 +673,28 @@ int brick_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, const floa
     project_brick_kernel<<<grid, PB_THREADS, bs.smem, st>>>(mv, mt, P);
     FCB_CUDA_TRY(cudaGetLastError());
   }
+  return FCB_OK;
+}
+
+// Launches the brick adjoint over `chunks`: vol += A^T (norm * proj), `vt` a scratch volume.
+int brick_adjoint_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, float* vol, float* vt,
+                         int nx, int ny, int nz, cudaStream_t st)
+{
+  const size_t smem = (size_t)bs.BC * PB_BD * bs.BZ * 4 + 16 + 16;
+  if (smem > 200 * 1024) return set_error(FCB_ERR_RANGE, "adjoint brick exceeds shared memory");
+  FCB_CUDA_TRY(cudaMemsetAsync(vt, 0, (size_t)nx * ny * nz * sizeof(float), st));
+  FCB_CUDA_TRY(cudaFuncSetAttribute(project_adjoint_brick_kernel,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (PjParams& P : chunks) {
+    P.BC = bs.BC;
+    P.BZ = bs.BZ;
+    dim3 grid((P.WH0 + PB_W - 1) / PB_W, (P.WH1 + PB_H - 1) / PB_H, P.nviews);
+    project_adjoint_brick_kernel<<<grid, 256, smem, st>>>(P, vol, vt);
+    FCB_CUDA_TRY(cudaGetLastError());
+  }
+  dim3 tg((nx + 31) / 32, (ny + 31) / 32, nz);
+  transpose_add_kernel<<<tg, dim3(32, 8), 0, st>>>(vt, vol, nx, ny);
+  FCB_CUDA_TRY(cudaGetLastError());
   return FCB_OK;
 }
 
@@ -728,13 +885,14 @@ int project_launch(const Problem& pb, int method, const float* vol, float* proj,
     chunks.push_back(P);
   }
   int rc = FCB_OK;
-  if (method == FCB_PROJ_EXPLICIT && !adj_vol && !compat) {
+  if (method == FCB_PROJ_EXPLICIT && !compat) {
     BrickSetup bs;
     FCB_TRY(brick_setup(chunks, nx, ny, st, &bs));
     if (bs.ok) {
       float* vt = nullptr;
       FCB_CUDA_TRY(cudaMallocAsync((void**)&vt, (size_t)nx * ny * nz * sizeof(float), st));
-      rc = brick_launch(chunks, bs, vol, vt, nx, ny, nz, st);
+      rc = adj_vol ? brick_adjoint_launch(chunks, bs, adj_vol, vt, nx, ny, nz, st)
+                   : brick_launch(chunks, bs, vol, vt, nx, ny, nz, st);
       cudaFreeAsync(vt, st);
       return rc;
     }
@@ -850,12 +1008,16 @@ extern "C" int fcb_proj_plan_execute(fcb_proj_plan* pl, const float* volume, flo
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (adjoint && pl->method == FCB_PROJ_TEXTURE)
     return set_error(FCB_ERR_INVALID, "the adjoint belongs to the explicit projector");
-  if (!adjoint && pl->bricks.ok) {
+  if (pl->bricks.ok) {
     for (PjParams& P : pl->chunks) {
       P.vol = volume;
       P.proj = proj;
     }
-    FCB_TRY(brick_launch(pl->chunks, pl->bricks, volume, pl->vt, pl->nx, pl->ny, pl->nz, st));
+    if (adjoint)
+      FCB_TRY(brick_adjoint_launch(pl->chunks, pl->bricks, const_cast<float*>(volume), pl->vt, pl->nx,
+                                   pl->ny, pl->nz, st));
+    else
+      FCB_TRY(brick_launch(pl->chunks, pl->bricks, volume, pl->vt, pl->nx, pl->ny, pl->nz, st));
     return ok();
   }
   if (pl->method == FCB_PROJ_TEXTURE) {
