@@ -94,7 +94,8 @@ def parse():
     ap.add_argument("--shard", default="replicas", choices=["replicas", "z"],
                     help="N>1: independent volumes per rank (weak scaling) or one volume in z-slabs "
                          "(strong scaling)")
-    ap.add_argument("--case", default=None, choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "conv-256"],
+    ap.add_argument("--case", default=None,
+                    choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "conv-256", "katsevich", "pipeline"],
                     help="profiling case: run only this kernel on a reduced workload (no JSON line)")
     return ap.parse_args()
 
@@ -106,7 +107,12 @@ def run_case(args):
     proj-512: the staged, unstaged and texture projectors on 512^3, 90 views, 768x512
     detector (0.5 GB volume);
     conv-256: one unrolled step's convolutions at 256^3 x 16 BF16 channels (0.54 GB per
-    activation): forward, input gradient (tensor cores) and weight gradient."""
+    activation): forward, input gradient (tensor cores) and weight gradient;
+    katsevich: the helical PI-window backprojection (512x512x384, 4640 views; 1.3 GB);
+    pipeline: every other kernel once at a moderate size, inputs above L2 where the workload
+    allows: phantom, FDK filter (ramp + Shepp-Logan), Katsevich filter, projector adjoint,
+    misaligned (generic) backprojection, reference-window backprojection and projection,
+    brick-size and footprint pre-passes, volume transpose."""
     import numpy as np
     import torch
 
@@ -137,11 +143,55 @@ def run_case(args):
         ms = e0.elapsed_time(e1) / args.steps
         upd = 1024 * 1024 * 128 * n
         print(json.dumps({"case": args.case, "ms": ms, "GUPS": upd / ms / 1e6, "box": plan.info()}))
+    elif args.case == "katsevich":
+        from fastcone_b200 import configs
+
+        gk = configs.helical_katsevich(pi_window=True)
+        pk = torch.randn(gk.proj_shape, device=dev)
+        vk = torch.zeros(gk.vol_shape, device=dev)
+        plan = ops.BackprojectPlan(gk, mode=_lib.MODE_KATSEVICH, dtype=torch.float32)
+        for _ in range(args.warmup):
+            plan(pk, vk)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            plan(pk, vk)
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"case": args.case, "ms": e0.elapsed_time(e1) / args.steps, **plan.info()}))
+    elif args.case == "pipeline":
+        import dataclasses
+
+        from fastcone_b200 import configs
+        from fastcone_b200.phantom import random_ellipsoids
+
+        gd = configs.diff_batch()                        # 256^3, 360 views, 384x256
+        vol = ops.phantom(gd.vol_xyz, random_ellipsoids(10, gd.vol_xyz, 3), device=dev)
+        proj = torch.randn(gd.proj_shape, device=dev)    # 141 MB
+        for _ in range(args.warmup + args.steps):
+            ops.fdk_filter(proj, gd)
+            ops.fdk_filter(proj, gd, window=_lib.FILTER_SHEPPLOGAN)
+            ops.project_adjoint(proj, gd)
+            ops.project(vol, gd, method=_lib.PROJ_EXPLICIT)   # includes pre-pass + transpose
+            gm = dataclasses.replace(gd, misalignments=np.array([1.5, -0.5, 2.0, 0.01, -0.01, 0.02], np.float32))
+            ops.backproject(proj, gm, mode=_lib.MODE_UNWEIGHTED)
+        gk = configs.helical_katsevich(pi_window=True)
+        pk = torch.randn(gk.proj_shape, device=dev)      # 874 MB
+        for _ in range(args.warmup + args.steps):
+            ops.katsevich_filter(pk, gk)
+        # reference-compatible windows on the 48^3 / 72-pixel geometry they change
+        gq = ConeGeometry((48, 48, 48), (72, 48), np.arange(36) * (2 * np.pi / 36), 200.0, 0.5,
+                          reference_windows=True)
+        vq = ops.phantom(gq.vol_xyz, random_ellipsoids(5, gq.vol_xyz, 4), device=dev)
+        for _ in range(args.warmup + args.steps):
+            pq = ops.project(vq, gq, method=_lib.PROJ_EXPLICIT)
+            ops.backproject(pq, gq, mode=_lib.MODE_FDK)
+        print(json.dumps({"case": args.case}))
     elif args.case == "conv-256":
         from fastcone_b200 import nn
 
         gen = torch.Generator(device=dev).manual_seed(0)
-        x = torch.randn((256, 256, 256, 16), device=dev, generator=gen).to(torch.bfloat16)
+        x = torch.randn((256, 256, 2, 256, 8), device=dev, generator=gen).to(torch.bfloat16)
         wk = (0.05 * torch.randn((27, 16, 16), device=dev, generator=gen)).to(torch.bfloat16)
         b = torch.zeros(16, device=dev)
         res = {}

@@ -45,6 +45,7 @@ EXPORTED_SYMBOLS = [
     "fcb_conv3d16_device", "fcb_conv3d16_wgrad_device",
     "fcb_proj_plan_create", "fcb_proj_plan_execute", "fcb_proj_plan_destroy",
     "fcb_reference_windows", "fcb_proj_plan_info",
+    "fcb_filter_plan_create", "fcb_filter_plan_execute", "fcb_filter_plan_destroy",
 ]
 
 
@@ -123,6 +124,9 @@ def lib():
                                                       ctypes.c_float, ctypes.c_int, vp]
             L.fcb_reference_windows.argtypes = [gp] + [c_int_p] * 8
             L.fcb_proj_plan_info.argtypes = [vp] + [c_int_p] * 4
+            L.fcb_filter_plan_create.argtypes = [ctypes.c_int] * 5 + [ctypes.POINTER(vp)]
+            L.fcb_filter_plan_execute.argtypes = [vp, vp, vp, ctypes.c_float, c_float_p, ctypes.c_int, vp]
+            L.fcb_filter_plan_destroy.argtypes = [vp]
             _lib = L
     return _lib
 

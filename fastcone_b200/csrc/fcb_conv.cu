@@ -1,7 +1,9 @@
 // fcb_conv.cu -- 3x3x3 convolutions (16 -> 16 channels, stride 1, zero padding 1) for the
 // learned reconstruction's CNN, on the 5th-generation tensor cores (sm_100a tcgen05).
 //
-// Activations are channels-last BF16, [z][y][x][16] (32 bytes per voxel); weights BF16
+// Activations are BF16 in a channel-half-major layout, [z][y][2][x][8]: for every (z, y) row
+// the 8 channels of half 0 of all x, then those of half 1, so that a TMA box of one half of
+// one row is contiguous (no 32-byte sector is fetched for 16 useful bytes).  Weights BF16
 // [27 taps][16 out][16 in]; accumulation FP32 in tensor memory.  Implicit GEMM: a CTA owns
 // 128 consecutive x-voxels of one (y, z) row -> D[128 x 16] = sum over 27 taps of
 // A_tap[128 x 16 in] * B_tap[16 in x 16 out].  The A operands of the three x-shifts of a tap
@@ -85,14 +87,21 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
-                                            int c2, int c3)
+__device__ __forceinline__ void tma_load_5d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
+                                            int c2, int c3, int c4)
 {
   asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dev::smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(dev::smem_u32(bar))
+      "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(dev::smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4),
+      "r"(dev::smem_u32(bar))
       : "memory");
+}
+
+// Offset (elements) of channel c of voxel (x, y, z) in the [z][y][2][x][8] layout.
+__host__ __device__ __forceinline__ size_t act_index(int x, int y, int z, int c, int nx, int ny)
+{
+  return ((((size_t)z * ny + y) * 2 + (c >> 3)) * nx + x) * 8 + (c & 7);
 }
 
 }  // namespace tc
@@ -101,11 +110,14 @@ constexpr int CV_TILE = 128;                  // voxels per CTA tile (MMA M)
 constexpr int CV_ROW = CV_TILE + 2;           // staged voxels per tap row (x halo)
 constexpr int CV_BOX_BYTES = CV_ROW * 16;     // one channel half of one tap row
 constexpr int CV_RB = 2176;                   // CV_BOX_BYTES rounded up to 128 B
+static_assert((CV_ROW + 2) / 2 * 32 <= CV_RB, "a box of voxel pairs fits its slot");
 constexpr int CV_A_BYTES = 9 * 2 * CV_RB;     // 39168
 constexpr int CV_W_BYTES = 27 * 512;          // 13824
 constexpr int CV_SMEM = CV_A_BYTES + CV_W_BYTES + 64 + 32 + 16;
 
 struct ConvParams {
+  int pairs;               // 1: boxes of voxel pairs (32-byte rows, even nx), 0: single voxels
+  uint32_t box_bytes;      // bytes of one staged half-row box
   const __nv_bfloat16* w;  // [27][16 out][16 in]
   const float* bias;       // [16] or null
   void* out;               // [z][y][x][16], bf16 or f32
@@ -146,11 +158,12 @@ __global__ void __launch_bounds__(128) conv3d16_kernel(const __grid_constant__ C
 
   if (threadIdx.x == 0) {
     dev::tma_prefetch(&xmap);
-    dev::mbar_arrive_expect_tx(&bars[0], 18u * CV_BOX_BYTES);
+    dev::mbar_arrive_expect_tx(&bars[0], 18u * P.box_bytes);
     for (int r = 0; r < 9; r++) {
       const int dz = r / 3, dy = r % 3;
       for (int kh = 0; kh < 2; kh++)
-        tc::tma_load_4d(A + (r * 2 + kh) * CV_RB, &xmap, &bars[0], kh * 8, x0 - 1, y + dy - 1, z + dz - 1);
+        tc::tma_load_5d(A + (r * 2 + kh) * CV_RB, &xmap, &bars[0], 0, P.pairs ? (x0 >> 1) - 1 : x0 - 1, kh,
+                        y + dy - 1, z + dz - 1);
     }
   }
   // weights -> core-matrix layout: tap t, K half kh, row n (out channel): 16 bytes of 8 in-channels
@@ -175,7 +188,7 @@ __global__ void __launch_bounds__(128) conv3d16_kernel(const __grid_constant__ C
       constexpr uint32_t IDESC = tc::idesc_bf16(CV_TILE, 16);
       for (int t = 0; t < 27; t++) {
         const int r = t / 3, dx = t % 3;
-        const uint64_t ad = tc::smem_desc(abase + r * 2 * CV_RB + dx * 16, CV_RB, 128);
+        const uint64_t ad = tc::smem_desc(abase + r * 2 * CV_RB + (dx + P.pairs) * 16, CV_RB, 128);
         const uint64_t bd = tc::smem_desc(wbase + t * 512, 256, 128);
         tc::mma_bf16(taddr, ad, bd, IDESC, t > 0 ? 1u : 0u);
       }
@@ -201,11 +214,14 @@ __global__ void __launch_bounds__(128) conv3d16_kernel(const __grid_constant__ C
         v[c] = __uint_as_float(r[c]) + bias[c];
         if (P.relu) v[c] = fmaxf(v[c], 0.0f);
       }
-      const size_t vox = ((size_t)z * P.ny + y) * P.nx + xv;
+      const size_t i0 = tc::act_index(xv, y, z, 0, P.nx, P.ny), i1 = tc::act_index(xv, y, z, 8, P.nx, P.ny);
       if (P.out_f32) {
-        float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + vox * 16);
-#pragma unroll
-        for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+        float4* o0 = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + i0);
+        float4* o1 = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + i1);
+        o0[0] = make_float4(v[0], v[1], v[2], v[3]);
+        o0[1] = make_float4(v[4], v[5], v[6], v[7]);
+        o1[0] = make_float4(v[8], v[9], v[10], v[11]);
+        o1[1] = make_float4(v[12], v[13], v[14], v[15]);
       } else {
         uint32_t pk[8];
 #pragma unroll
@@ -213,9 +229,9 @@ __global__ void __launch_bounds__(128) conv3d16_kernel(const __grid_constant__ C
           __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
           pk[q] = *reinterpret_cast<uint32_t*>(&b);
         }
-        uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(P.out) + vox * 16);
-        o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-        o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+        __nv_bfloat16* ob = reinterpret_cast<__nv_bfloat16*>(P.out);
+        *reinterpret_cast<uint4*>(ob + i0) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+        *reinterpret_cast<uint4*>(ob + i1) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
       }
     }
   } else if (threadIdx.x == 32) {
@@ -305,11 +321,12 @@ __global__ void __launch_bounds__(CVP_THREADS, 1) conv3d16p_kernel(const __grid_
         const int yz = tile / P.tiles_x;
         const int y = yz % P.ny, z = yz / P.ny;
         unsigned char* As = A + s * CV_A_BYTES;
-        dev::mbar_arrive_expect_tx(&full[s], 18u * CV_BOX_BYTES);
+        dev::mbar_arrive_expect_tx(&full[s], 18u * P.box_bytes);
         for (int r = 0; r < 9; r++) {
           const int dz = r / 3, dy = r % 3;
           for (int kh = 0; kh < 2; kh++)
-            tc::tma_load_4d(As + (r * 2 + kh) * CV_RB, &xmap, &full[s], kh * 8, x0 - 1, y + dy - 1, z + dz - 1);
+            tc::tma_load_5d(As + (r * 2 + kh) * CV_RB, &xmap, &full[s], 0, P.pairs ? (x0 >> 1) - 1 : x0 - 1,
+                            kh, y + dy - 1, z + dz - 1);
         }
       }
       // no copy may still be landing in shared memory when the CTA leaves (bounded waits;
@@ -333,7 +350,7 @@ __global__ void __launch_bounds__(CVP_THREADS, 1) conv3d16p_kernel(const __grid_
         const uint32_t abase = dev::smem_u32(A + s * CV_A_BYTES);
         for (int t = 0; t < 27; t++) {
           const int r = t / 3, dx = t % 3;
-          const uint64_t ad = tc::smem_desc(abase + r * 2 * CV_RB + dx * 16, CV_RB, 128);
+          const uint64_t ad = tc::smem_desc(abase + r * 2 * CV_RB + (dx + P.pairs) * 16, CV_RB, 128);
           const uint64_t bd = tc::smem_desc(wbase + t * 512, 256, 128);
           tc::mma_bf16(taddr + (uint32_t)(b * 16), ad, bd, IDESC, t > 0 ? 1u : 0u);
         }
@@ -368,11 +385,14 @@ __global__ void __launch_bounds__(CVP_THREADS, 1) conv3d16p_kernel(const __grid_
           v[c] = __uint_as_float(r[c]) + bias[c];
           if (P.relu) v[c] = fmaxf(v[c], 0.0f);
         }
-        const size_t vox = ((size_t)z * P.ny + y) * P.nx + xv;
+        const size_t i0 = tc::act_index(xv, y, z, 0, P.nx, P.ny), i1 = tc::act_index(xv, y, z, 8, P.nx, P.ny);
         if (P.out_f32) {
-          float4* o = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + vox * 16);
-#pragma unroll
-          for (int q = 0; q < 4; q++) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          float4* o0 = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + i0);
+          float4* o1 = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + i1);
+          o0[0] = make_float4(v[0], v[1], v[2], v[3]);
+          o0[1] = make_float4(v[4], v[5], v[6], v[7]);
+          o1[0] = make_float4(v[8], v[9], v[10], v[11]);
+          o1[1] = make_float4(v[12], v[13], v[14], v[15]);
         } else {
           uint32_t pk[8];
 #pragma unroll
@@ -380,9 +400,9 @@ __global__ void __launch_bounds__(CVP_THREADS, 1) conv3d16p_kernel(const __grid_
             __nv_bfloat162 bb = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
             pk[q] = *reinterpret_cast<uint32_t*>(&bb);
           }
-          uint4* o = reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(P.out) + vox * 16);
-          o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-          o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+          __nv_bfloat16* ob = reinterpret_cast<__nv_bfloat16*>(P.out);
+          *reinterpret_cast<uint4*>(ob + i0) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+          *reinterpret_cast<uint4*>(ob + i1) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
         }
       }
     }
@@ -434,14 +454,14 @@ __global__ void __launch_bounds__(256) conv3d16_wgrad_kernel(const WgradParams P
       const int zz = z + r / 3 - 1, yy = y + r % 3 - 1, xx = x0 + xr - 1;
       float v = 0.0f;
       if (zz >= 0 && zz < P.nz && yy >= 0 && yy < P.ny && xx >= 0 && xx < P.nx)
-        v = ld_act(P.x + (((size_t)zz * P.ny + yy) * P.nx + xx) * 16 + c);
+        v = ld_act(P.x + tc::act_index(xx, yy, zz, c, P.nx, P.ny));
       xs[r][xr][c] = v;
     }
     for (int i = threadIdx.x; i < WG_TILE * 16; i += blockDim.x) {
       const int c = i & 15, xr = i >> 4, xx = x0 + xr;
       float v = 0.0f;
       if (xx < P.nx) {
-        const size_t o = (((size_t)z * P.ny + y) * P.nx + xx) * 16 + c;
+        const size_t o = tc::act_index(xx, y, z, c, P.nx, P.ny);
         v = P.dy_f32 ? reinterpret_cast<const float*>(P.dy)[o]
                      : ld_act(reinterpret_cast<const __nv_bfloat16*>(P.dy) + o);
       }
@@ -479,13 +499,20 @@ extern "C" int fcb_conv3d16_device(const void* x, const void* w, const float* bi
     return set_error(FCB_ERR_INVALID, "conv3d buffers must be 16-byte aligned");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   CUtensorMap map;
-  const uint64_t dims[4] = {16, (uint64_t)nx, (uint64_t)ny, (uint64_t)nz};
-  const uint64_t strides[3] = {32, 32ull * nx, 32ull * nx * ny};
-  const uint32_t box[4] = {8, CV_ROW, 1, 1};
-  FCB_TRY(encode_tmap(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(x), dims, strides, box));
+  // [z][y][2][x][8]: dims (channels of a voxel pair or of one voxel, x, half, y, z).  With
+  // even nx a box row is a voxel pair (32 bytes, one L2 sector): 66 pairs cover voxels
+  // x0-2 .. x0+129, and the MMA operands start one voxel into the box.  Single-voxel rows
+  // (16 bytes) would fetch every sector twice.
+  const bool pairs = nx % 2 == 0;
+  const uint64_t dims[5] = {pairs ? 16u : 8u, (uint64_t)(pairs ? nx / 2 : nx), 2, (uint64_t)ny, (uint64_t)nz};
+  const uint64_t strides[4] = {pairs ? 32u : 16u, 16ull * nx, 32ull * nx, 32ull * nx * ny};
+  const uint32_t box[5] = {pairs ? 16u : 8u, pairs ? (uint32_t)(CV_ROW + 2) / 2 : (uint32_t)CV_ROW, 1, 1, 1};
+  FCB_TRY(encode_tmap(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(x), dims, strides, box));
   int* status = nullptr;
   FCB_TRY(device_status_ptr(&status));
   ConvParams P;
+  P.pairs = pairs ? 1 : 0;
+  P.box_bytes = box[0] * box[1] * 2;
   P.w = reinterpret_cast<const __nv_bfloat16*>(w);
   P.bias = bias;
   P.out = y;

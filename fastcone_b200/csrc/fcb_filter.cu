@@ -109,86 +109,143 @@ __global__ void phantom_kernel(const __grid_constant__ PhParams P, int e0)
 
 using namespace fcb;
 
+// Reusable filter: cuFFT plans, scratch (padded rows, spectra) and the filter response made
+// once; execute() is stream-ordered, allocates nothing and does not synchronise.
+struct fcb_filter_plan {
+  int nviews = 0, H = 0, W = 0, outType = FCB_F32, window = FCB_FILTER_RAMLAK;
+  int n2 = 0, nb = 0, batch = 0;
+  float* pad = nullptr;
+  cufftComplex* spec = nullptr;
+  float* dfilt = nullptr;
+  float* dz = nullptr;  // per-view zOrigin (nviews floats)
+  cufftHandle pf = 0, pi = 0;
+  ~fcb_filter_plan()
+  {
+    if (pf) cufftDestroy(pf);
+    if (pi) cufftDestroy(pi);
+    cudaFree(pad);
+    cudaFree(spec);
+    cudaFree(dfilt);
+    cudaFree(dz);
+  }
+};
+
+extern "C" int fcb_filter_plan_create(int nviews, int H, int W, int outType, int window,
+                                      fcb_filter_plan** out)
+{
+  if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
+  *out = nullptr;
+  if (nviews <= 0 || H <= 0 || W <= 0) return set_error(FCB_ERR_INVALID, "bad filter sizes");
+  if (outType != FCB_F32 && outType != FCB_F16 && outType != FCB_BF16)
+    return set_error(FCB_ERR_INVALID, "unknown output type");
+  if (window != FCB_FILTER_RAMLAK && window != FCB_FILTER_SHEPPLOGAN)
+    return set_error(FCB_ERR_INVALID, "unknown filter window");
+  auto* pl = new fcb_filter_plan();
+  pl->nviews = nviews; pl->H = H; pl->W = W; pl->outType = outType; pl->window = window;
+  pl->n2 = 2 * W;
+  pl->nb = W + 1;
+  // filter response, computed in double like numpy: |fftfreq(2W)|, DC = f1/8, * pi
+  std::vector<float> filt(pl->nb);
+  for (int k = 0; k < pl->nb; k++) {
+    double f = (double)k / (double)pl->n2;
+    if (k == 0) f = 0.125 * (1.0 / (double)pl->n2);
+    if (window == FCB_FILTER_SHEPPLOGAN && k > 0) {
+      const double x = M_PI * (double)k / (double)pl->n2;
+      f *= sin(x) / x;
+    }
+    filt[k] = (float)(M_PI * f);
+  }
+  const long long rows = (long long)nviews * H;
+  pl->batch = (int)std::min<long long>(rows, std::max<long long>(1, (256ll << 20) / (8ll * pl->n2)));
+  int rc = FCB_OK;
+  do {
+    if (cudaMalloc(&pl->pad, (size_t)pl->batch * pl->n2 * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&pl->spec, (size_t)pl->batch * pl->nb * sizeof(cufftComplex)) != cudaSuccess ||
+        cudaMalloc(&pl->dfilt, pl->nb * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&pl->dz, nviews * sizeof(float)) != cudaSuccess) {
+      cudaGetLastError();
+      rc = set_error(FCB_ERR_NOMEM, "filter scratch");
+      break;
+    }
+    if (cudaMemcpy(pl->dfilt, filt.data(), pl->nb * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+      rc = set_error(FCB_ERR_CUDA, "filter response upload failed");
+      break;
+    }
+    int n[1] = {pl->n2};
+    if (cufftPlanMany(&pl->pf, 1, n, nullptr, 1, pl->n2, nullptr, 1, pl->nb, CUFFT_R2C, pl->batch) != CUFFT_SUCCESS ||
+        cufftPlanMany(&pl->pi, 1, n, nullptr, 1, pl->nb, nullptr, 1, pl->n2, CUFFT_C2R, pl->batch) != CUFFT_SUCCESS) {
+      rc = set_error(FCB_ERR_CUDA, "cufftPlanMany failed");
+      break;
+    }
+  } while (0);
+  if (rc) {
+    delete pl;
+    return rc;
+  }
+  *out = pl;
+  return ok();
+}
+
+// out = filter(in) as outType; zOrigin (host, nviews floats) is read before the call returns.
+extern "C" int fcb_filter_plan_execute(fcb_filter_plan* pl, const float* in, void* out, float D,
+                                       const float* zOrigin, int cosineWeight, void* stream)
+{
+  if (!pl || !in || !out) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
+  if (cosineWeight && (!zOrigin || !(D > 0.0f)))
+    return set_error(FCB_ERR_INVALID, "cosine weighting needs D > 0 and zOrigin");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int n2 = pl->n2, nb = pl->nb, W = pl->W, H = pl->H, batch = pl->batch;
+  if (cosineWeight)
+    FCB_CUDA_TRY(cudaMemcpyAsync(pl->dz, zOrigin, pl->nviews * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (cufftSetStream(pl->pf, st) != CUFFT_SUCCESS || cufftSetStream(pl->pi, st) != CUFFT_SUCCESS)
+    return set_error(FCB_ERR_CUDA, "cufftSetStream failed");
+  const float scale = 1.0f / (float)n2;
+  const long long rows = (long long)pl->nviews * H;
+  for (long long r0 = 0; r0 < rows; r0 += batch) {
+    const int nr = (int)std::min<long long>(batch, rows - r0);
+    long long tot = (long long)nr * n2;
+    pad_weight_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, pl->pad, r0, nr, H, W, D, pl->dz,
+                                                                   cosineWeight);
+    // cuFFT plans are for `batch` rows; the tail batch is zero-padded in `pad`
+    if (nr < batch)
+      FCB_CUDA_TRY(cudaMemsetAsync(pl->pad + (size_t)nr * n2, 0, (size_t)(batch - nr) * n2 * sizeof(float), st));
+    if (cufftExecR2C(pl->pf, pl->pad, pl->spec) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecR2C failed");
+    tot = (long long)nr * nb;
+    spectrum_mul_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(pl->spec, pl->dfilt, nr, nb);
+    if (cufftExecC2R(pl->pi, pl->spec, pl->pad) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecC2R failed");
+    tot = (long long)nr * W;
+    const unsigned g = (unsigned)((tot + 255) / 256);
+    if (pl->outType == FCB_F32) crop_store_kernel<float><<<g, 256, 0, st>>>(pl->pad, (float*)out, r0, nr, W, scale);
+    else if (pl->outType == FCB_F16) crop_store_kernel<__half><<<g, 256, 0, st>>>(pl->pad, (__half*)out, r0, nr, W, scale);
+    else crop_store_kernel<__nv_bfloat16><<<g, 256, 0, st>>>(pl->pad, (__nv_bfloat16*)out, r0, nr, W, scale);
+  }
+  FCB_CUDA_TRY(cudaGetLastError());
+  return ok();
+}
+
+extern "C" int fcb_filter_plan_destroy(fcb_filter_plan* pl)
+{
+  delete pl;
+  return ok();
+}
+
 extern "C" int fcb_fdk_filter_device(const float* in, void* out, int outType, int nviews, int H,
                                      int W, float D, const float* zOrigin, int cosineWeight,
                                      int window, void* stream)
 {
   if (!in || !out || nviews <= 0 || H <= 0 || W <= 0)
     return set_error(FCB_ERR_INVALID, "bad filter arguments");
-  if (outType != FCB_F32 && outType != FCB_F16 && outType != FCB_BF16)
-    return set_error(FCB_ERR_INVALID, "unknown output type");
   if (cosineWeight && (!zOrigin || !(D > 0.0f)))
     return set_error(FCB_ERR_INVALID, "cosine weighting needs D > 0 and zOrigin");
-  if (window != FCB_FILTER_RAMLAK && window != FCB_FILTER_SHEPPLOGAN)
-    return set_error(FCB_ERR_INVALID, "unknown filter window");
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
-  const int n2 = 2 * W, nb = W + 1;
-  // filter response, computed in double like numpy: |fftfreq(2W)|, DC = f1/8, * pi
-  std::vector<float> filt(nb);
-  for (int k = 0; k < nb; k++) {
-    double f = (double)k / (double)n2;
-    if (k == 0) f = 0.125 * (1.0 / (double)n2);
-    if (window == FCB_FILTER_SHEPPLOGAN && k > 0) {
-      const double x = M_PI * (double)k / (double)n2;
-      f *= sin(x) / x;
-    }
-    filt[k] = (float)(M_PI * f);
-  }
-  const long long rows = (long long)nviews * H;
-  const int batch = (int)std::min<long long>(rows, std::max<long long>(1, (256ll << 20) / (8ll * n2)));
-  float *pad = nullptr, *dfilt = nullptr, *dz = nullptr;
-  cufftComplex* spec = nullptr;
-  cufftHandle pf = 0, pi = 0;
-  int rc = FCB_OK;
-  auto fail = [&](int code, const char* m) { rc = set_error(code, m); };
-  do {
-    if (cudaMalloc(&pad, (size_t)batch * n2 * sizeof(float)) != cudaSuccess) { fail(FCB_ERR_NOMEM, "filter scratch"); break; }
-    if (cudaMalloc(&spec, (size_t)batch * nb * sizeof(cufftComplex)) != cudaSuccess) { fail(FCB_ERR_NOMEM, "filter scratch"); break; }
-    if (cudaMalloc(&dfilt, nb * sizeof(float)) != cudaSuccess) { fail(FCB_ERR_NOMEM, "filter scratch"); break; }
-    cudaMemcpyAsync(dfilt, filt.data(), nb * sizeof(float), cudaMemcpyHostToDevice, st);
-    if (cosineWeight) {
-      if (cudaMalloc(&dz, nviews * sizeof(float)) != cudaSuccess) { fail(FCB_ERR_NOMEM, "filter scratch"); break; }
-      cudaMemcpyAsync(dz, zOrigin, nviews * sizeof(float), cudaMemcpyHostToDevice, st);
-    }
-    int n[1] = {n2};
-    if (cufftPlanMany(&pf, 1, n, nullptr, 1, n2, nullptr, 1, nb, CUFFT_R2C, batch) != CUFFT_SUCCESS ||
-        cufftPlanMany(&pi, 1, n, nullptr, 1, nb, nullptr, 1, n2, CUFFT_C2R, batch) != CUFFT_SUCCESS) {
-      fail(FCB_ERR_CUDA, "cufftPlanMany failed");
-      break;
-    }
-    cufftSetStream(pf, st);
-    cufftSetStream(pi, st);
-    const float scale = 1.0f / (float)n2;
-    for (long long r0 = 0; r0 < rows; r0 += batch) {
-      const int nr = (int)std::min<long long>(batch, rows - r0);
-      long long tot = (long long)nr * n2;
-      pad_weight_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, pad, r0, nr, H, W, D, dz, cosineWeight);
-      // cuFFT plans are for `batch` rows; the tail batch is zero-padded in `pad`
-      if (nr < batch) cudaMemsetAsync(pad + (size_t)nr * n2, 0, (size_t)(batch - nr) * n2 * sizeof(float), st);
-      if (cufftExecR2C(pf, pad, spec) != CUFFT_SUCCESS) { fail(FCB_ERR_CUDA, "cufftExecR2C failed"); break; }
-      tot = (long long)nr * nb;
-      spectrum_mul_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(spec, dfilt, nr, nb);
-      if (cufftExecC2R(pi, spec, pad) != CUFFT_SUCCESS) { fail(FCB_ERR_CUDA, "cufftExecC2R failed"); break; }
-      tot = (long long)nr * W;
-      const unsigned g = (unsigned)((tot + 255) / 256);
-      if (outType == FCB_F32) crop_store_kernel<float><<<g, 256, 0, st>>>(pad, (float*)out, r0, nr, W, scale);
-      else if (outType == FCB_F16) crop_store_kernel<__half><<<g, 256, 0, st>>>(pad, (__half*)out, r0, nr, W, scale);
-      else crop_store_kernel<__nv_bfloat16><<<g, 256, 0, st>>>(pad, (__nv_bfloat16*)out, r0, nr, W, scale);
-    }
-    if (rc) break;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) { fail(FCB_ERR_CUDA, cudaGetErrorString(e)); break; }
-    // scratch is freed below; wait for the queued work that uses it
-    e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) { fail(FCB_ERR_CUDA, cudaGetErrorString(e)); break; }
-  } while (0);
-  if (pf) cufftDestroy(pf);
-  if (pi) cufftDestroy(pi);
-  cudaFree(pad);
-  cudaFree(spec);
-  cudaFree(dfilt);
-  cudaFree(dz);
-  return rc ? rc : ok();
+  fcb_filter_plan* pl = nullptr;
+  FCB_TRY(fcb_filter_plan_create(nviews, H, W, outType, window, &pl));
+  int rc = fcb_filter_plan_execute(pl, in, out, D, zOrigin, cosineWeight, stream);
+  // the plan's scratch is freed below; wait for the queued work that uses it
+  const cudaError_t e = cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
+  fcb_filter_plan_destroy(pl);
+  if (rc) return rc;
+  if (e != cudaSuccess) return set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
+  return ok();
 }
 
 extern "C" int fcb_phantom_device(float* vol, const int volDim[3], const double* params, int n,

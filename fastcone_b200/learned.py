@@ -49,6 +49,7 @@ class Operators:
         self.Bplan = ops.BackprojectPlan(self.g, mode=_lib.MODE_UNWEIGHTED)
         gf = configs.with_fdk_norm(self.g)
         self.fdk_plan = ops.BackprojectPlan(gf, mode=_lib.MODE_FDK)
+        self.filter_plan = ops.FilterPlan(self.g.proj_shape)
         dev = torch.device("cuda", torch.cuda.current_device())
         ones_v = torch.ones(self.g.vol_shape, device=dev)
         ones_p = torch.ones(self.g.proj_shape, device=dev)
@@ -63,7 +64,7 @@ class Operators:
         return self.C * self.B((y - self.A(x)) * self.R)
 
     def fdk(self, y):
-        f = ops.fdk_filter(y, self.g)
+        f = self.filter_plan(y, zorigin=self.g.hmid, D=self.g.D)
         v = torch.zeros(self.g.vol_shape, device=y.device)
         # the reference's FDK scale is pw times the attenuation (pw = 1 voxel here)
         return self.fdk_plan(f, v).mul_(1.0 / self.g.pw).clamp_(min=0.0)
@@ -97,17 +98,19 @@ class UnrolledNet(torch.nn.Module):
 
     @staticmethod
     def pack(x, g):
-        """[x, g] -> channels-last BF16 with 16 channels (14 zero)."""
-        t = torch.zeros(x.shape + (16,), device=x.device, dtype=torch.bfloat16)
-        t[..., 0] = (x * X_SCALE).to(torch.bfloat16)
-        t[..., 1] = (g * X_SCALE).to(torch.bfloat16)
+        """[x, g] -> BF16 activations of 16 channels (14 zero) in the convolution layout
+        [nz, ny, 2, nx, 8]."""
+        nz, ny, nx = x.shape
+        t = torch.zeros((nz, ny, 2, nx, 8), device=x.device, dtype=torch.bfloat16)
+        t[:, :, 0, :, 0] = (x * X_SCALE).to(torch.bfloat16)
+        t[:, :, 0, :, 1] = (g * X_SCALE).to(torch.bfloat16)
         return t
 
     def step(self, k, x, g):
         h = self.pack(x, g)
         for layer in self.blocks[k]:
             h = layer(h)
-        return h[..., 0].float() / X_SCALE
+        return h[:, :, 0, :, 0].float() / X_SCALE
 
     def forward(self, x0, y, ops_: Operators, callback=None):
         x = x0

@@ -1,7 +1,9 @@
 """3x3x3 convolutions on the tcgen05 kernels, as torch autograd functions.
 
-Activations are channels-last BF16 volumes ``[nz, ny, nx, 16]``; a layer with fewer channels
-is zero-padded to 16 (the kernels' fixed width).  Forward and input gradient run the
+Activations are BF16 volumes of 16 channels in the kernels' channel-half-major layout
+``[nz, ny, 2, nx, 8]`` (channel c at ``[:, :, c // 8, :, c % 8]``; ``to_layout`` /
+``from_layout`` convert from / to ``[16, nz, ny, nx]``); a layer with fewer channels is
+zero-padded to 16 (the kernels' fixed width).  Forward and input gradient run the
 tensor-core kernel (``fcb_conv3d16_device``), the weight gradient the CUDA-core reduction
 (``fcb_conv3d16_wgrad_device``); master weights stay FP32 and are rounded to BF16 per call.
 """
@@ -32,14 +34,32 @@ def from_kernel_weights(wk: torch.Tensor) -> torch.Tensor:
     return wk.reshape(3, 3, 3, wk.shape[1], wk.shape[2]).permute(3, 4, 0, 1, 2)
 
 
+def to_layout(t: torch.Tensor) -> torch.Tensor:
+    """[16, nz, ny, nx] -> the kernels' [nz, ny, 2, nx, 8]."""
+    c, nz, ny, nx = t.shape
+    return t.reshape(2, 8, nz, ny, nx).permute(2, 3, 0, 4, 1).contiguous()
+
+
+def from_layout(t: torch.Tensor) -> torch.Tensor:
+    """[nz, ny, 2, nx, 8] -> [16, nz, ny, nx]."""
+    nz, ny, _, nx, _ = t.shape
+    return t.permute(2, 4, 0, 1, 3).reshape(16, nz, ny, nx)
+
+
+def _check_act(x: torch.Tensor, name: str):
+    if x.dim() != 5 or x.shape[2] != 2 or x.shape[4] != 8 or not x.is_contiguous():
+        raise ValueError(f"{name} must be contiguous [nz, ny, 2, nx, 8]")
+
+
 def conv3d16(x: torch.Tensor, wk: torch.Tensor, bias: torch.Tensor | None = None, relu: bool = False,
              out_dtype=torch.bfloat16) -> torch.Tensor:
-    """y = act(conv3d(x, w) + b); x BF16 [nz, ny, nx, 16], wk BF16 [27, 16, 16]."""
-    if x.dtype != torch.bfloat16 or x.dim() != 4 or x.shape[-1] != 16 or not x.is_contiguous():
-        raise ValueError("x must be contiguous BF16 [nz, ny, nx, 16]")
+    """y = act(conv3d(x, w) + b); x BF16 [nz, ny, 2, nx, 8], wk BF16 [27, 16, 16]."""
+    _check_act(x, "x")
+    if x.dtype != torch.bfloat16:
+        raise ValueError("x must be BF16")
     wk = wk.to(torch.bfloat16).contiguous()
-    nz, ny, nx, _ = x.shape
-    y = torch.empty((nz, ny, nx, 16), device=x.device, dtype=out_dtype)
+    nz, ny, _, nx, _ = x.shape
+    y = torch.empty(x.shape, device=x.device, dtype=out_dtype)
     b = bias.float().contiguous() if bias is not None else None
     check(lib().fcb_conv3d16_device(_p(x), _p(wk), _p(b) if b is not None else None, _p(y),
                                     _lib.FCB_F32 if out_dtype == torch.float32 else _lib.FCB_BF16,
@@ -48,8 +68,9 @@ def conv3d16(x: torch.Tensor, wk: torch.Tensor, bias: torch.Tensor | None = None
 
 
 def conv3d16_wgrad(x: torch.Tensor, gy: torch.Tensor) -> torch.Tensor:
-    """dW[t][co][ci] = sum_v gy[v][co] x[v + tap t][ci] (FP32)."""
-    nz, ny, nx, _ = x.shape
+    """dW[t][co][ci] = sum_v gy[v][co] x[v + tap t][ci] (FP32); both [nz, ny, 2, nx, 8]."""
+    _check_act(x, "x")
+    nz, ny, _, nx, _ = x.shape
     dw = torch.zeros((27, 16, 16), device=x.device, dtype=torch.float32)
     gy = gy.contiguous()
     check(lib().fcb_conv3d16_wgrad_device(_p(x), _p(gy), _lib.FCB_F32 if gy.dtype == torch.float32 else _lib.FCB_BF16,
@@ -78,7 +99,7 @@ class Conv3d16Function(torch.autograd.Function):
         gx = conv3d16(gb, wt, None, relu=False, out_dtype=torch.float32).to(torch.bfloat16)
         dwk = conv3d16_wgrad(x, gb)
         dw = from_kernel_weights(dwk)
-        db = g.sum(dim=(0, 1, 2))
+        db = g.sum(dim=(0, 1, 3)).reshape(16)
         return gx, dw, db, None
 
 

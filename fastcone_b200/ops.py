@@ -178,6 +178,39 @@ def fdk_filter(proj: torch.Tensor, geom: ConeGeometry | None = None, out_dtype=t
     return out
 
 
+class FilterPlan:
+    """Reusable FDK filter (cosine weight + ramp / Shepp-Logan) for projections of shape
+    (nviews, H, W): cuFFT plans and scratch made once; calls are stream-ordered, allocate
+    nothing and do not synchronise."""
+
+    def __init__(self, shape, out_dtype=torch.float32, window: int = _lib.FILTER_RAMLAK):
+        self.shape = tuple(int(v) for v in shape)
+        self.out_dtype = out_dtype
+        self._h = ctypes.c_void_p()
+        n, H, W = self.shape
+        check(lib().fcb_filter_plan_create(n, H, W, _DTYPES[out_dtype], int(window), ctypes.byref(self._h)))
+
+    def __call__(self, proj: torch.Tensor, zorigin=None, D: float | None = None, cosine_weight: bool = True,
+                 out: torch.Tensor | None = None) -> torch.Tensor:
+        if tuple(proj.shape) != self.shape:
+            raise ValueError("projection shape does not match the plan")
+        if out is None:
+            out = torch.empty(self.shape, device=proj.device, dtype=self.out_dtype)
+        z = np.ascontiguousarray(np.asarray(zorigin if zorigin is not None else np.zeros(self.shape[0]), np.float32))
+        check(lib().fcb_filter_plan_execute(self._h, _dev(proj, "proj", torch.float32), _dev(out, "out"),
+                                            float(D or 0.0), z.ctypes.data_as(_lib.c_float_p),
+                                            1 if cosine_weight else 0, _stream()))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            try:
+                lib().fcb_filter_plan_destroy(self._h)
+            except Exception:
+                pass
+            self._h = ctypes.c_void_p()
+
+
 def katsevich_filter(proj: torch.Tensor, geom: ConeGeometry, n_kappa: int = 0,
                      out: torch.Tensor | None = None) -> torch.Tensor:
     """Katsevich filtering of helical projections (float32 (n, H, W)) for geom's helix."""

@@ -203,6 +203,16 @@ int fcb_fdk_filter_device(const float* in, void* out, int outType, int nviews, i
                           float D, const float* zOrigin, int cosineWeight, int window,
                           void* stream);
 
+/* The same filter as a reusable plan: cuFFT plans, scratch and the filter response are made
+ * once; execute is stream-ordered, allocates nothing and does not synchronise (zOrigin, host,
+ * is read before it returns).  One execute at a time per plan (the scratch is the plan's). */
+typedef struct fcb_filter_plan fcb_filter_plan;
+int fcb_filter_plan_create(int nviews, int H, int W, int outType, int window,
+                           fcb_filter_plan** plan);
+int fcb_filter_plan_execute(fcb_filter_plan* plan, const float* in, void* out, float D,
+                            const float* zOrigin, int cosineWeight, void* stream);
+int fcb_filter_plan_destroy(fcb_filter_plan* plan);
+
 /* Katsevich filtering of helical projections (no counterpart in the reference, whose
  * Katsevich backprojection, coneBeamGPU.cu:258-338, expects pre-filtered data): derivative
  * at fixed ray direction, length correction, rebinning onto nkappa kappa-lines (<= 1: 2H),
@@ -216,16 +226,18 @@ int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, 
                                 void* stream);
 
 /* 3x3x3 convolution, 16 -> 16 channels, stride 1, zero padding 1, on the tcgen05 tensor
- * cores (BF16 inputs, FP32 accumulation).  x: BF16 [nz][ny][nx][16] (channels last), w: BF16
- * [27 taps (dz,dy,dx) z-major][16 out][16 in], bias: 16 floats or NULL, y: [nz][ny][nx][16] of
- * yType (FCB_F32 / FCB_BF16), ReLU applied when relu != 0.  Buffers 16-byte aligned.  The
- * input gradient is the same call with dY as x and w'[t][ci][co] = w[26 - t][co][ci].
- * No counterpart in the reference (the learned reconstruction is new). */
+ * cores (BF16 inputs, FP32 accumulation).  Activations in the channel-half-major layout
+ * [nz][ny][2][nx][8] (channel c of voxel (x,y,z) at ((z*ny + y)*2 + c/8)*nx*8 + x*8 + c%8).
+ * x: BF16, w: BF16 [27 taps (dz,dy,dx) z-major][16 out][16 in], bias: 16 floats or NULL,
+ * y: the same layout, of yType (FCB_F32 / FCB_BF16), ReLU applied when relu != 0.  Buffers
+ * 16-byte aligned.  The input gradient is the same call with dY as x and
+ * w'[t][ci][co] = w[26 - t][co][ci].  No counterpart in the reference (the learned
+ * reconstruction is new). */
 int fcb_conv3d16_device(const void* x, const void* w, const float* bias, void* y, int yType, int nx,
                         int ny, int nz, int relu, void* stream);
 
 /* Weight gradient of fcb_conv3d16_device: dw[t][co][ci] += sum_v dy[v][co] x[v + tap t][ci]
- * (FP32, accumulated); dy of dyType (FCB_F32 / FCB_BF16), x BF16. */
+ * (FP32, accumulated); dy of dyType (FCB_F32 / FCB_BF16), x BF16, both [nz][ny][2][nx][8]. */
 int fcb_conv3d16_wgrad_device(const void* x, const void* dy, int dyType, float* dw, int nx, int ny,
                               int nz, void* stream);
 

@@ -6,15 +6,26 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _ref(x_cl, w, b, relu):
+def _ref(x_l, w, b, relu):
     import torch
     import torch.nn.functional as F
 
-    x = x_cl.float().permute(3, 0, 1, 2).unsqueeze(0)          # [1, C, z, y, x]
+    from fastcone_b200 import nn
+
+    x = nn.from_layout(x_l).float().unsqueeze(0)                 # [1, C, z, y, x]
     y = F.conv3d(x, w.float(), b.float(), padding=1)
     if relu:
         y = torch.relu(y)
-    return y.squeeze(0).permute(1, 2, 3, 0)                      # [z, y, x, C]
+    return nn.to_layout(y.squeeze(0))                            # [z, y, 2, x, 8]
+
+
+def _act(shape, g, dtype=None):
+    import torch
+
+    from fastcone_b200 import nn
+
+    t = nn.to_layout(torch.randn((16,) + tuple(shape), device="cuda", generator=g))
+    return t.to(dtype) if dtype is not None else t
 
 
 def _rel(a, b):
@@ -29,7 +40,7 @@ def test_conv_forward_vs_torch(shape, relu):
     from fastcone_b200 import nn
 
     g = torch.Generator(device="cuda").manual_seed(0)
-    x = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
+    x = _act(shape, g, torch.bfloat16)
     w = (torch.randn(16, 16, 3, 3, 3, device="cuda", generator=g) * 0.1).to(torch.bfloat16).float()
     b = torch.randn(16, device="cuda", generator=g)
     y = nn.conv3d16(x, nn.to_kernel_weights(w).to(torch.bfloat16).contiguous(), b, relu=relu,
@@ -46,10 +57,10 @@ def test_conv_gradients_vs_torch():
 
     g = torch.Generator(device="cuda").manual_seed(1)
     shape = (12, 10, 140)
-    x = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
+    x = _act(shape, g, torch.bfloat16)
     w = (torch.randn(16, 16, 3, 3, 3, device="cuda", generator=g) * 0.1).to(torch.bfloat16).float()
     b = torch.randn(16, device="cuda", generator=g) * 0.1
-    gy = torch.randn(shape + (16,), device="cuda", generator=g)
+    gy = _act(shape, g)
 
     # ours: gradients through the custom function
     xin = x.clone().requires_grad_(True)
@@ -58,12 +69,12 @@ def test_conv_gradients_vs_torch():
     y2 = nn.Conv3d16Function.apply(xin, w2, b2, True)
     (y2.float() * gy).sum().backward()
     # reference in FP32
-    xr = x.float().permute(3, 0, 1, 2).unsqueeze(0).clone().requires_grad_(True)
+    xr = nn.from_layout(x).float().unsqueeze(0).clone().requires_grad_(True)
     wr = w.clone().requires_grad_(True)
     br = b.clone().requires_grad_(True)
-    yr = torch.relu(F.conv3d(xr, wr, br, padding=1)).squeeze(0).permute(1, 2, 3, 0)
+    yr = nn.to_layout(torch.relu(F.conv3d(xr, wr, br, padding=1)).squeeze(0))
     (yr * gy).sum().backward()
-    gx_ref = xr.grad.squeeze(0).permute(1, 2, 3, 0)
+    gx_ref = nn.to_layout(xr.grad.squeeze(0))
     assert _rel(xin.grad, gx_ref) < 1e-2
     assert _rel(w2.grad, wr.grad) < 1e-2
     assert _rel(b2.grad, br.grad) < 1e-2
@@ -79,7 +90,7 @@ def test_persistent_conv_equals_one_tile_per_cta(shape, monkeypatch):
     from fastcone_b200 import nn
 
     g = torch.Generator(device="cuda").manual_seed(1)
-    x = torch.randn(shape + (16,), device="cuda", generator=g).to(torch.bfloat16)
+    x = _act(shape, g, torch.bfloat16)
     wk = (torch.randn(27, 16, 16, device="cuda", generator=g) * 0.1).to(torch.bfloat16)
     b = torch.randn(16, device="cuda", generator=g)
     monkeypatch.delenv("FCB_CONV_SIMPLE", raising=False)
