@@ -12,12 +12,16 @@
 //      and length correction g2 = D / sqrt(u^2+D^2+v^2) g1      (deriv_kernel)
 //   2. forward height rebinning onto kappa-lines v_k(u, psi) = P/(2 pi)(psi + psi/tan(psi) u/D)
 //      (rebin_fwd_kernel, per-(kappa, column) interpolation table built on the host in FP64)
-//   3. Hilbert transform along u, band-limited kernel (1 - cos(pi n))/(pi n) (hilbert_kernel)
+//   3. Hilbert transform along u, band-limited kernel (1 - cos(pi n))/(pi n): a linear
+//      convolution done with cuFFT (kernel spectrum in FP64 on the host); kats_hilbert_kernel
+//      is the direct O(W^2) form, kept for comparison
 //   4. backward rebinning through the kappa-line of smallest |psi| (rebin_bwd_kernel,
 //      per-(row, column) table).
 // Backprojection with weight U over each voxel's PI interval and norm dlam/(2 pi D) then
 // reconstructs (fdk_tma_kernel with the Tam-Danielsson window).
+#include <cufft.h>
 #include <math.h>
+#include <stdlib.h>
 
 #include <algorithm>
 #include <vector>
@@ -99,6 +103,39 @@ __global__ void kats_hilbert_kernel(const float* __restrict__ in, float* __restr
     for (int j = (i & 1) ^ 1; j < W; j += 2) acc = fmaf(row[j], __frcp_rn((float)(i - j)), acc);
     out[r * W + i] = c * acc;
   }
+}
+
+// FFT form of the same transform: rows zero-padded to L = 2W (linear, not circular,
+// convolution for |i - j| < W), multiplied by the spectrum of the discrete kernel, inverted.
+__global__ void kats_pad_kernel(const float* __restrict__ in, float* __restrict__ pad, long long row0,
+                                int nrows, int W, int L)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nrows * L) return;
+  const int c = (int)(i % L);
+  const long long r = i / L;
+  pad[i] = c < W ? in[(row0 + r) * W + c] : 0.0f;
+}
+
+// spec[r][k] *= i * himag[k] (the kernel is odd, so its spectrum is purely imaginary)
+__global__ void kats_spec_kernel(cufftComplex* __restrict__ spec, const float* __restrict__ himag,
+                                 int nrows, int nb)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nrows * nb) return;
+  const float h = himag[i % nb];
+  const cufftComplex z = spec[i];
+  spec[i] = make_cuFloatComplex(-z.y * h, z.x * h);
+}
+
+__global__ void kats_crop_kernel(const float* __restrict__ pad, float* __restrict__ out, long long row0,
+                                 int nrows, int W, int L, float scale)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nrows * W) return;
+  const int c = (int)(i % W);
+  const long long r = i / W;
+  out[(row0 + r) * W + c] = scale * pad[r * L + c];
 }
 
 // gF[t][j][i] = g4[t][k0][i] * (1-a) + g4[t][k0+1][i] * a from the (row, column) table
@@ -193,6 +230,9 @@ extern "C" int fcb_katsevich_filter_device(const float* in, float* out, int nvie
   const size_t nhw = (size_t)nviews * H * W, nkw = (size_t)nviews * K * W;
   float *g2 = nullptr, *g3 = nullptr, *g4 = nullptr, *dfa = nullptr, *dba = nullptr;
   int *dfj = nullptr, *dbk = nullptr;
+  float *hpad = nullptr, *dhim = nullptr;
+  cufftComplex* hspec = nullptr;
+  cufftHandle pf = 0, pi = 0;
   int rc = FCB_OK;
   do {
     if (cudaMalloc(&g2, nhw * 4) || cudaMalloc(&g3, nkw * 4) || cudaMalloc(&g4, nkw * 4) ||
@@ -210,13 +250,57 @@ extern "C" int fcb_katsevich_filter_device(const float* in, float* out, int nvie
                                                                      pw, D, (float)su);
     kats_rebin_fwd_kernel<<<(unsigned)((nkw + 255) / 256), 256, 0, st>>>(g2, g3, dfj, dfa, nviews, H, W, K);
     // the published Hilbert transform runs along increasing u; along w it changes sign when u = -w
-    kats_hilbert_kernel<<<(unsigned)((size_t)nviews * K), 256, W * sizeof(float), st>>>(g3, g4, W,
-                                                                                        (float)su);
+    const char* direct = getenv("FCB_KATS_DIRECT_HILBERT");
+    if (direct && direct[0] == '1') {
+      kats_hilbert_kernel<<<(unsigned)((size_t)nviews * K), 256, W * sizeof(float), st>>>(g3, g4, W,
+                                                                                          (float)su);
+    } else {
+      // spectrum of the kernel embedded in L = 2W: h(m) = 2/(pi m) for odd m, h(L-m) = -h(m);
+      // H[k] = sum_m h(m) e^{-2 pi i k m / L} = -2 i sum_{m odd < W} h(m) sin(2 pi k m / L)
+      const int L = 2 * W, nb = W + 1;
+      std::vector<float> himag(nb);
+      for (int k = 0; k < nb; k++) {
+        double acc = 0.0;
+        for (int m = 1; m < W; m += 2) acc += (2.0 / (M_PI * m)) * sin(2.0 * M_PI * (double)k * m / L);
+        himag[k] = (float)(-2.0 * acc);
+      }
+      const long long rows = (long long)nviews * K;
+      const int batch = (int)std::min<long long>(rows, std::max<long long>(1, (256ll << 20) / (8ll * L)));
+      if (cudaMalloc(&hpad, (size_t)batch * L * 4) || cudaMalloc(&hspec, (size_t)batch * nb * sizeof(cufftComplex)) ||
+          cudaMalloc(&dhim, nb * 4)) {
+        cudaGetLastError();
+        rc = set_error(FCB_ERR_NOMEM, "Katsevich filter scratch");
+        break;
+      }
+      cudaMemcpyAsync(dhim, himag.data(), nb * 4, cudaMemcpyHostToDevice, st);
+      int n1[1] = {L};
+      if (cufftPlanMany(&pf, 1, n1, nullptr, 1, L, nullptr, 1, nb, CUFFT_R2C, batch) != CUFFT_SUCCESS ||
+          cufftPlanMany(&pi, 1, n1, nullptr, 1, nb, nullptr, 1, L, CUFFT_C2R, batch) != CUFFT_SUCCESS ||
+          cufftSetStream(pf, st) != CUFFT_SUCCESS || cufftSetStream(pi, st) != CUFFT_SUCCESS) {
+        rc = set_error(FCB_ERR_CUDA, "cufftPlanMany failed");
+        break;
+      }
+      const float scale = (float)su / (float)L;
+      for (long long r0 = 0; r0 < rows && !rc; r0 += batch) {
+        const int nr = (int)std::min<long long>(batch, rows - r0);
+        kats_pad_kernel<<<(unsigned)(((long long)batch * L + 255) / 256), 256, 0, st>>>(g3, hpad, r0, nr, W, L);
+        if (nr < batch) cudaMemsetAsync(hpad + (size_t)nr * L, 0, (size_t)(batch - nr) * L * 4, st);
+        if (cufftExecR2C(pf, hpad, hspec) != CUFFT_SUCCESS) { rc = set_error(FCB_ERR_CUDA, "cufftExecR2C failed"); break; }
+        kats_spec_kernel<<<(unsigned)(((long long)nr * nb + 255) / 256), 256, 0, st>>>(hspec, dhim, nr, nb);
+        if (cufftExecC2R(pi, hspec, hpad) != CUFFT_SUCCESS) { rc = set_error(FCB_ERR_CUDA, "cufftExecC2R failed"); break; }
+        kats_crop_kernel<<<(unsigned)(((long long)nr * W + 255) / 256), 256, 0, st>>>(hpad, g4, r0, nr, W, L, scale);
+      }
+      if (rc) break;
+    }
     kats_rebin_bwd_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(g4, out, dbk, dba, nviews, H, W, K);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
   } while (0);
+  if (rc) cudaStreamSynchronize(st);  // nothing queued may still use the scratch freed below
+  if (pf) cufftDestroy(pf);
+  if (pi) cufftDestroy(pi);
   cudaFree(g2); cudaFree(g3); cudaFree(g4); cudaFree(dfa); cudaFree(dba); cudaFree(dfj); cudaFree(dbk);
+  cudaFree(hpad); cudaFree(hspec); cudaFree(dhim);
   return rc ? rc : ok();
 }
