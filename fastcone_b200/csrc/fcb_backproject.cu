@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "fcb_internal.h"
@@ -195,6 +196,25 @@ struct Tap<__nv_bfloat16, OFF> {
   static __device__ __forceinline__ float ld(uint32_t a) { return __uint_as_float(lds_u16<OFF * 2>(a) << 16); }
 };
 
+// ---- 16-bit staged boxes widened to FP32 (8 values per 16-byte load)
+template <typename T>
+__device__ __forceinline__ float wide16(uint32_t bits16);
+template <>
+__device__ __forceinline__ float wide16<__nv_bfloat16>(uint32_t b) { return __uint_as_float(b << 16); }
+template <>
+__device__ __forceinline__ float wide16<__half>(uint32_t b)
+{
+  return __half2float(__ushort_as_half((unsigned short)b));
+}
+template <typename T>
+__device__ __forceinline__ void widen8(uint4 q, float4& lo, float4& hi)
+{
+  lo = make_float4(wide16<T>(q.x & 0xffffu), wide16<T>(q.x >> 16), wide16<T>(q.y & 0xffffu),
+                   wide16<T>(q.y >> 16));
+  hi = make_float4(wide16<T>(q.z & 0xffffu), wide16<T>(q.z >> 16), wide16<T>(q.w & 0xffffu),
+                   wide16<T>(q.w >> 16));
+}
+
 // ---- packed FP32 pairs (sm_100 f32x2 arithmetic): two z-voxels per instruction
 __device__ __forceinline__ u64 pk2(float lo, float hi)
 {
@@ -242,12 +262,20 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
 {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int ES = (int)sizeof(T);
+  // 16-bit storage with the pair path: each staged box is widened into one of two FP32
+  // buffers by the consumers, which then interpolate exactly as for FP32 storage
+  constexpr bool CVT = X2 && ES == 2;
+  using TC = typename std::conditional<CVT, float, T>::type;
+  constexpr int ESC = (int)sizeof(TC);
   const int stage_elems = P.BW * P.BH;
   const int stage_bytes = ((stage_elems * ES) + 127) & ~127;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)P.stages * stage_bytes);
   uint64_t* empty = full + P.stages;
-  int4* origin = reinterpret_cast<int4*>(empty + P.stages);  // box origin w, h; view (-1: end)
+  // per stage: box origin w, h; view (-1: end of the list); rows the tile's footprint needs
+  int4* origin = reinterpret_cast<int4*>(empty + P.stages);
   const uint32_t smem_base = dev::smem_u32(smem_raw);
+  const int fbuf_bytes = ((stage_elems * 4) + 127) & ~127;
+  const size_t fbuf_off = ((size_t)P.stages * stage_bytes + (size_t)P.stages * 32 + 127) & ~(size_t)127;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int tx, ty, tz;
@@ -293,7 +321,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
               ok = 0;
             } else {
               if (snw > P.BW || snh > P.BH) dev::record_status(P.status, DEV_RANGE);
-              origin[s] = make_int4(sw0, sh0, vb + l, 0);
+              origin[s] = make_int4(sw0, sh0, vb + l, snh);
               dev::mbar_arrive_expect_tx(&full[s], bytes);
               dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], sw0, sh0,
                                P.view0 + vb + l);
@@ -321,7 +349,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
           }
         }
         if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
-        origin[s] = make_int4(w0, h0, v, 0);
+        origin[s] = make_int4(w0, h0, v, nh);
         dev::mbar_arrive_expect_tx(&full[s], bytes);
         dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + v);
         issued++;
@@ -353,7 +381,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   const float x = P.ox + (float)xl, y = P.oy + (float)yl, zf = P.oz + (float)zl;
   const float MAGIC = 12582912.0f;  // 1.5 * 2^23: adding it in round-down mode floors
   const uint32_t MAGIC_BITS = 0x4B400000u;
-  const uint32_t rowb = (uint32_t)(P.BW * ES);  // bytes per staged row
+  const uint32_t rowb = (uint32_t)(P.BW * ESC);  // bytes per row of the box read below
 
   constexpr int NACC = X2 ? NZ / 2 : NZ;
   static_assert(!X2 || (NZ % 2 == 0), "pairs");
@@ -369,13 +397,53 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   // window: only views that reach the tile, then an end marker)
   for (int j = 0; PIW || j < P.nviews; j++) {
     const int s = j % P.stages;
-    if (!dev::mbar_wait(&full[s], (j / P.stages) & 1)) {
-      dev::record_status(P.status, DEV_TIMEOUT);
-      return;
+    bool okw = dev::mbar_wait(&full[s], (j / P.stages) & 1);
+    if constexpr (!CVT) {
+      if (!okw) {
+        dev::record_status(P.status, DEV_TIMEOUT);
+        return;
+      }
     }
     const int4 org = origin[s];
     const int v = PIW ? org.z : j;
-    if (PIW && v < 0) break;
+    if (!CVT && PIW && v < 0) break;
+    uint32_t fbase = 0;
+    if constexpr (CVT) {
+      // widen the staged 16-bit box into FP32 buffer j & 1 (16-byte chunks: 8 values), free
+      // the stage for the producer, and meet the other consumer warps; the barrier also
+      // makes the outcome of the wait uniform (a warp that timed out leaves with the rest)
+      float* fb = reinterpret_cast<float*>(smem_raw + fbuf_off + (size_t)(j & 1) * fbuf_bytes);
+      const bool real = okw && !(PIW && v < 0);  // the end marker has no data
+      if (real) {
+        const uint4* src = reinterpret_cast<const uint4*>(smem_raw + (size_t)s * stage_bytes);
+        float4* dst = reinterpret_cast<float4*>(fb);
+        // only the rows this tile's footprint reaches (taps stay below row org.w - 1)
+        const int nconv = min(org.w, P.BH) * (P.BW / 8);
+        for (int e = threadIdx.x; e < nconv; e += FDK_CWARPS * 32) {
+          float4 lo, hi;
+          widen8<T>(src[e], lo, hi);
+          dst[2 * e] = lo;
+          dst[2 * e + 1] = hi;
+        }
+      }
+      __syncwarp();
+      if (lane == 0 && real) dev::mbar_arrive(&empty[s]);
+      int all_ok;
+      asm volatile(
+          "{\n\t.reg .pred p, q;\n\t"
+          "setp.ne.u32 p, %1, 0;\n\t"
+          "bar.red.and.pred q, 1, %2, p;\n\t"
+          "selp.u32 %0, 1, 0, q;\n\t}"
+          : "=r"(all_ok)
+          : "r"((uint32_t)okw), "n"(FDK_CWARPS * 32)
+          : "memory");
+      if (!all_ok) {
+        dev::record_status(P.status, DEV_TIMEOUT);
+        return;
+      }
+      if (PIW && v < 0) break;
+      fbase = dev::smem_u32(fb);
+    }
     const FdkView& V = P.v[v];
 
     const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
@@ -409,8 +477,8 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
     }
 
     // byte address of tap (row r, column iw) = bits(MAGIC + r) * rowb + base
-    const uint32_t base = smem_base + (uint32_t)s * (uint32_t)stage_bytes + (uint32_t)iw * ES -
-                          MAGIC_BITS * rowb;
+    const uint32_t base = (CVT ? fbase : smem_base + (uint32_t)s * (uint32_t)stage_bytes) +
+                          (uint32_t)iw * ESC - MAGIC_BITS * rowb;
     if constexpr (X2) {
       const u64 MAG2 = pk2(MAGIC, MAGIC);
       const u64 FW2 = pk2(fw, fw);
@@ -426,10 +494,10 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         const uint32_t a0 = (uint32_t)__float_as_uint(t0) * rowb + base;
         const uint32_t a1 = (uint32_t)__float_as_uint(t1) * rowb + base;
         const uint32_t c0 = a0 + rowb, c1 = a1 + rowb;
-        const u64 A = pk2(Tap<T, 0>::ld(a0), Tap<T, 0>::ld(a1));
-        const u64 B = pk2(Tap<T, 1>::ld(a0), Tap<T, 1>::ld(a1));
-        const u64 C = pk2(Tap<T, 0>::ld(c0), Tap<T, 0>::ld(c1));
-        const u64 Dd = pk2(Tap<T, 1>::ld(c0), Tap<T, 1>::ld(c1));
+        const u64 A = pk2(Tap<TC, 0>::ld(a0), Tap<TC, 0>::ld(a1));
+        const u64 B = pk2(Tap<TC, 1>::ld(a0), Tap<TC, 1>::ld(a1));
+        const u64 C = pk2(Tap<TC, 0>::ld(c0), Tap<TC, 0>::ld(c1));
+        const u64 Dd = pk2(Tap<TC, 1>::ld(c0), Tap<TC, 1>::ld(c1));
         const u64 R0 = fma2(FW2, sub2(B, A), A);
         const u64 R1 = fma2(FW2, sub2(Dd, C), C);
         const u64 VAL = fma2(FH, sub2(R1, R0), R0);
@@ -460,8 +528,10 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         acc[k] = fmaf(wk, val, acc[k]);
       }
     }
-    __syncwarp();
-    if (lane == 0) dev::mbar_arrive(&empty[s]);
+    if constexpr (!CVT) {
+      __syncwarp();
+      if (lane == 0) dev::mbar_arrive(&empty[s]);
+    }
   }
 
   if (xl < P.nx && yl < P.ny) {
@@ -625,7 +695,12 @@ template <typename T, int NZ, bool PIW, bool X2, int MINB = fdk_min_blocks<NZ>()
 int launch_fdk(fcb_bp_plan* pl, const CUtensorMap& map, int chunk, int tz0, int tz1, cudaStream_t st)
 {
   const size_t stage_bytes = ((size_t)pl->BW * pl->BH * sizeof(T) + 127) & ~(size_t)127;
-  const size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int4));
+  size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int4));
+  if (X2 && sizeof(T) == 2) {
+    // two FP32 buffers for the widened boxes (layout of fdk_tma_kernel)
+    const size_t fbuf = ((size_t)pl->BW * pl->BH * 4 + 127) & ~(size_t)127;
+    smem = ((smem + 127) & ~(size_t)127) + 2 * fbuf;
+  }
   auto kern = fdk_tma_kernel<T, NZ, PIW, X2, MINB>;
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int c = 0; c < (int)pl->fdk.size(); c++) {
@@ -805,7 +880,10 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
     } else {
       const size_t es = dtype_size(projType);
       const size_t stage_bytes = (((size_t)pl->BW * pl->BH * es) + 127) & ~(size_t)127;
-      int st = (int)(smem_budget / stage_bytes);
+      // 16-bit storage also keeps two FP32 buffers of the widened box in the budget
+      const size_t wide = es == 2 ? 2 * ((((size_t)pl->BW * pl->BH * 4) + 127) & ~(size_t)127) : 0;
+      int st = (int)(((size_t)smem_budget > wide + 2 * stage_bytes ? smem_budget - wide : 2 * stage_bytes) /
+                     stage_bytes);
       pl->stages = std::max(2, std::min(8, st));
       for (FdkParams& P : pl->fdk) {
         P.BW = pl->BW; P.BH = pl->BH; P.stages = pl->stages;
@@ -887,8 +965,9 @@ int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void
                            (uint64_t)pb.projWHSize[0] * pb.projWHSize[1] * es, pl->BW, pl->BH, 1));
     for (FdkParams& P : pl->fdk) P.vol = volume;
     const bool piw = pl->fdk[0].piwin != 0;
-    // FCB_FDK_SCALAR=1 selects the one-voxel-per-instruction FP32 path (for comparison)
-    static const bool scalar = getenv("FCB_FDK_SCALAR") && getenv("FCB_FDK_SCALAR")[0] == '1';
+    // FCB_FDK_SCALAR=1 selects the one-voxel-per-instruction paths (for comparison)
+    const char* scal = getenv("FCB_FDK_SCALAR");
+    const bool scalar = scal && scal[0] == '1';
     if (pl->ptype == FCB_F32 && scalar) {
       if (piw) FCB_TRY((launch_fdk<float, 32, true, false>(pl, map, chunk, tz0, tz1, st)));
       else FCB_TRY((launch_fdk<float, 32, false, false>(pl, map, chunk, tz0, tz1, st)));
@@ -905,12 +984,19 @@ int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void
     } else if (pl->ptype == FCB_F32) {
       if (piw) FCB_TRY((launch_fdk<float, 32, true, true>(pl, map, chunk, tz0, tz1, st)));
       else FCB_TRY((launch_fdk<float, 32, false, true>(pl, map, chunk, tz0, tz1, st)));
-    } else if (pl->ptype == FCB_F16) {
+    } else if (pl->ptype == FCB_F16 && scalar) {
+      // 16-bit taps read one by one (the path before widening, for comparison)
       if (piw) FCB_TRY((launch_fdk<__half, 32, true, false>(pl, map, chunk, tz0, tz1, st)));
       else FCB_TRY((launch_fdk<__half, 32, false, false>(pl, map, chunk, tz0, tz1, st)));
-    } else {
+    } else if (pl->ptype == FCB_BF16 && scalar) {
       if (piw) FCB_TRY((launch_fdk<__nv_bfloat16, 32, true, false>(pl, map, chunk, tz0, tz1, st)));
       else FCB_TRY((launch_fdk<__nv_bfloat16, 32, false, false>(pl, map, chunk, tz0, tz1, st)));
+    } else if (pl->ptype == FCB_F16) {
+      if (piw) FCB_TRY((launch_fdk<__half, 32, true, true>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<__half, 32, false, true>(pl, map, chunk, tz0, tz1, st)));
+    } else {
+      if (piw) FCB_TRY((launch_fdk<__nv_bfloat16, 32, true, true>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk<__nv_bfloat16, 32, false, true>(pl, map, chunk, tz0, tz1, st)));
     }
     return ok();
   }
