@@ -207,15 +207,18 @@ def run_case(args):
         b = torch.zeros(16, device=dev)
         res = {}
 
-        def fwd_simple():
-            os.environ["FCB_CONV_SIMPLE"] = "1"
-            try:
-                return nn.conv3d16(x, wk, b, relu=True)
-            finally:
-                os.environ.pop("FCB_CONV_SIMPLE", None)
+        def fwd_variant(v):
+            def run():
+                os.environ["FCB_CONV_SIMPLE"] = v
+                try:
+                    return nn.conv3d16(x, wk, b, relu=True)
+                finally:
+                    os.environ.pop("FCB_CONV_SIMPLE", None)
+            return run
 
         for name, fn in (("fwd", lambda: nn.conv3d16(x, wk, b, relu=True)),
-                         ("fwd_one_tile_per_cta", fwd_simple),
+                         ("fwd_one_tile_per_cta", fwd_variant("1")),
+                         ("fwd_persistent_no_row_reuse", fwd_variant("2")),
                          ("wgrad", lambda: nn.conv3d16_wgrad(x, x))):
             for _ in range(args.warmup):
                 fn()
@@ -248,6 +251,15 @@ def run_case(args):
             e1.record()
             torch.cuda.synchronize()
             res[name] = {"ms": e0.elapsed_time(e1) / args.steps, **(plan.info() if meth == _lib.PROJ_EXPLICIT else {})}
+            if meth != _lib.PROJ_TEXTURE:
+                # the transpose of the same plan
+                vt = plan.adjoint(p)
+                e0.record()
+                for _ in range(args.steps):
+                    plan.adjoint(p, vt)
+                e1.record()
+                torch.cuda.synchronize()
+                res[name]["adjoint_ms"] = e0.elapsed_time(e1) / args.steps
         print(json.dumps({"case": args.case, **res}))
     ops.sync_status()
     torch.cuda.synchronize()

@@ -110,7 +110,7 @@ constexpr int CV_TILE = 128;                  // voxels per CTA tile (MMA M)
 constexpr int CV_ROW = CV_TILE + 2;           // staged voxels per tap row (x halo)
 constexpr int CV_BOX_BYTES = CV_ROW * 16;     // one channel half of one tap row
 constexpr int CV_RB = 2176;                   // CV_BOX_BYTES rounded up to 128 B
-static_assert((CV_ROW + 2) / 2 * 32 <= CV_RB, "a box of voxel pairs fits its slot");
+static_assert((CV_ROW + 2) / 2 * 32 <= CV_RB && CV_BOX_BYTES <= CV_RB, "a staged box fits its slot");
 constexpr int CV_A_BYTES = 9 * 2 * CV_RB;     // 39168
 constexpr int CV_W_BYTES = 27 * 512;          // 13824
 constexpr int CV_SMEM = CV_A_BYTES + CV_W_BYTES + 64 + 32 + 16;
@@ -422,6 +422,207 @@ __global__ void __launch_bounds__(CVP_THREADS, 1) conv3d16p_kernel(const __grid_
   }
 }
 
+// Row-reusing form (default): a CTA walks chunks of CVR_YCH consecutive y rows of one
+// (x tile, z) column.  Neighbouring tiles share two of their three dy rows, so the input rows
+// live in a ring of 4 slots per dz (slot dz * 4 + (row & 3)) and each tile loads only its 3
+// new rows (9 at the start of a chunk): a third of the row traffic of conv3d16p_kernel.
+//   warp 4 (one lane): TMA producer; before refilling the slots of row y+1 it waits for
+//                      the MMAs of tile y-2, the last reader of the row it replaces;
+//   warp 5 (one lane): MMA issuer (27 MMAs per tile, taps addressed through the ring),
+//                      commits to the tile's done barrier and to the accumulator barrier;
+//   warps 0-3:         epilogue, as in conv3d16p_kernel.
+constexpr int CVR_YCH = 32;                 // rows per chunk
+constexpr int CVR_SLOTS = 12;               // 3 dz x 4 ring positions
+constexpr int CVR_THREADS = 192;
+constexpr int CVR_SMEM = CVR_SLOTS * 2 * CV_RB + CV_W_BYTES + 64 + 8 * (4 + 4 + 2 + 2) + 16;
+
+__global__ void __launch_bounds__(CVR_THREADS, 2) conv3d16r_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                                  const __grid_constant__ ConvParams P,
+                                                                  int nchunks)
+{
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* A = smem;
+  unsigned char* Wsm = smem + CVR_SLOTS * 2 * CV_RB;
+  float* bias = reinterpret_cast<float*>(Wsm + CV_W_BYTES);
+  uint64_t* rows_full = reinterpret_cast<uint64_t*>(Wsm + CV_W_BYTES + 64);  // [4] per tile
+  uint64_t* tile_done = rows_full + 4;                                         // [4] per tile
+  uint64_t* accf = tile_done + 4;                                              // [2]
+  uint64_t* acce = accf + 2;                                                   // [2]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ych = (P.ny + CVR_YCH - 1) / CVR_YCH;
+
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < 4; q++) {
+      dev::mbar_init(&rows_full[q], 1);
+      dev::mbar_init(&tile_done[q], 1);
+    }
+    for (int b = 0; b < 2; b++) {
+      dev::mbar_init(&accf[b], 1);
+      dev::mbar_init(&acce[b], 4);
+    }
+    dev::fence_mbar_init();
+  }
+  if (warp == 5) {
+    tc::tmem_alloc(tslot, 32);
+    tc::tmem_relinquish();
+  }
+  const uint4* wg = reinterpret_cast<const uint4*>(P.w);
+  for (int i = threadIdx.x; i < 27 * 16 * 2; i += blockDim.x) {
+    const int t = i / 32, n = (i / 2) % 16, kh = i % 2;
+    reinterpret_cast<uint4*>(Wsm + t * 512 + kh * 256 + n * 16)[0] = wg[(t * 16 + n) * 2 + kh];
+  }
+  if (threadIdx.x < 16) bias[threadIdx.x] = P.bias ? P.bias[threadIdx.x] : 0.0f;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t taddr = *tslot;
+
+  // chunk c -> x tile, z, rows [y0, y1)
+  auto chunk_of = [&](int c, int& x0, int& z, int& y0, int& y1) {
+    const int yc = c % ych, col = c / ych;
+    x0 = (col % P.tiles_x) * CV_TILE;
+    z = col / P.tiles_x;
+    y0 = yc * CVR_YCH;
+    y1 = min(P.ny, y0 + CVR_YCH);
+  };
+  int last = -1;  // tiles this CTA handles, minus one (same count in every role)
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    int x0, z, y0, y1;
+    chunk_of(c, x0, z, y0, y1);
+    last += y1 - y0;
+  }
+
+  if (warp == 4) {
+    // ---------------------------------------------------------------- TMA producer
+    if (lane == 0) {
+      dev::tma_prefetch(&xmap);
+      int i = 0, issued = 0;
+      bool failed = false;
+      for (int c = blockIdx.x; c < nchunks && !failed; c += gridDim.x) {
+        int x0, z, y0, y1;
+        chunk_of(c, x0, z, y0, y1);
+        for (int y = y0; y < y1; y++, i++) {
+          const bool start = y == y0;
+          // slots about to be refilled must be done with: tile i-2 (in a chunk) or every
+          // earlier tile (a new chunk replaces all rows)
+          const int wt = start ? i - 1 : i - 2;
+          if (wt >= 0 && !dev::mbar_wait(&tile_done[wt & 3], (wt >> 2) & 1)) {
+            dev::record_status(P.status, DEV_TIMEOUT);
+            failed = true;
+            break;
+          }
+          const int r0 = start ? -1 : 1;  // new rows y + r0 .. y + 1
+          const int nrows = 3 * (2 - r0);
+          dev::mbar_arrive_expect_tx(&rows_full[i & 3], (uint32_t)nrows * 2u * P.box_bytes);
+          for (int dz = 0; dz < 3; dz++)
+            for (int dy = r0; dy <= 1; dy++) {
+              const int yy = y + dy;
+              unsigned char* slot = A + (dz * 4 + (yy & 3)) * 2 * CV_RB;
+              for (int kh = 0; kh < 2; kh++)
+                tc::tma_load_5d(slot + kh * CV_RB, &xmap, &rows_full[i & 3], 0,
+                                P.pairs ? (x0 >> 1) - 1 : x0 - 1, kh, yy, z + dz - 1);
+            }
+          issued = i + 1;
+        }
+      }
+      for (int j = max(0, issued - 4); j < issued; j++)
+        dev::mbar_wait(&rows_full[j & 3], (j >> 2) & 1, 100000000ull);
+    }
+  } else if (warp == 5) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t wbase = dev::smem_u32(Wsm), abase = dev::smem_u32(A);
+      constexpr uint32_t IDESC = tc::idesc_bf16(CV_TILE, 16);
+      int i = 0;
+      bool failed = false;
+      for (int c = blockIdx.x; c < nchunks && !failed; c += gridDim.x) {
+        int x0, z, y0, y1;
+        chunk_of(c, x0, z, y0, y1);
+        for (int y = y0; y < y1; y++, i++) {
+          const int b = i & 1;
+          if (!dev::mbar_wait(&rows_full[i & 3], (i >> 2) & 1) ||
+              (i >= 2 && !dev::mbar_wait(&acce[b], ((i >> 1) - 1) & 1))) {
+            dev::record_status(P.status, DEV_TIMEOUT);
+            failed = true;
+            break;
+          }
+          tc::fence_after();
+          for (int t = 0; t < 27; t++) {
+            const int dz = t / 9, dy = (t / 3) % 3, dx = t % 3;
+            const int slot = dz * 4 + ((y + dy - 1) & 3);
+            const uint64_t ad = tc::smem_desc(abase + slot * 2 * CV_RB + (dx + P.pairs) * 16, CV_RB, 128);
+            const uint64_t bd = tc::smem_desc(wbase + t * 512, 256, 128);
+            tc::mma_bf16(taddr + (uint32_t)(b * 16), ad, bd, IDESC, t > 0 ? 1u : 0u);
+          }
+          tc::mma_commit(&tile_done[i & 3]);
+          tc::mma_commit(&accf[b]);
+        }
+      }
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue (warps 0-3)
+    int i = 0;
+    bool failed = false;
+    for (int c = blockIdx.x; c < nchunks && !failed; c += gridDim.x) {
+      int x0, z, y0, y1;
+      chunk_of(c, x0, z, y0, y1);
+      for (int y = y0; y < y1; y++, i++) {
+        const int b = i & 1;
+        if (!__all_sync(0xffffffffu, dev::mbar_wait(&accf[b], (i >> 1) & 1))) {
+          if (lane == 0) dev::record_status(P.status, DEV_TIMEOUT);
+          failed = true;
+          break;
+        }
+        tc::fence_after();
+        uint32_t r[16];
+        tc::tmem_ld16(taddr + (uint32_t)(b * 16) + ((uint32_t)(warp * 32) << 16), r);
+        tc::fence_before();
+        __syncwarp();
+        if (lane == 0) dev::mbar_arrive(&acce[b]);
+        const int xv = x0 + warp * 32 + lane;
+        if (xv < P.nx) {
+          float v[16];
+#pragma unroll
+          for (int q = 0; q < 16; q++) {
+            v[q] = __uint_as_float(r[q]) + bias[q];
+            if (P.relu) v[q] = fmaxf(v[q], 0.0f);
+          }
+          const size_t i0 = tc::act_index(xv, y, z, 0, P.nx, P.ny), i1 = tc::act_index(xv, y, z, 8, P.nx, P.ny);
+          if (P.out_f32) {
+            float4* o0 = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + i0);
+            float4* o1 = reinterpret_cast<float4*>(reinterpret_cast<float*>(P.out) + i1);
+            o0[0] = make_float4(v[0], v[1], v[2], v[3]);
+            o0[1] = make_float4(v[4], v[5], v[6], v[7]);
+            o1[0] = make_float4(v[8], v[9], v[10], v[11]);
+            o1[1] = make_float4(v[12], v[13], v[14], v[15]);
+          } else {
+            uint32_t pk[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+              __nv_bfloat162 bb = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
+              pk[q] = *reinterpret_cast<uint32_t*>(&bb);
+            }
+            __nv_bfloat16* ob = reinterpret_cast<__nv_bfloat16*>(P.out);
+            *reinterpret_cast<uint4*>(ob + i0) = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            *reinterpret_cast<uint4*>(ob + i1) = make_uint4(pk[4], pk[5], pk[6], pk[7]);
+          }
+        }
+      }
+    }
+  }
+  // every MMA issued must be complete before the columns are released
+  if (warp == 5 && lane == 0 && last >= 0) dev::mbar_wait(&accf[last & 1], (last >> 1) & 1, 100000000ull);
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 5) {
+    tc::fence_after();
+    tc::tmem_dealloc(taddr, 32);
+  }
+}
+
 // Weight gradient on the CUDA cores: dW[t][co][ci] += sum_v dY[v][co] * X[v + off(t)][ci].
 // Thread (co, ci) slides along a row of 128 voxels keeping the three x-neighbours of each of
 // the 9 tap rows in registers; CTAs loop over tiles and add their 27 partial sums once.
@@ -523,19 +724,25 @@ extern "C" int fcb_conv3d16_device(const void* x, const void* w, const float* bi
   P.status = status;
   const long long tiles = (long long)P.tiles_x * ny * nz;
   if (tiles > 0x7fffffffll) return set_error(FCB_ERR_RANGE, "conv3d volume too large");
-  // FCB_CONV_SIMPLE=1: one CTA per tile without the pipeline (for comparison)
+  // FCB_CONV_SIMPLE=1: one CTA per tile; FCB_CONV_SIMPLE=2: persistent without row reuse
+  // (for comparison); default: persistent with row reuse
   const char* env = getenv("FCB_CONV_SIMPLE");
-  const bool simple = env && env[0] == '1';
-  if (simple) {
+  const int variant = env ? atoi(env) : 0;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (variant == 1) {
     FCB_CUDA_TRY(cudaFuncSetAttribute(conv3d16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CV_SMEM));
     conv3d16_kernel<<<(unsigned)tiles, 128, CV_SMEM, st>>>(map, P);
-  } else {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  } else if (variant == 2) {
     FCB_CUDA_TRY(cudaFuncSetAttribute(conv3d16p_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CVP_SMEM));
     const int grid = (int)std::min<long long>(tiles, sms);
     conv3d16p_kernel<<<grid, CVP_THREADS, CVP_SMEM, st>>>(map, P, (int)tiles);
+  } else {
+    const long long nchunks = (long long)P.tiles_x * nz * ((ny + CVR_YCH - 1) / CVR_YCH);
+    FCB_CUDA_TRY(cudaFuncSetAttribute(conv3d16r_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CVR_SMEM));
+    const int grid = (int)std::min<long long>(nchunks, 2ll * sms);
+    conv3d16r_kernel<<<grid, CVR_THREADS, CVR_SMEM, st>>>(map, P, (int)nchunks);
   }
   FCB_CUDA_TRY(cudaGetLastError());
   return ok();

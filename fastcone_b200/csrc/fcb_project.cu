@@ -488,7 +488,11 @@ __global__ void __launch_bounds__(256) project_adjoint_brick_kernel(const __grid
   float s[3], d[3];
   int m0 = 1, m1 = 0;
   float y = 0.0f;
-  const int wl = bw0 + lane, hl = bh0 + warp;
+  // rays of a warp at least two pixels apart (one parity class of a 32 x 4 block): at the
+  // same step their taps rarely share a voxel, so one shared atomic instruction rarely
+  // serialises on an address
+  const int pc = warp & 3, rg = warp >> 2;
+  const int wl = bw0 + 2 * (lane & 15) + (pc & 1), hl = bh0 + 4 * rg + 2 * (lane >> 4) + (pc >> 1);
   if (wl < P.WH0 && hl < P.WH1) {
     y = V.wt * __ldg(P.proj + ((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl);
     ray_of(V, wl, hl, s, d);

@@ -80,11 +80,12 @@ def test_conv_gradients_vs_torch():
     assert _rel(b2.grad, br.grad) < 1e-2
 
 
-@pytest.mark.parametrize("shape", [(20, 17, 130), (4, 3, 512), (1, 1, 5), (37, 41, 300)])
+@pytest.mark.parametrize("shape", [(20, 17, 130), (4, 3, 512), (1, 1, 5), (37, 41, 300), (6, 70, 128)])
 def test_persistent_conv_equals_one_tile_per_cta(shape, monkeypatch):
-    """The persistent pipelined kernel (default) and the one-tile-per-CTA kernel issue the
-    same MMAs in the same order: identical outputs, including when a CTA owns many tiles
-    and when tiles are fewer than SMs."""
+    """The row-reusing persistent kernel (default), the persistent kernel without reuse and
+    the one-tile-per-CTA kernel issue the same MMAs in the same order: identical outputs,
+    including chunks of many rows (70 > one chunk of 32), CTAs with many chunks, and fewer
+    tiles than SMs."""
     import torch
 
     from fastcone_b200 import nn
@@ -94,8 +95,11 @@ def test_persistent_conv_equals_one_tile_per_cta(shape, monkeypatch):
     wk = (torch.randn(27, 16, 16, device="cuda", generator=g) * 0.1).to(torch.bfloat16)
     b = torch.randn(16, device="cuda", generator=g)
     monkeypatch.delenv("FCB_CONV_SIMPLE", raising=False)
-    y1 = nn.conv3d16(x, wk, b, relu=True, out_dtype=torch.float32)
+    y1 = nn.conv3d16(x, wk, b, relu=True, out_dtype=torch.float32)      # row reuse
     monkeypatch.setenv("FCB_CONV_SIMPLE", "1")
-    y2 = nn.conv3d16(x, wk, b, relu=True, out_dtype=torch.float32)
+    y2 = nn.conv3d16(x, wk, b, relu=True, out_dtype=torch.float32)      # one tile per CTA
+    monkeypatch.setenv("FCB_CONV_SIMPLE", "2")
+    y3 = nn.conv3d16(x, wk, b, relu=True, out_dtype=torch.float32)      # persistent, no reuse
     torch.cuda.synchronize()
     assert torch.equal(y1, y2)
+    assert torch.equal(y3, y2)
