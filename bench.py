@@ -39,13 +39,13 @@ VOXEL_MM, PITCH_MM, SOD_MM, SDD_MM = 0.25, 0.4, 500.0, 1000.0
 FDK_BYTES_PER_UPDATE = {"f32": 16, "bf16": 8}  # bilinear gather: 4 detector samples
 
 
-# DRAM bytes per FDK launch (1024^3, <= 900 views): ncu dram__bytes_read.sum +
-# dram__bytes_write.sum of the 128-plane / 64-view slab capture
-# (profiles/fdk_tma_kernel_fdk-slab.md), scaled per component: the volume read-modify-write
-# with the voxels (x8), the staged detector rows with voxels x views (x8 x 720 / 64 for the
-# mean launch of 720 views).
-FDK_TRAFFIC_PER_LAUNCH = round((2 * 0.540e9) * 8 + 0.123e9 * 8 * 720 / 64)
-FDK_TRAFFIC_NOTE = "scaled from the ncu slab capture (volume x8, detector rows x8 x 720/64 views)"
+# DRAM bytes per FDK launch (1024^3, 180 views per launch): ncu dram__bytes_read.sum +
+# dram__bytes_write.sum of every launch of one step of this benchmark (a one-pass capture of
+# `bench.py --steps 1 --warmup 1`), mean over the step's 8 launches; they range from 15.2 GB
+# (views near 0 and 180 degrees) to 68.3 GB (near 90 and 270 degrees), 326 GB per step
+# (profiles/fdk_tma_kernel_fdk-slab.md).
+FDK_TRAFFIC_PER_LAUNCH = 40.72e9
+FDK_TRAFFIC_NOTE = "measured by ncu on the 8 launches of one step (mean; 15.2-68.3 GB per launch)"
 
 
 def pi_window_fraction(g, nvox=4096, seed=0):
@@ -613,7 +613,7 @@ def main():
                    "parallelism": parallelism},
         "gpu_launches": launches_per_step * args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": FDK_TRAFFIC_PER_LAUNCH,
+                     "frac": achieved / hbm, "traffic": round(FDK_TRAFFIC_PER_LAUNCH),
                      "note": f"achieved = 16 B/update bilinear gather bytes per launch / launch time "
                              f"(CUDA events); peak = {peak_kind} HBM copy bandwidth. frac > 1: the gathers "
                              f"are served from shared memory (TMA-staged boxes), see smem_roofline; "

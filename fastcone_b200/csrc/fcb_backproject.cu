@@ -40,7 +40,8 @@ struct FdkView {
   float wt;      // normalisation factor of the view
 };
 
-constexpr int FDK_MAXV = 900;
+constexpr int FDK_MAXV = 900;      // views a launch's parameters can hold
+constexpr int FDK_L2_VIEWS = 180;  // views per launch by default (see bp_plan_build)
 constexpr int FDK_TX = 16, FDK_TY = 16;
 constexpr int FDK_CWARPS = 8;                          // consumer warps
 constexpr int FDK_THREADS = (FDK_CWARPS + 1) * 32;     // + producer warp
@@ -754,6 +755,15 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
     return set_error(FCB_ERR_INVALID, "unknown projection storage type");
   auto* pl = new fcb_bp_plan();
   pl->maxv = std::max(1, std::min(FDK_MAXV, maxViewsPerLaunch));
+  // Views per launch.  A launch's CTAs drift apart in view index, so what stays in L2 is a
+  // z-layer's detector rows of all the launch's views: at 1024^3 / 1536 x 1024, 900 views
+  // (343 MB) overflow the 126 MB L2 and each launch reads ~0.55 TB from HBM, while 180
+  // views keep it near the compulsory traffic (the volume's read-modify-write per launch)
+  // at the same speed (measured 909 vs 906 ms per 1440-view step).  With the PI window most
+  // views are skipped per tile, and the full launch size stays.
+  if (maxViewsPerLaunch >= FDK_MAXV && !(kernelMode == 1 && g && g->piWindow)) pl->maxv = FDK_L2_VIEWS;
+  // tuning knob: views per launch
+  if (const char* e = getenv("FCB_FDK_VIEWS")) pl->maxv = std::max(1, std::min(FDK_MAXV, atoi(e)));
   // tuning knobs: z-voxels per thread (16/32/64) and the shared-memory budget per CTA
   if (const char* e = getenv("FCB_FDK_NZ")) {
     const int nz = atoi(e);
