@@ -516,14 +516,17 @@ def main():
     torch.cuda.synchronize()
     ops.sync_status()
     ms_k = barrier_max(e0.elapsed_time(e1)) / kk
-    # Katsevich filtering of the same projections (synchronous entry point: host clock)
-    fk = ops.katsevich_filter(pk, gk)
+    # Katsevich filtering of the same projections through a filter plan (CUDA events)
+    kfp = ops.KatsevichPlan(gk)
+    fk = kfp(pk)
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ops.katsevich_filter(pk, gk, out=fk)
+    e0.record(st)
+    for _ in range(kk):
+        kfp(pk, fk)
+    e1.record(st)
     torch.cuda.synchronize()
-    ms_kf = (time.perf_counter() - t0) * 1e3
-    del fk
+    ms_kf = barrier_max(e0.elapsed_time(e1)) / kk
+    del fk, kfp
     dense = gk.vol_shape[0] * gk.vol_shape[1] * gk.vol_shape[2] * gk.nviews
     frac = pi_window_fraction(gk)
     katsevich = {"workload": "helical 512x512x384, 4 turns x 1160 views, 736x64 detector, PI window",

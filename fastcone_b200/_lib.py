@@ -46,6 +46,7 @@ EXPORTED_SYMBOLS = [
     "fcb_proj_plan_create", "fcb_proj_plan_execute", "fcb_proj_plan_destroy",
     "fcb_reference_windows", "fcb_proj_plan_info",
     "fcb_filter_plan_create", "fcb_filter_plan_execute", "fcb_filter_plan_destroy",
+    "fcb_katsevich_plan_create", "fcb_katsevich_plan_execute", "fcb_katsevich_plan_destroy",
 ]
 
 
@@ -127,6 +128,11 @@ def lib():
             L.fcb_filter_plan_create.argtypes = [ctypes.c_int] * 5 + [ctypes.POINTER(vp)]
             L.fcb_filter_plan_execute.argtypes = [vp, vp, vp, ctypes.c_float, c_float_p, ctypes.c_int, vp]
             L.fcb_filter_plan_destroy.argtypes = [vp]
+            L.fcb_katsevich_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_float_p,
+                                                    ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                                    ctypes.c_int, ctypes.POINTER(vp)]
+            L.fcb_katsevich_plan_execute.argtypes = [vp, vp, vp, vp]
+            L.fcb_katsevich_plan_destroy.argtypes = [vp]
             _lib = L
     return _lib
 

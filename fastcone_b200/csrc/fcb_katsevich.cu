@@ -175,13 +175,34 @@ static double frac_index(const std::vector<double>& xs, double x)
   return lo + (x - xs[lo]) / (xs[hi] - xs[lo]);
 }
 
-extern "C" int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, int W,
-                                           const float* angles, float D, float pw, float pitch,
-                                           int nkappa, void* stream)
+// Reusable Katsevich filter for one helix and detector: the kappa-line tables, the Hilbert
+// kernel's spectrum, the cuFFT plans and the intermediate buffers are made once; execute()
+// is stream-ordered, allocates nothing and does not synchronise.
+struct fcb_katsevich_plan {
+  int nviews = 0, H = 0, W = 0, K = 0, L = 0, nb = 0, batch = 0;
+  float dlam = 0.0f, pw = 0.0f, D = 0.0f, su = 0.0f;
+  float *g2 = nullptr, *g3 = nullptr, *g4 = nullptr, *dfa = nullptr, *dba = nullptr;
+  int *dfj = nullptr, *dbk = nullptr;
+  float *hpad = nullptr, *dhim = nullptr;
+  cufftComplex* hspec = nullptr;
+  cufftHandle pf = 0, pi = 0;
+  ~fcb_katsevich_plan()
+  {
+    if (pf) cufftDestroy(pf);
+    if (pi) cufftDestroy(pi);
+    cudaFree(g2); cudaFree(g3); cudaFree(g4); cudaFree(dfa); cudaFree(dba); cudaFree(dfj);
+    cudaFree(dbk); cudaFree(hpad); cudaFree(hspec); cudaFree(dhim);
+  }
+};
+
+extern "C" int fcb_katsevich_plan_create(int nviews, int H, int W, const float* angles, float D,
+                                         float pw, float pitch, int nkappa,
+                                         fcb_katsevich_plan** out)
 {
-  if (!in || !out || !angles || nviews < 2 || H < 2 || W < 2 || !(D > 0) || !(pw > 0) || pitch == 0.0f)
+  if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
+  *out = nullptr;
+  if (!angles || nviews < 2 || H < 2 || W < 2 || !(D > 0) || !(pw > 0) || pitch == 0.0f)
     return set_error(FCB_ERR_INVALID, "bad Katsevich filter arguments");
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   // mean angular step; float32 angles of several turns carry ~1e-6 rad of rounding each
   const double dlam = ((double)angles[nviews - 1] - (double)angles[0]) / (nviews - 1);
   for (int t = 1; t < nviews; t++) {
@@ -227,80 +248,112 @@ extern "C" int fcb_katsevich_filter_device(const float* in, float* out, int nvie
       ba[(size_t)j * W + i] = (float)(f - k0);
     }
   }
+  // spectrum of the Hilbert kernel embedded in L = 2W: h(m) = 2/(pi m) for odd m,
+  // h(L-m) = -h(m); H[k] = -2 i sum_{m odd < W} h(m) sin(2 pi k m / L)
+  const int L = 2 * W, nb = W + 1;
+  std::vector<float> himag(nb);
+  for (int k = 0; k < nb; k++) {
+    double acc = 0.0;
+    for (int m = 1; m < W; m += 2) acc += (2.0 / (M_PI * m)) * sin(2.0 * M_PI * (double)k * m / L);
+    himag[k] = (float)(-2.0 * acc);
+  }
+  auto* pl = new fcb_katsevich_plan();
+  pl->nviews = nviews; pl->H = H; pl->W = W; pl->K = K; pl->L = L; pl->nb = nb;
+  pl->dlam = (float)dlam; pl->pw = pw; pl->D = D; pl->su = (float)su;
+  const long long rows = (long long)nviews * K;
+  pl->batch = (int)std::min<long long>(rows, std::max<long long>(1, (256ll << 20) / (8ll * L)));
   const size_t nhw = (size_t)nviews * H * W, nkw = (size_t)nviews * K * W;
-  float *g2 = nullptr, *g3 = nullptr, *g4 = nullptr, *dfa = nullptr, *dba = nullptr;
-  int *dfj = nullptr, *dbk = nullptr;
-  float *hpad = nullptr, *dhim = nullptr;
-  cufftComplex* hspec = nullptr;
-  cufftHandle pf = 0, pi = 0;
   int rc = FCB_OK;
   do {
-    if (cudaMalloc(&g2, nhw * 4) || cudaMalloc(&g3, nkw * 4) || cudaMalloc(&g4, nkw * 4) ||
-        cudaMalloc(&dfa, fa.size() * 4) || cudaMalloc(&dba, ba.size() * 4) ||
-        cudaMalloc(&dfj, fj0.size() * 4) || cudaMalloc(&dbk, bk0.size() * 4)) {
+    if (cudaMalloc(&pl->g2, nhw * 4) || cudaMalloc(&pl->g3, nkw * 4) || cudaMalloc(&pl->g4, nkw * 4) ||
+        cudaMalloc(&pl->dfa, fa.size() * 4) || cudaMalloc(&pl->dba, ba.size() * 4) ||
+        cudaMalloc(&pl->dfj, fj0.size() * 4) || cudaMalloc(&pl->dbk, bk0.size() * 4) ||
+        cudaMalloc(&pl->hpad, (size_t)pl->batch * L * 4) ||
+        cudaMalloc(&pl->hspec, (size_t)pl->batch * nb * sizeof(cufftComplex)) || cudaMalloc(&pl->dhim, nb * 4)) {
       cudaGetLastError();
       rc = set_error(FCB_ERR_NOMEM, "Katsevich filter scratch");
       break;
     }
-    cudaMemcpyAsync(dfa, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(dba, ba.data(), ba.size() * 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(dfj, fj0.data(), fj0.size() * 4, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(dbk, bk0.data(), bk0.size() * 4, cudaMemcpyHostToDevice, st);
-    kats_deriv_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(in, g2, nviews, H, W, (float)dlam,
-                                                                     pw, D, (float)su);
-    kats_rebin_fwd_kernel<<<(unsigned)((nkw + 255) / 256), 256, 0, st>>>(g2, g3, dfj, dfa, nviews, H, W, K);
-    // the published Hilbert transform runs along increasing u; along w it changes sign when u = -w
-    const char* direct = getenv("FCB_KATS_DIRECT_HILBERT");
-    if (direct && direct[0] == '1') {
-      kats_hilbert_kernel<<<(unsigned)((size_t)nviews * K), 256, W * sizeof(float), st>>>(g3, g4, W,
-                                                                                          (float)su);
-    } else {
-      // spectrum of the kernel embedded in L = 2W: h(m) = 2/(pi m) for odd m, h(L-m) = -h(m);
-      // H[k] = sum_m h(m) e^{-2 pi i k m / L} = -2 i sum_{m odd < W} h(m) sin(2 pi k m / L)
-      const int L = 2 * W, nb = W + 1;
-      std::vector<float> himag(nb);
-      for (int k = 0; k < nb; k++) {
-        double acc = 0.0;
-        for (int m = 1; m < W; m += 2) acc += (2.0 / (M_PI * m)) * sin(2.0 * M_PI * (double)k * m / L);
-        himag[k] = (float)(-2.0 * acc);
-      }
-      const long long rows = (long long)nviews * K;
-      const int batch = (int)std::min<long long>(rows, std::max<long long>(1, (256ll << 20) / (8ll * L)));
-      if (cudaMalloc(&hpad, (size_t)batch * L * 4) || cudaMalloc(&hspec, (size_t)batch * nb * sizeof(cufftComplex)) ||
-          cudaMalloc(&dhim, nb * 4)) {
-        cudaGetLastError();
-        rc = set_error(FCB_ERR_NOMEM, "Katsevich filter scratch");
-        break;
-      }
-      cudaMemcpyAsync(dhim, himag.data(), nb * 4, cudaMemcpyHostToDevice, st);
-      int n1[1] = {L};
-      if (cufftPlanMany(&pf, 1, n1, nullptr, 1, L, nullptr, 1, nb, CUFFT_R2C, batch) != CUFFT_SUCCESS ||
-          cufftPlanMany(&pi, 1, n1, nullptr, 1, nb, nullptr, 1, L, CUFFT_C2R, batch) != CUFFT_SUCCESS ||
-          cufftSetStream(pf, st) != CUFFT_SUCCESS || cufftSetStream(pi, st) != CUFFT_SUCCESS) {
-        rc = set_error(FCB_ERR_CUDA, "cufftPlanMany failed");
-        break;
-      }
-      const float scale = (float)su / (float)L;
-      for (long long r0 = 0; r0 < rows && !rc; r0 += batch) {
-        const int nr = (int)std::min<long long>(batch, rows - r0);
-        kats_pad_kernel<<<(unsigned)(((long long)batch * L + 255) / 256), 256, 0, st>>>(g3, hpad, r0, nr, W, L);
-        if (nr < batch) cudaMemsetAsync(hpad + (size_t)nr * L, 0, (size_t)(batch - nr) * L * 4, st);
-        if (cufftExecR2C(pf, hpad, hspec) != CUFFT_SUCCESS) { rc = set_error(FCB_ERR_CUDA, "cufftExecR2C failed"); break; }
-        kats_spec_kernel<<<(unsigned)(((long long)nr * nb + 255) / 256), 256, 0, st>>>(hspec, dhim, nr, nb);
-        if (cufftExecC2R(pi, hspec, hpad) != CUFFT_SUCCESS) { rc = set_error(FCB_ERR_CUDA, "cufftExecC2R failed"); break; }
-        kats_crop_kernel<<<(unsigned)(((long long)nr * W + 255) / 256), 256, 0, st>>>(hpad, g4, r0, nr, W, L, scale);
-      }
-      if (rc) break;
+    if (cudaMemcpy(pl->dfa, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(pl->dba, ba.data(), ba.size() * 4, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(pl->dfj, fj0.data(), fj0.size() * 4, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(pl->dbk, bk0.data(), bk0.size() * 4, cudaMemcpyHostToDevice) ||
+        cudaMemcpy(pl->dhim, himag.data(), nb * 4, cudaMemcpyHostToDevice)) {
+      rc = set_error(FCB_ERR_CUDA, "Katsevich table upload failed");
+      break;
     }
-    kats_rebin_bwd_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(g4, out, dbk, dba, nviews, H, W, K);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) rc = set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
+    int n1[1] = {L};
+    if (cufftPlanMany(&pl->pf, 1, n1, nullptr, 1, L, nullptr, 1, nb, CUFFT_R2C, pl->batch) != CUFFT_SUCCESS ||
+        cufftPlanMany(&pl->pi, 1, n1, nullptr, 1, nb, nullptr, 1, L, CUFFT_C2R, pl->batch) != CUFFT_SUCCESS) {
+      rc = set_error(FCB_ERR_CUDA, "cufftPlanMany failed");
+      break;
+    }
   } while (0);
-  if (rc) cudaStreamSynchronize(st);  // nothing queued may still use the scratch freed below
-  if (pf) cufftDestroy(pf);
-  if (pi) cufftDestroy(pi);
-  cudaFree(g2); cudaFree(g3); cudaFree(g4); cudaFree(dfa); cudaFree(dba); cudaFree(dfj); cudaFree(dbk);
-  cudaFree(hpad); cudaFree(hspec); cudaFree(dhim);
-  return rc ? rc : ok();
+  if (rc) {
+    delete pl;
+    return rc;
+  }
+  *out = pl;
+  return ok();
+}
+
+extern "C" int fcb_katsevich_plan_execute(fcb_katsevich_plan* pl, const float* in, float* out,
+                                          void* stream)
+{
+  if (!pl || !in || !out) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  const int nviews = pl->nviews, H = pl->H, W = pl->W, K = pl->K, L = pl->L, nb = pl->nb;
+  const size_t nhw = (size_t)nviews * H * W, nkw = (size_t)nviews * K * W;
+  kats_deriv_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(in, pl->g2, nviews, H, W, pl->dlam,
+                                                                   pl->pw, pl->D, pl->su);
+  kats_rebin_fwd_kernel<<<(unsigned)((nkw + 255) / 256), 256, 0, st>>>(pl->g2, pl->g3, pl->dfj, pl->dfa,
+                                                                       nviews, H, W, K);
+  // the published Hilbert transform runs along increasing u; along w it changes sign when u = -w
+  const char* direct = getenv("FCB_KATS_DIRECT_HILBERT");
+  if (direct && direct[0] == '1') {
+    kats_hilbert_kernel<<<(unsigned)((size_t)nviews * K), 256, W * sizeof(float), st>>>(pl->g3, pl->g4, W,
+                                                                                        pl->su);
+  } else {
+    if (cufftSetStream(pl->pf, st) != CUFFT_SUCCESS || cufftSetStream(pl->pi, st) != CUFFT_SUCCESS)
+      return set_error(FCB_ERR_CUDA, "cufftSetStream failed");
+    const float scale = pl->su / (float)L;
+    const long long rows = (long long)nviews * K;
+    const int batch = pl->batch;
+    for (long long r0 = 0; r0 < rows; r0 += batch) {
+      const int nr = (int)std::min<long long>(batch, rows - r0);
+      kats_pad_kernel<<<(unsigned)(((long long)batch * L + 255) / 256), 256, 0, st>>>(pl->g3, pl->hpad, r0, nr, W, L);
+      if (nr < batch)
+        FCB_CUDA_TRY(cudaMemsetAsync(pl->hpad + (size_t)nr * L, 0, (size_t)(batch - nr) * L * 4, st));
+      if (cufftExecR2C(pl->pf, pl->hpad, pl->hspec) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecR2C failed");
+      kats_spec_kernel<<<(unsigned)(((long long)nr * nb + 255) / 256), 256, 0, st>>>(pl->hspec, pl->dhim, nr, nb);
+      if (cufftExecC2R(pl->pi, pl->hspec, pl->hpad) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecC2R failed");
+      kats_crop_kernel<<<(unsigned)(((long long)nr * W + 255) / 256), 256, 0, st>>>(pl->hpad, pl->g4, r0, nr, W, L, scale);
+    }
+  }
+  kats_rebin_bwd_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(pl->g4, out, pl->dbk, pl->dba, nviews, H,
+                                                                      W, K);
+  FCB_CUDA_TRY(cudaGetLastError());
+  return ok();
+}
+
+extern "C" int fcb_katsevich_plan_destroy(fcb_katsevich_plan* pl)
+{
+  delete pl;
+  return ok();
+}
+
+extern "C" int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, int W,
+                                           const float* angles, float D, float pw, float pitch,
+                                           int nkappa, void* stream)
+{
+  if (!in || !out) return set_error(FCB_ERR_INVALID, "bad Katsevich filter arguments");
+  fcb_katsevich_plan* pl = nullptr;
+  FCB_TRY(fcb_katsevich_plan_create(nviews, H, W, angles, D, pw, pitch, nkappa, &pl));
+  const int rc = fcb_katsevich_plan_execute(pl, in, out, stream);
+  // the plan's buffers are freed below; wait for the queued work that uses them
+  const cudaError_t e = cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(stream));
+  fcb_katsevich_plan_destroy(pl);
+  if (rc) return rc;
+  if (e != cudaSuccess) return set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
+  return ok();
 }

@@ -225,6 +225,38 @@ def katsevich_filter(proj: torch.Tensor, geom: ConeGeometry, n_kappa: int = 0,
     return out
 
 
+class KatsevichPlan:
+    """Reusable Katsevich filter for geom's helix and detector (tables, cuFFT plans and
+    intermediate buffers made once); calls are stream-ordered and allocate nothing."""
+
+    def __init__(self, geom: ConeGeometry, n_kappa: int = 0):
+        if geom.helical_pitch == 0.0:
+            raise ValueError("Katsevich filtering needs a helical geometry (helical_pitch != 0)")
+        self.shape = geom.proj_shape
+        self._h = ctypes.c_void_p()
+        n, H, W = self.shape
+        check(lib().fcb_katsevich_plan_create(n, H, W, geom.angles.ctypes.data_as(_lib.c_float_p), float(geom.D),
+                                              float(geom.pw), float(geom.helical_pitch), int(n_kappa),
+                                              ctypes.byref(self._h)))
+
+    def __call__(self, proj: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        if tuple(proj.shape) != self.shape:
+            raise ValueError("projection shape does not match the plan")
+        if out is None:
+            out = torch.empty_like(proj)
+        check(lib().fcb_katsevich_plan_execute(self._h, _dev(proj, "proj", torch.float32),
+                                               _dev(out, "out", torch.float32), _stream()))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            try:
+                lib().fcb_katsevich_plan_destroy(self._h)
+            except Exception:
+                pass
+            self._h = ctypes.c_void_p()
+
+
 def katsevich_reconstruct(proj: torch.Tensor, geom: ConeGeometry, n_kappa: int = 0,
                           dtype=torch.float32) -> torch.Tensor:
     """Exact helical reconstruction: Katsevich filtering, then backprojection with weight U

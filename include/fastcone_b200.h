@@ -225,6 +225,16 @@ int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, 
                                 const float* angles, float D, float pw, float pitch, int nkappa,
                                 void* stream);
 
+/* The same filter as a reusable plan for one helix and detector: kappa-line tables, the
+ * Hilbert kernel's spectrum, cuFFT plans and intermediate buffers made once (about
+ * 4 x nviews x 2H x W floats of device memory); execute is stream-ordered, allocates nothing
+ * and does not synchronise.  One execute at a time per plan. */
+typedef struct fcb_katsevich_plan fcb_katsevich_plan;
+int fcb_katsevich_plan_create(int nviews, int H, int W, const float* angles, float D, float pw,
+                              float pitch, int nkappa, fcb_katsevich_plan** plan);
+int fcb_katsevich_plan_execute(fcb_katsevich_plan* plan, const float* in, float* out, void* stream);
+int fcb_katsevich_plan_destroy(fcb_katsevich_plan* plan);
+
 /* 3x3x3 convolution, 16 -> 16 channels, stride 1, zero padding 1, on the tcgen05 tensor
  * cores (BF16 inputs, FP32 accumulation).  Activations in the channel-half-major layout
  * [nz][ny][2][nx][8] (channel c of voxel (x,y,z) at ((z*ny + y)*2 + c/8)*nx*8 + x*8 + c%8).

@@ -76,3 +76,21 @@ def test_fft_hilbert_matches_direct_sum(monkeypatch):
     torch.cuda.synchronize()
     rel = float((a - b).norm() / a.norm())
     assert rel < 2e-5, rel
+
+
+def test_katsevich_plan_equals_one_shot():
+    """The reusable Katsevich filter plan gives the one-shot filter's result, call after call."""
+    import numpy as np
+    import torch
+
+    from fastcone_b200 import ops
+    from fastcone_b200.geometry import ConeGeometry
+
+    g = ConeGeometry.helical((48, 48, 40), 1.0, (96, 24), 1.0, 150.0, 300.0, 3, 80, 24.0, pi_window=True)
+    p = torch.from_numpy(np.random.default_rng(8).random(g.proj_shape, dtype=np.float32)).cuda()
+    ref = ops.katsevich_filter(p, g)
+    plan = ops.KatsevichPlan(g)
+    for _ in range(2):
+        got = plan(p)
+        torch.cuda.synchronize()
+        assert torch.equal(got, ref)
