@@ -29,7 +29,7 @@ FCB_ERR_RANGE = 6
 FCB_F32, FCB_F16, FCB_BF16 = 0, 1, 2
 MODE_UNWEIGHTED, MODE_KATSEVICH, MODE_FDK = 0, 1, 2
 PROJ_TEXTURE, PROJ_EXPLICIT, PROJ_EXPLICIT_GLOBAL = 0, 1, 2
-FILTER_RAMLAK, FILTER_SHEPPLOGAN = 0, 1
+FILTER_RAMLAK, FILTER_SHEPPLOGAN, FILTER_COSRAMP, FILTER_GAUSSRAMP = 0, 1, 2, 3
 
 # Every symbol include/fastcone_b200.h declares (checked by the CPU test suite).
 EXPORTED_SYMBOLS = [
@@ -45,7 +45,8 @@ EXPORTED_SYMBOLS = [
     "fcb_conv3d16_device", "fcb_conv3d16_wgrad_device",
     "fcb_proj_plan_create", "fcb_proj_plan_execute", "fcb_proj_plan_destroy",
     "fcb_reference_windows", "fcb_proj_plan_info",
-    "fcb_filter_plan_create", "fcb_filter_plan_execute", "fcb_filter_plan_destroy",
+    "fcb_filter_plan_create", "fcb_filter_plan_create_ex", "fcb_filter_plan_execute",
+    "fcb_filter_plan_destroy",
     "fcb_katsevich_plan_create", "fcb_katsevich_plan_execute", "fcb_katsevich_plan_destroy",
 ]
 
@@ -126,6 +127,7 @@ def lib():
             L.fcb_reference_windows.argtypes = [gp] + [c_int_p] * 8
             L.fcb_proj_plan_info.argtypes = [vp] + [c_int_p] * 4
             L.fcb_filter_plan_create.argtypes = [ctypes.c_int] * 5 + [ctypes.POINTER(vp)]
+            L.fcb_filter_plan_create_ex.argtypes = [ctypes.c_int] * 5 + [ctypes.c_double, ctypes.POINTER(vp)]
             L.fcb_filter_plan_execute.argtypes = [vp, vp, vp, ctypes.c_float, c_float_p, ctypes.c_int, vp]
             L.fcb_filter_plan_destroy.argtypes = [vp]
             L.fcb_katsevich_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_float_p,

@@ -3,9 +3,10 @@
 // fcb_fdk_filter_device replaces the host-side numpy loops of fastcone.fbp / rampfilter
 // (fastcone.py:260-292): cosine weight, zero-padding to 2W with the data at [0, W), real
 // FFT, multiplication by pi*|fftfreq(2W)| (DC bin = 1/8 of the first bin), inverse FFT,
-// crop to [0, W).  The FFTs are cuFFT batched R2C/C2R transforms over row batches; the
-// weighting, padding, filter multiply, crop, 1/(2W) scaling and the cast to the storage
-// type are this file's kernels.
+// crop to [0, W).  The apodised variants cosrampfilter / gaussrampfilter (fastcone.py:
+// 294-319) transform rows of length W unpadded.  The FFTs are cuFFT batched R2C/C2R
+// transforms over row batches; the weighting, padding, filter multiply, crop, 1/L scaling
+// and the cast to the storage type are this file's kernels.
 #include <cufft.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -19,14 +20,14 @@
 namespace fcb {
 
 __global__ void pad_weight_kernel(const float* __restrict__ in, float* __restrict__ pad,
-                                  long long row0, int nrows, int H, int W, float D,
+                                  long long row0, int nrows, int H, int W, int L, float D,
                                   const float* __restrict__ zorig, int cosw)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long total = (long long)nrows * 2 * W;
+  const long long total = (long long)nrows * L;
   if (i >= total) return;
-  const int c = (int)(i % (2 * W));
-  const long long r = i / (2 * W);
+  const int c = (int)(i % L);
+  const long long r = i / L;
   float v = 0.0f;
   if (c < W) {
     const long long gr = row0 + r;
@@ -64,13 +65,13 @@ __device__ __forceinline__ __nv_bfloat16 to_store<__nv_bfloat16>(float v) { retu
 
 template <typename T>
 __global__ void crop_store_kernel(const float* __restrict__ pad, T* __restrict__ out, long long row0,
-                                  int nrows, int W, float scale)
+                                  int nrows, int W, int L, float scale)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= (long long)nrows * W) return;
   const int c = (int)(i % W);
   const long long r = i / W;
-  out[(row0 + r) * W + c] = to_store<T>(pad[r * 2 * W + c] * scale);
+  out[(row0 + r) * W + c] = to_store<T>(pad[r * L + c] * scale);
 }
 
 // ------------------------------------------------------------------- phantom
@@ -130,31 +131,68 @@ struct fcb_filter_plan {
   }
 };
 
-extern "C" int fcb_filter_plan_create(int nviews, int H, int W, int outType, int window,
-                                      fcb_filter_plan** out)
+// Filter response on the plan's nb = L/2 + 1 frequency bins, in double like numpy.
+//  RAMLAK / SHEPPLOGAN (fastcone.rampfilter, fastcone.py:272-292): L = 2W, pi * |fftfreq(2W)|
+//    with the DC bin 1/8 of the first, times sinc for Shepp-Logan.
+//  COSRAMP (fastcone.cosrampfilter, fastcone.py:294-304): L = W, a_k = |fftfreq(W)[k]| = k/W,
+//    times cos(0.5 * a_k * pi / W) exactly as written there.
+//  GAUSSRAMP (fastcone.gaussrampfilter, fastcone.py:306-319): L = W, a_k times a Gaussian of
+//    standard deviation gaussScale * W centred at (W - 1) / 2 and shifted by -W/2 samples
+//    (zero beyond the last sample), i.e. exp(-((k + 1/2) / sigma)^2 / 2) for k + W/2 <= W - 1.
+static int filter_response(int W, int window, double gaussScale, int* L, std::vector<float>& filt)
+{
+  if (window == FCB_FILTER_RAMLAK || window == FCB_FILTER_SHEPPLOGAN) {
+    *L = 2 * W;
+  } else if (window == FCB_FILTER_COSRAMP || window == FCB_FILTER_GAUSSRAMP) {
+    *L = W;
+    if (window == FCB_FILTER_GAUSSRAMP && !(gaussScale > 0.0))
+      return set_error(FCB_ERR_INVALID, "Gaussian window needs gaussScale > 0");
+  } else {
+    return set_error(FCB_ERR_INVALID, "unknown filter window");
+  }
+  const int nb = *L / 2 + 1;
+  filt.assign(nb, 0.0f);
+  for (int k = 0; k < nb; k++) {
+    double f;
+    if (*L == 2 * W) {
+      f = (double)k / (double)*L;
+      if (k == 0) f = 0.125 * (1.0 / (double)*L);
+      if (window == FCB_FILTER_SHEPPLOGAN && k > 0) {
+        const double x = M_PI * (double)k / (double)*L;
+        f *= sin(x) / x;
+      }
+      f *= M_PI;
+    } else {
+      const double a = (double)k / (double)W;
+      if (window == FCB_FILTER_COSRAMP) {
+        f = a * cos(0.5 * a * M_PI / (double)W);
+      } else {
+        const double src = (double)k + 0.5 * (double)W;  // sample the shifted window reads
+        const double sig = gaussScale * (double)W;
+        const double d = ((double)k + 0.5) / sig;
+        f = src <= (double)(W - 1) ? a * exp(-0.5 * d * d) : 0.0;
+      }
+    }
+    filt[k] = (float)f;
+  }
+  return FCB_OK;
+}
+
+extern "C" int fcb_filter_plan_create_ex(int nviews, int H, int W, int outType, int window,
+                                         double gaussScale, fcb_filter_plan** out)
 {
   if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
   *out = nullptr;
   if (nviews <= 0 || H <= 0 || W <= 0) return set_error(FCB_ERR_INVALID, "bad filter sizes");
   if (outType != FCB_F32 && outType != FCB_F16 && outType != FCB_BF16)
     return set_error(FCB_ERR_INVALID, "unknown output type");
-  if (window != FCB_FILTER_RAMLAK && window != FCB_FILTER_SHEPPLOGAN)
-    return set_error(FCB_ERR_INVALID, "unknown filter window");
+  std::vector<float> filt;
+  int L = 0;
+  FCB_TRY(filter_response(W, window, gaussScale, &L, filt));
   auto* pl = new fcb_filter_plan();
   pl->nviews = nviews; pl->H = H; pl->W = W; pl->outType = outType; pl->window = window;
-  pl->n2 = 2 * W;
-  pl->nb = W + 1;
-  // filter response, computed in double like numpy: |fftfreq(2W)|, DC = f1/8, * pi
-  std::vector<float> filt(pl->nb);
-  for (int k = 0; k < pl->nb; k++) {
-    double f = (double)k / (double)pl->n2;
-    if (k == 0) f = 0.125 * (1.0 / (double)pl->n2);
-    if (window == FCB_FILTER_SHEPPLOGAN && k > 0) {
-      const double x = M_PI * (double)k / (double)pl->n2;
-      f *= sin(x) / x;
-    }
-    filt[k] = (float)(M_PI * f);
-  }
+  pl->n2 = L;
+  pl->nb = L / 2 + 1;
   const long long rows = (long long)nviews * H;
   pl->batch = (int)std::min<long long>(rows, std::max<long long>(1, (256ll << 20) / (8ll * pl->n2)));
   int rc = FCB_OK;
@@ -186,6 +224,12 @@ extern "C" int fcb_filter_plan_create(int nviews, int H, int W, int outType, int
   return ok();
 }
 
+extern "C" int fcb_filter_plan_create(int nviews, int H, int W, int outType, int window,
+                                      fcb_filter_plan** out)
+{
+  return fcb_filter_plan_create_ex(nviews, H, W, outType, window, 0.125, out);
+}
+
 // out = filter(in) as outType; zOrigin (host, nviews floats) is read before the call returns.
 extern "C" int fcb_filter_plan_execute(fcb_filter_plan* pl, const float* in, void* out, float D,
                                        const float* zOrigin, int cosineWeight, void* stream)
@@ -204,7 +248,7 @@ extern "C" int fcb_filter_plan_execute(fcb_filter_plan* pl, const float* in, voi
   for (long long r0 = 0; r0 < rows; r0 += batch) {
     const int nr = (int)std::min<long long>(batch, rows - r0);
     long long tot = (long long)nr * n2;
-    pad_weight_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, pl->pad, r0, nr, H, W, D, pl->dz,
+    pad_weight_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, pl->pad, r0, nr, H, W, n2, D, pl->dz,
                                                                    cosineWeight);
     // cuFFT plans are for `batch` rows; the tail batch is zero-padded in `pad`
     if (nr < batch)
@@ -215,9 +259,9 @@ extern "C" int fcb_filter_plan_execute(fcb_filter_plan* pl, const float* in, voi
     if (cufftExecC2R(pl->pi, pl->spec, pl->pad) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecC2R failed");
     tot = (long long)nr * W;
     const unsigned g = (unsigned)((tot + 255) / 256);
-    if (pl->outType == FCB_F32) crop_store_kernel<float><<<g, 256, 0, st>>>(pl->pad, (float*)out, r0, nr, W, scale);
-    else if (pl->outType == FCB_F16) crop_store_kernel<__half><<<g, 256, 0, st>>>(pl->pad, (__half*)out, r0, nr, W, scale);
-    else crop_store_kernel<__nv_bfloat16><<<g, 256, 0, st>>>(pl->pad, (__nv_bfloat16*)out, r0, nr, W, scale);
+    if (pl->outType == FCB_F32) crop_store_kernel<float><<<g, 256, 0, st>>>(pl->pad, (float*)out, r0, nr, W, n2, scale);
+    else if (pl->outType == FCB_F16) crop_store_kernel<__half><<<g, 256, 0, st>>>(pl->pad, (__half*)out, r0, nr, W, n2, scale);
+    else crop_store_kernel<__nv_bfloat16><<<g, 256, 0, st>>>(pl->pad, (__nv_bfloat16*)out, r0, nr, W, n2, scale);
   }
   FCB_CUDA_TRY(cudaGetLastError());
   return ok();

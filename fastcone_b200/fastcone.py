@@ -158,23 +158,49 @@ def rampfilter(proj, window="ramlak", GPUID=0):
     _filter_inplace(proj, 0.0, None, cosine=False, window=window, GPUID=GPUID)
 
 
-def _filter_inplace(proj, D, zOrigin, cosine, window, GPUID):
+def cosrampfilter(proj, GPUID=0):
+    """Cosine-apodised ramp filter of fastcone.py:294-304 (rows of length W, unpadded,
+    response |f| * cos(0.5 |f| pi / W)), in place, on the GPU.  Every view is filtered (the
+    reference's loop stores only the last view, and its inverse FFT has length W - 1 for an
+    odd W; here the inverse has length W)."""
+    _filter_inplace(proj, 0.0, None, cosine=False, window="cosramp", GPUID=GPUID)
+
+
+def gaussrampfilter(proj, scale=0.125, GPUID=0):
+    """Gaussian-apodised ramp filter of fastcone.py:306-319 (rows of length W, unpadded;
+    |f| times the Gaussian of sigma = scale * W shifted by -W/2 samples), in place, on the
+    GPU, every view filtered."""
+    _filter_inplace(proj, 0.0, None, cosine=False, window="gaussramp", GPUID=GPUID, gauss_scale=scale)
+
+
+_WINDOWS = {"ramlak": _lib.FILTER_RAMLAK, "shepplogan": _lib.FILTER_SHEPPLOGAN,
+            "cosramp": _lib.FILTER_COSRAMP, "gaussramp": _lib.FILTER_GAUSSRAMP}
+
+
+def _filter_inplace(proj, D, zOrigin, cosine, window, GPUID, gauss_scale=0.125):
     import torch  # plumbing for device memory and the stream
 
     if proj.dtype != FLOAT_TYPE or not proj.flags.c_contiguous:
         raise FastconeArgumentError("Projection array must be C-contiguous np.float32")
-    win = {"ramlak": _lib.FILTER_RAMLAK, "shepplogan": _lib.FILTER_SHEPPLOGAN}[window]
+    win = _WINDOWS[window]
+    n, H, W = proj.shape
     dev = torch.device("cuda", GPUID)
     with torch.cuda.device(dev):
         t = torch.from_numpy(proj).to(dev)
-        z = np.ascontiguousarray(zOrigin if zOrigin is not None else np.zeros(proj.shape[0]), dtype=FLOAT_TYPE)
+        z = np.ascontiguousarray(zOrigin if zOrigin is not None else np.zeros(n), dtype=FLOAT_TYPE)
         st = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
-        _lib.check(lib().fcb_fdk_filter_device(ctypes.c_void_p(t.data_ptr()), ctypes.c_void_p(t.data_ptr()),
-                                               _lib.FCB_F32, proj.shape[0], proj.shape[1], proj.shape[2],
-                                               float(D), z.ctypes.data_as(c_float_p), 1 if cosine else 0,
-                                               win, st))
-        proj[...] = t.cpu().numpy()
+        plan = ctypes.c_void_p()
+        _lib.check(lib().fcb_filter_plan_create_ex(n, H, W, _lib.FCB_F32, win, float(gauss_scale),
+                                                   ctypes.byref(plan)))
+        try:
+            _lib.check(lib().fcb_filter_plan_execute(plan, ctypes.c_void_p(t.data_ptr()),
+                                                     ctypes.c_void_p(t.data_ptr()), float(D),
+                                                     z.ctypes.data_as(c_float_p), 1 if cosine else 0, st))
+            proj[...] = t.cpu().numpy()
+        finally:
+            torch.cuda.current_stream().synchronize()
+            lib().fcb_filter_plan_destroy(plan)
 
 
-__all__ = ["project", "backproject", "fbp", "rampfilter", "FastconeArgumentError", "FastconeError",
+__all__ = ["project", "backproject", "fbp", "rampfilter", "cosrampfilter", "gaussrampfilter", "FastconeArgumentError", "FastconeError",
            "FLOAT_TYPE", "INT_TYPE"]

@@ -179,16 +179,19 @@ def fdk_filter(proj: torch.Tensor, geom: ConeGeometry | None = None, out_dtype=t
 
 
 class FilterPlan:
-    """Reusable FDK filter (cosine weight + ramp / Shepp-Logan) for projections of shape
+    """Reusable FDK filter (cosine weight + ramp / Shepp-Logan, or the unpadded cosine /
+    Gaussian apodised ramps with ``window=FILTER_COSRAMP / FILTER_GAUSSRAMP``) for projections of shape
     (nviews, H, W): cuFFT plans and scratch made once; calls are stream-ordered, allocate
     nothing and do not synchronise."""
 
-    def __init__(self, shape, out_dtype=torch.float32, window: int = _lib.FILTER_RAMLAK):
+    def __init__(self, shape, out_dtype=torch.float32, window: int = _lib.FILTER_RAMLAK,
+                 gauss_scale: float = 0.125):
         self.shape = tuple(int(v) for v in shape)
         self.out_dtype = out_dtype
         self._h = ctypes.c_void_p()
         n, H, W = self.shape
-        check(lib().fcb_filter_plan_create(n, H, W, _DTYPES[out_dtype], int(window), ctypes.byref(self._h)))
+        check(lib().fcb_filter_plan_create_ex(n, H, W, _DTYPES[out_dtype], int(window), float(gauss_scale),
+                                              ctypes.byref(self._h)))
 
     def __call__(self, proj: torch.Tensor, zorigin=None, D: float | None = None, cosine_weight: bool = True,
                  out: torch.Tensor | None = None) -> torch.Tensor:

@@ -53,9 +53,14 @@ extern "C" {
 #define FCB_PROJ_EXPLICIT_GLOBAL 2 /* the same samples and arithmetic (bit-identical results), every
                                       tap read from global memory: the unstaged comparison */
 
-/* ramp-filter windows for fcb_fdk_filter_device */
-#define FCB_FILTER_RAMLAK 0
-#define FCB_FILTER_SHEPPLOGAN 1
+/* ramp-filter windows for fcb_fdk_filter_device / fcb_filter_plan_create */
+#define FCB_FILTER_RAMLAK 0      /* fastcone.rampfilter, fastcone.py:272-292 */
+#define FCB_FILTER_SHEPPLOGAN 1  /* the same with the sinc (Shepp-Logan) apodisation */
+#define FCB_FILTER_COSRAMP 2     /* fastcone.cosrampfilter, fastcone.py:294-304: rows of length W
+                                    unpadded, |f| * cos(0.5 |f| pi / W), applied to every view */
+#define FCB_FILTER_GAUSSRAMP 3   /* fastcone.gaussrampfilter, fastcone.py:306-319: rows of length W
+                                    unpadded, |f| times the half-Gaussian of sigma = scale * W
+                                    (scale 1/8 unless fcb_filter_plan_create_ex sets it) */
 
 int fcb_version(void);
 int fcb_last_status(void);
@@ -196,7 +201,8 @@ int fcb_sync_status(void* stream);
 /* FDK pre-processing on the GPU (fastcone.py:260-292): optional cosine weight
  * D / sqrt(D^2 + (h - zOrigin[t])^2 + (w - W/2)^2) in detector pixels, then the ramp
  * filter of fastcone.rampfilter (zero-pad rows to 2W, pi*|f| with DC = 1/8 of the first
- * bin; FCB_FILTER_SHEPPLOGAN multiplies by sinc(f)), output stored as outType.
+ * bin; FCB_FILTER_SHEPPLOGAN multiplies by sinc(f); FCB_FILTER_COSRAMP / GAUSSRAMP are the
+ * unpadded apodised variants of fastcone.py:294-319), output stored as outType.
  * in: float [nviews][H][W] device; out: [nviews][H][W] of outType (may alias in when
  * outType == FCB_F32). */
 int fcb_fdk_filter_device(const float* in, void* out, int outType, int nviews, int H, int W,
@@ -209,6 +215,10 @@ int fcb_fdk_filter_device(const float* in, void* out, int outType, int nviews, i
 typedef struct fcb_filter_plan fcb_filter_plan;
 int fcb_filter_plan_create(int nviews, int H, int W, int outType, int window,
                            fcb_filter_plan** plan);
+/* As fcb_filter_plan_create; gaussScale is the Gaussian's sigma as a fraction of W for
+ * FCB_FILTER_GAUSSRAMP (gaussrampfilter's `scale`, fastcone.py:306) and ignored otherwise. */
+int fcb_filter_plan_create_ex(int nviews, int H, int W, int outType, int window,
+                              double gaussScale, fcb_filter_plan** plan);
 int fcb_filter_plan_execute(fcb_filter_plan* plan, const float* in, void* out, float D,
                             const float* zOrigin, int cosineWeight, void* stream);
 int fcb_filter_plan_destroy(fcb_filter_plan* plan);

@@ -385,6 +385,37 @@ def ramp_filter_response(w, window="ramlak"):
     return f[: w + 1]
 
 
+def apodised_ramp_response(w, window="cosramp", scale=0.125):
+    """Response of fastcone.cosrampfilter / gaussrampfilter (fastcone.py:294-319) on the
+    w//2 + 1 bins of an unpadded length-w rfft: a_k = |fftfreq(w)[k]| = k/w, times
+    cos(0.5 a_k pi / w) (cosine, as written there), or times the Gaussian window of
+    sigma = scale*w centred at (w-1)/2 and shifted by -w/2 samples with zeros beyond the
+    last sample (scipy.ndimage.shift of scipy.signal gaussian; for an even w the shift is a
+    whole number of samples and this is that window exactly; for an odd w the reference
+    raises before filtering, and the Gaussian is sampled at the shifted position)."""
+    k = np.arange(w // 2 + 1, dtype=np.float64)
+    a = k / w
+    if window == "cosramp":
+        return a * np.cos(0.5 * a * np.pi / w)
+    if window == "gaussramp":
+        g = np.exp(-0.5 * ((k + 0.5) / (scale * w)) ** 2)
+        return a * np.where(k + 0.5 * w <= w - 1, g, 0.0)
+    raise ValueError(window)
+
+
+def apodised_rampfilter(proj, window="cosramp", scale=0.125):
+    """fastcone.cosrampfilter / gaussrampfilter (fastcone.py:294-319) applied to every view
+    (the reference's store sits after its loop, so it writes only the last view) with an
+    inverse transform of length w (numpy's default length, 2*(w//2), is w - 1 for odd w)."""
+    proj = np.asarray(proj)
+    n, h, w = proj.shape
+    filt = apodised_ramp_response(w, window, scale)
+    out = np.empty_like(proj)
+    for t in range(n):
+        out[t] = np.fft.irfft(np.fft.rfft(proj[t], axis=1) * filt, n=w, axis=1)
+    return out
+
+
 def fbp_cosine_weight(proj, D, zOrigin):
     """Cosine pre-weight of fastcone.fbp (fastcone.py:261-267): D / sqrt(D^2 + h^2 + w^2)
     with h measured from zOrigin[t] and w from W/2, both in detector pixels."""

@@ -1,5 +1,5 @@
-"""GPU FDK pre-processing (cosine weight + ramp / Shepp-Logan filter) and phantom
-voxelisation vs the CPU restatements."""
+"""GPU FDK pre-processing (cosine weight + ramp / Shepp-Logan filter, the unpadded cosine /
+Gaussian apodised ramps) and phantom voxelisation vs the CPU restatements."""
 import numpy as np
 import pytest
 
@@ -34,6 +34,37 @@ def test_rampfilter_api_inplace():
     proj = np.random.default_rng(1).random((4, 12, 20), dtype=np.float32)
     want = O.rampfilter(proj.astype(np.float64))
     fc.rampfilter(proj)
+    assert O.rel_l2(proj, want) < 1e-5
+
+
+@pytest.mark.parametrize("window,scale", [("cosramp", 0.125), ("gaussramp", 0.125), ("gaussramp", 0.3),
+                                          ("gaussramp", 0.05)])
+@pytest.mark.parametrize("shape", [(5, 16, 24), (3, 7, 33), (2, 64, 192), (2, 3, 736)])
+def test_apodised_filter_vs_oracle(window, scale, shape):
+    import torch
+
+    from fastcone_b200 import _lib, ops
+
+    rng = np.random.default_rng(4)
+    proj = rng.standard_normal(shape).astype(np.float32)
+    want = O.apodised_rampfilter(proj.astype(np.float64), window, scale)
+    win = _lib.FILTER_COSRAMP if window == "cosramp" else _lib.FILTER_GAUSSRAMP
+    for dt, tol in ((torch.float32, 1e-5), (torch.bfloat16, 5e-3)):
+        plan = ops.FilterPlan(shape, out_dtype=dt, window=win, gauss_scale=scale)
+        got = plan(torch.from_numpy(proj).cuda(), cosine_weight=False).float().cpu().numpy()
+        assert O.rel_l2(got, want) < tol, (dt, O.rel_l2(got, want))
+
+
+@pytest.mark.parametrize("fn,window,kw", [("cosrampfilter", "cosramp", {}),
+                                          ("gaussrampfilter", "gaussramp", {}),
+                                          ("gaussrampfilter", "gaussramp", {"scale": 0.2})])
+def test_apodised_api_inplace(fn, window, kw):
+    """fastcone.cosrampfilter / gaussrampfilter filter every view in place."""
+    from fastcone_b200 import fastcone as fc
+
+    proj = np.random.default_rng(6).random((4, 12, 20), dtype=np.float32)
+    want = O.apodised_rampfilter(proj.astype(np.float64), window, kw.get("scale", 0.125))
+    getattr(fc, fn)(proj, **kw)
     assert O.rel_l2(proj, want) < 1e-5
 
 

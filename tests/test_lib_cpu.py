@@ -48,6 +48,12 @@ def test_invalid_arguments_return_status():
     assert L.fcb_bp_plan_create(ctypes.byref(bad), 2, 0, ctypes.byref(plan)) == _lib.FCB_ERR_INVALID
     assert L.fcb_bp_plan_create(ctypes.byref(s), 2, 7, ctypes.byref(plan)) == _lib.FCB_ERR_INVALID
     assert L.fcb_fdk_filter_device(None, None, 0, 1, 1, 1, 1.0, None, 0, 0, None) == _lib.FCB_ERR_INVALID
+    # filter windows are checked before any device work
+    assert L.fcb_filter_plan_create(2, 3, 8, 0, 9, ctypes.byref(plan)) == _lib.FCB_ERR_INVALID
+    assert b"window" in L.fcb_last_error()
+    assert L.fcb_filter_plan_create_ex(2, 3, 8, 0, _lib.FILTER_GAUSSRAMP, 0.0,
+                                       ctypes.byref(plan)) == _lib.FCB_ERR_INVALID
+    assert b"gaussScale" in L.fcb_last_error()
 
 
 def test_reference_entry_point_bad_device_sets_status():

@@ -127,6 +127,33 @@ def test_rampfilter_restatement_matches_reference_golden(name):
     assert O.rel_l2(got, d["output"]) < 1e-6
 
 
+@pytest.mark.parametrize("name,window,scale", [("cosramp_a", "cosramp", 0.125),
+                                                ("gaussramp_a", "gaussramp", 0.125),
+                                                ("gaussramp_b", "gaussramp", 0.3)])
+def test_apodised_ramp_restatement_matches_reference_golden(name, window, scale):
+    """cosrampfilter / gaussrampfilter (fastcone.py:294-319), run view by view by the
+    reference itself (tests/golden/make_golden.py), against the oracle's restatement."""
+    path = os.path.join(GOLDEN, name + ".npz")
+    if not os.path.exists(path):
+        pytest.skip("golden vectors not generated")
+    d = np.load(path)
+    got = O.apodised_rampfilter(d["input"].astype(np.float64), window, scale)
+    assert O.rel_l2(got, d["output"]) < 1e-6
+
+
+@pytest.mark.parametrize("w", [24, 38, 736, 1536])
+@pytest.mark.parametrize("scale", [0.05, 0.125, 0.3])
+def test_gauss_window_is_the_shifted_scipy_window_for_even_rows(w, scale):
+    """For an even row length the reference's window, scipy.ndimage.shift of a Gaussian by
+    -w/2 samples (fastcone.py:310-311), is the closed form the oracle and the library use."""
+    import scipy.ndimage
+    import scipy.signal
+
+    g = scipy.ndimage.shift(scipy.signal.windows.gaussian(w, scale * w), -0.5 * w)
+    want = np.abs(np.fft.fftfreq(w))[: w // 2 + 1] * g[: w // 2 + 1]
+    assert np.allclose(O.apodised_ramp_response(w, "gaussramp", scale), want, rtol=0, atol=1e-15)
+
+
 def test_fbp_weight_restatement_matches_reference_golden():
     path = os.path.join(GOLDEN, "fbp_weight.npz")
     if not os.path.exists(path):
