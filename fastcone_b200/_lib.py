@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = [
     "fcb_filter_plan_create", "fcb_filter_plan_create_ex", "fcb_filter_plan_execute",
     "fcb_filter_plan_destroy",
     "fcb_katsevich_plan_create", "fcb_katsevich_plan_execute", "fcb_katsevich_plan_destroy",
+    "fcb_detector_rows",
 ]
 
 
@@ -135,6 +136,7 @@ def lib():
                                                     ctypes.c_int, ctypes.POINTER(vp)]
             L.fcb_katsevich_plan_execute.argtypes = [vp, vp, vp, vp]
             L.fcb_katsevich_plan_destroy.argtypes = [vp]
+            L.fcb_detector_rows.argtypes = [gp, ctypes.c_int, c_int_p, c_int_p]
             _lib = L
     return _lib
 

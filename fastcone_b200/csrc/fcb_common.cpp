@@ -3,6 +3,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
+#include <cmath>
 #include <mutex>
 
 #include "fcb_internal.h"
@@ -264,3 +266,52 @@ int encode_tmap_3d(CUtensorMap* map, CUtensorMapDataType dtype, void* base, uint
 
 extern "C" int fcb_last_status(void) { return fcb::t_status; }
 extern "C" const char* fcb_last_error(void) { return fcb::t_msg.c_str(); }
+
+// --------------------------------------------------------------- slab footprints
+// Detector rows a sub-volume reaches in each view, for splitting one volume into z-slabs
+// over several GPUs: the 8 corners of the interpolation support (voxel indices volStart - 1
+// .. volEnd) through the view's projective map; a box in front of the source maps inside
+// the hull of its corners' images.  Rows [lo, hi) are global detector rows; a view whose
+// footprint misses the detector gets lo = hi = 0.
+extern "C" int fcb_detector_rows(const fcb_geometry* g, int margin, int* rowLo, int* rowHi)
+{
+  using namespace fcb;
+  if (!rowLo || !rowHi || margin < 0) return set_error(FCB_ERR_INVALID, "bad detector-rows arguments");
+  Problem pb;
+  FCB_TRY(make_problem(g, &pb));
+  const int W = pb.projDim[0], H = pb.projDim[1];
+  double c[3][2];
+  for (int a = 0; a < 3; a++) {
+    c[a][0] = (double)(pb.volStart[a] - 1 - pb.volDim[a] / 2);
+    c[a][1] = (double)(pb.volEnd[a] - pb.volDim[a] / 2);
+  }
+  for (int t = 0; t < pb.nviews; t++) {
+    double M[12], kappa;
+    view_matrix(pb, t, M, &kappa);
+    double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
+    bool behind = false;
+    for (int k = 0; k < 8; k++) {
+      const double x = c[0][k & 1], y = c[1][(k >> 1) & 1], z = c[2][(k >> 2) & 1];
+      const double s = M[8] * x + M[9] * y + M[10] * z + M[11];
+      if (!(s > 1e-9)) { behind = true; break; }
+      const double u = (M[0] * x + M[1] * y + M[2] * z + M[3]) / s + pb.woff[t];
+      const double v = (M[4] * x + M[5] * y + M[6] * z + M[7]) / s + pb.hoff[t];
+      umin = std::min(umin, u); umax = std::max(umax, u);
+      vmin = std::min(vmin, v); vmax = std::max(vmax, v);
+    }
+    if (behind) {
+      rowLo[t] = 0;
+      rowHi[t] = H;
+      continue;
+    }
+    const double lo = std::floor(vmin) - margin, hi = std::floor(vmax) + 2 + margin;
+    const double wl = std::floor(umin) - margin, wh = std::floor(umax) + 2 + margin;
+    if (hi <= 0.0 || lo >= (double)H || wh <= 0.0 || wl >= (double)W) {
+      rowLo[t] = rowHi[t] = 0;
+      continue;
+    }
+    rowLo[t] = (int)std::max(0.0, lo);
+    rowHi[t] = (int)std::min((double)H, hi);
+  }
+  return ok();
+}

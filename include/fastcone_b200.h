@@ -278,6 +278,14 @@ int fcb_phantom_device(float* vol, const int volDim[3], const double* params, in
 int fcb_reference_windows(const fcb_geometry* g, int* subVolDim, int* subProjDim, int* tiles,
                           int* ws, int* hs, int* sweepStart, int* sweepSteps, int* matters);
 
+/* Per view t, the global detector rows [rowLo[t], rowHi[t]) that the sub-volume
+ * volStart..volEnd (widened by one voxel: the interpolation support) projects to, widened by
+ * `margin` rows and clipped to the detector; rowLo = rowHi = 0 where the footprint misses the
+ * detector.  FP64, host only.  Used to split one volume into z-slabs over several GPUs:
+ * each slab needs only these rows of each view (mpi_fastcone.py:450-526 moves whole
+ * per-chunk detector windows between MPI ranks for the same purpose). */
+int fcb_detector_rows(const fcb_geometry* g, int margin, int* rowLo, int* rowHi);
+
 #ifdef __cplusplus
 }
 #endif
