@@ -21,6 +21,7 @@
 // reconstructs (fdk_tma_kernel with the Tam-Danielsson window).
 #include <cufft.h>
 #include <math.h>
+#include <stdint.h>
 #include <stdlib.h>
 
 #include <algorithm>
@@ -30,130 +31,195 @@
 
 namespace fcb {
 
+// Element-wise stages: each thread handles CPT consecutive columns (4 with 16-byte vector
+// loads and stores when W is a multiple of 4, else 1); grid.x runs over the column groups of
+// one view, grid.y over the views.
+template <int CPT>
+__device__ __forceinline__ void ldv(const float* __restrict__ p, float (&v)[CPT])
+{
+  if constexpr (CPT == 4) {
+    const float4 x = *reinterpret_cast<const float4*>(p);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+    v[0] = *p;
+  }
+}
+template <int CPT>
+__device__ __forceinline__ void ldv(const int* __restrict__ p, int (&v)[CPT])
+{
+  if constexpr (CPT == 4) {
+    const int4 x = *reinterpret_cast<const int4*>(p);
+    v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+  } else {
+    v[0] = *p;
+  }
+}
+template <int CPT>
+__device__ __forceinline__ void stv(float* __restrict__ p, const float (&v)[CPT])
+{
+  if constexpr (CPT == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  else *p = v[0];
+}
+
+template <int CPT>
 __global__ void kats_deriv_kernel(const float* __restrict__ g, float* __restrict__ g2, int n, int H,
                                   int W, float dlam, float pw, float D, float su)
 {
-  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long tot = (long long)n * H * W;
-  if (idx >= tot) return;
-  const int i = (int)(idx % W);
-  const long long r = idx / W;
-  const int j = (int)(r % H), t = (int)(r / H);
+  const int Wq = W / CPT;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= H * Wq) return;
+  const int t = blockIdx.y;
+  const int j = q / Wq, i0 = (q - j * Wq) * CPT;
   const size_t plane = (size_t)H * W;
-  const float* gt = g + (size_t)t * plane;
+  const size_t o = (size_t)t * plane + (size_t)j * W + i0;
+  float c[CPT], a[CPT], b[CPT], dl[CPT], dgu[CPT], dgv[CPT], r[CPT];
+  ldv<CPT>(g + o, c);
   // dg/dlam: central inside, one-sided at the ends (numpy.gradient, edge order 1)
-  float dl;
-  if (n == 1) dl = 0.0f;
-  else if (t == 0) dl = (g[plane + (size_t)j * W + i] - gt[(size_t)j * W + i]) / dlam;
-  else if (t == n - 1) dl = (gt[(size_t)j * W + i] - g[(size_t)(t - 1) * plane + (size_t)j * W + i]) / dlam;
-  else dl = (g[(size_t)(t + 1) * plane + (size_t)j * W + i] - g[(size_t)(t - 1) * plane + (size_t)j * W + i]) / (2.0f * dlam);
-  // dg/du with u_i = su * (i - W/2) pw
+  if (n == 1) {
+#pragma unroll
+    for (int k = 0; k < CPT; k++) dl[k] = 0.0f;
+  } else if (t == 0) {
+    ldv<CPT>(g + o + plane, a);
+#pragma unroll
+    for (int k = 0; k < CPT; k++) dl[k] = (a[k] - c[k]) / dlam;
+  } else if (t == n - 1) {
+    ldv<CPT>(g + o - plane, b);
+#pragma unroll
+    for (int k = 0; k < CPT; k++) dl[k] = (c[k] - b[k]) / dlam;
+  } else {
+    ldv<CPT>(g + o + plane, a);
+    ldv<CPT>(g + o - plane, b);
+#pragma unroll
+    for (int k = 0; k < CPT; k++) dl[k] = (a[k] - b[k]) / (2.0f * dlam);
+  }
+  // dg/du with u_i = su * (i - W/2) pw; e = the row from column i0 - 1 to i0 + CPT
   const float du = su * pw;
-  float dgu;
-  if (W == 1) dgu = 0.0f;
-  else if (i == 0) dgu = (gt[(size_t)j * W + 1] - gt[(size_t)j * W]) / du;
-  else if (i == W - 1) dgu = (gt[(size_t)j * W + i] - gt[(size_t)j * W + i - 1]) / du;
-  else dgu = (gt[(size_t)j * W + i + 1] - gt[(size_t)j * W + i - 1]) / (2.0f * du);
-  float dgv;
-  if (H == 1) dgv = 0.0f;
-  else if (j == 0) dgv = (gt[(size_t)W + i] - gt[i]) / pw;
-  else if (j == H - 1) dgv = (gt[(size_t)j * W + i] - gt[(size_t)(j - 1) * W + i]) / pw;
-  else dgv = (gt[(size_t)(j + 1) * W + i] - gt[(size_t)(j - 1) * W + i]) / (2.0f * pw);
-  const float u = su * (float)(i - W / 2) * pw, v = (float)(j - H / 2) * pw;
-  const float g1 = dl + ((u * u + D * D) / D) * dgu + (u * v / D) * dgv;
-  g2[idx] = g1 * (D * rsqrtf(u * u + D * D + v * v));
+  float e[CPT + 2];
+  e[0] = i0 > 0 ? g[o - 1] : 0.0f;
+#pragma unroll
+  for (int k = 0; k < CPT; k++) e[k + 1] = c[k];
+  e[CPT + 1] = i0 + CPT < W ? g[o + CPT] : 0.0f;
+#pragma unroll
+  for (int k = 0; k < CPT; k++) {
+    const int i = i0 + k;
+    if (W == 1) dgu[k] = 0.0f;
+    else if (i == 0) dgu[k] = (e[k + 2] - e[k + 1]) / du;
+    else if (i == W - 1) dgu[k] = (e[k + 1] - e[k]) / du;
+    else dgu[k] = (e[k + 2] - e[k]) / (2.0f * du);
+  }
+  if (H == 1) {
+#pragma unroll
+    for (int k = 0; k < CPT; k++) dgv[k] = 0.0f;
+  } else if (j == 0) {
+    ldv<CPT>(g + o + W, a);
+#pragma unroll
+    for (int k = 0; k < CPT; k++) dgv[k] = (a[k] - c[k]) / pw;
+  } else if (j == H - 1) {
+    ldv<CPT>(g + o - W, b);
+#pragma unroll
+    for (int k = 0; k < CPT; k++) dgv[k] = (c[k] - b[k]) / pw;
+  } else {
+    ldv<CPT>(g + o + W, a);
+    ldv<CPT>(g + o - W, b);
+#pragma unroll
+    for (int k = 0; k < CPT; k++) dgv[k] = (a[k] - b[k]) / (2.0f * pw);
+  }
+  const float v = (float)(j - H / 2) * pw;
+#pragma unroll
+  for (int k = 0; k < CPT; k++) {
+    const float u = su * (float)(i0 + k - W / 2) * pw;
+    const float g1 = dl[k] + ((u * u + D * D) / D) * dgu[k] + (u * v / D) * dgv[k];
+    r[k] = g1 * (D * rsqrtf(u * u + D * D + v * v));
+  }
+  stv<CPT>(g2 + o, r);
 }
 
-// g3[t][k][i] = g2[t][j0][i] * (1-a) + g2[t][j0+1][i] * a from the (kappa, column) table
+// g3[t][k][i] = g2[t][j0][i] * (1-a) + g2[t][j0+1][i] * a from the (kappa, column) table,
+// into rows of length L whose columns [W, L) stay zero (the Hilbert transform's padding,
+// written once when the plan is made).
+template <int CPT>
 __global__ void kats_rebin_fwd_kernel(const float* __restrict__ g2, float* __restrict__ g3,
                                       const int* __restrict__ j0tab, const float* __restrict__ atab,
-                                      int n, int H, int W, int K)
+                                      int H, int W, int K, int L)
 {
-  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long tot = (long long)n * K * W;
-  if (idx >= tot) return;
-  const int i = (int)(idx % W);
-  const long long r = idx / W;
-  const int k = (int)(r % K), t = (int)(r / K);
-  const int j0 = j0tab[(size_t)k * W + i];
-  float val = 0.0f;
-  if (j0 >= 0) {
-    const float a = atab[(size_t)k * W + i];
-    const float* col = g2 + (size_t)t * H * W + i;
-    const float v0 = col[(size_t)j0 * W];
-    const float v1 = (j0 + 1 < H) ? col[(size_t)(j0 + 1) * W] : v0;
-    val = fmaf(a, v1 - v0, v0);
+  const int Wq = W / CPT;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= K * Wq) return;
+  const int t = blockIdx.y;
+  const int k = q / Wq, i0 = (q - k * Wq) * CPT;
+  int j0[CPT];
+  float a[CPT], val[CPT];
+  ldv<CPT>(j0tab + (size_t)k * W + i0, j0);
+  ldv<CPT>(atab + (size_t)k * W + i0, a);
+  const float* base = g2 + (size_t)t * H * W + i0;
+#pragma unroll
+  for (int m = 0; m < CPT; m++) {
+    val[m] = 0.0f;
+    if (j0[m] >= 0) {
+      const float* col = base + m;
+      const float v0 = col[(size_t)j0[m] * W];
+      const float v1 = (j0[m] + 1 < H) ? col[(size_t)(j0[m] + 1) * W] : v0;
+      val[m] = fmaf(a[m], v1 - v0, v0);
+    }
   }
-  g3[idx] = val;
+  stv<CPT>(g3 + ((size_t)t * K + k) * L + i0, val);
 }
 
 // Hilbert transform of each row along u: out[i] = sgn * sum_j h(i - j) in[j],
-// h(m) = 2 / (pi m) for odd m, 0 otherwise; one block per row, the row staged in shared memory.
-__global__ void kats_hilbert_kernel(const float* __restrict__ in, float* __restrict__ out, int W,
-                                    float sgn)
+// h(m) = 2 / (pi m) for odd m, 0 otherwise; one block per row (stride L), the row staged in
+// shared memory (so the transform may run in place).
+__global__ void kats_hilbert_kernel(float* __restrict__ rows, int W, int L, float sgn)
 {
   extern __shared__ float row[];
   const size_t r = blockIdx.x;
-  for (int j = threadIdx.x; j < W; j += blockDim.x) row[j] = in[r * W + j];
+  for (int j = threadIdx.x; j < W; j += blockDim.x) row[j] = rows[r * L + j];
   __syncthreads();
   const float c = sgn * 0.63661977236758134f;  // 2 / pi
   for (int i = threadIdx.x; i < W; i += blockDim.x) {
     float acc = 0.0f;
     // j = i - m with m odd: j runs over the columns of opposite parity to i
     for (int j = (i & 1) ^ 1; j < W; j += 2) acc = fmaf(row[j], __frcp_rn((float)(i - j)), acc);
-    out[r * W + i] = c * acc;
+    rows[r * L + i] = c * acc;
   }
 }
 
-// FFT form of the same transform: rows zero-padded to L = 2W (linear, not circular,
-// convolution for |i - j| < W), multiplied by the spectrum of the discrete kernel, inverted.
-__global__ void kats_pad_kernel(const float* __restrict__ in, float* __restrict__ pad, long long row0,
-                                int nrows, int W, int L)
-{
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nrows * L) return;
-  const int c = (int)(i % L);
-  const long long r = i / L;
-  pad[i] = c < W ? in[(row0 + r) * W + c] : 0.0f;
-}
-
 // spec[r][k] *= i * himag[k] (the kernel is odd, so its spectrum is purely imaginary)
+// One block per row.
 __global__ void kats_spec_kernel(cufftComplex* __restrict__ spec, const float* __restrict__ himag,
-                                 int nrows, int nb)
+                                 int nb)
 {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nrows * nb) return;
-  const float h = himag[i % nb];
-  const cufftComplex z = spec[i];
-  spec[i] = make_cuFloatComplex(-z.y * h, z.x * h);
+  cufftComplex* row = spec + (size_t)blockIdx.x * nb;
+  for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+    const float h = himag[k];
+    const cufftComplex z = row[k];
+    row[k] = make_cuFloatComplex(-z.y * h, z.x * h);
+  }
 }
 
-__global__ void kats_crop_kernel(const float* __restrict__ pad, float* __restrict__ out, long long row0,
-                                 int nrows, int W, int L, float scale)
-{
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nrows * W) return;
-  const int c = (int)(i % W);
-  const long long r = i / W;
-  out[(row0 + r) * W + c] = scale * pad[r * L + c];
-}
-
-// gF[t][j][i] = g4[t][k0][i] * (1-a) + g4[t][k0+1][i] * a from the (row, column) table
+// gF[t0 + tl][j][i] = scale * (g4[tl][k0][i] * (1-a) + g4[tl][k0+1][i] * a) from the
+// (row, column) table; g4 holds the transformed kappa rows (length L) of views t0, t0 + 1, ...
+template <int CPT>
 __global__ void kats_rebin_bwd_kernel(const float* __restrict__ g4, float* __restrict__ gF,
                                       const int* __restrict__ k0tab, const float* __restrict__ atab,
-                                      int n, int H, int W, int K)
+                                      int H, int W, int K, int L, float scale, int t0)
 {
-  const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long tot = (long long)n * H * W;
-  if (idx >= tot) return;
-  const int i = (int)(idx % W);
-  const long long r = idx / W;
-  const int j = (int)(r % H), t = (int)(r / H);
-  const int k0 = k0tab[(size_t)j * W + i];
-  const float a = atab[(size_t)j * W + i];
-  const float* col = g4 + (size_t)t * K * W + i;
-  const float v0 = col[(size_t)k0 * W], v1 = col[(size_t)(k0 + 1) * W];
-  gF[idx] = fmaf(a, v1 - v0, v0);
+  const int Wq = W / CPT;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= H * Wq) return;
+  const int tl = blockIdx.y;
+  const int j = q / Wq, i0 = (q - j * Wq) * CPT;
+  int k0[CPT];
+  float a[CPT], r[CPT];
+  ldv<CPT>(k0tab + (size_t)j * W + i0, k0);
+  ldv<CPT>(atab + (size_t)j * W + i0, a);
+  const float* base = g4 + (size_t)tl * K * L + i0;
+#pragma unroll
+  for (int m = 0; m < CPT; m++) {
+    const float* col = base + m;
+    const float v0 = col[(size_t)k0[m] * L], v1 = col[(size_t)(k0[m] + 1) * L];
+    r[m] = scale * fmaf(a[m], v1 - v0, v0);
+  }
+  stv<CPT>(gF + ((size_t)(t0 + tl) * H + j) * W + i0, r);
 }
 
 }  // namespace fcb
@@ -179,19 +245,22 @@ static double frac_index(const std::vector<double>& xs, double x)
 // kernel's spectrum, the cuFFT plans and the intermediate buffers are made once; execute()
 // is stream-ordered, allocates nothing and does not synchronise.
 struct fcb_katsevich_plan {
-  int nviews = 0, H = 0, W = 0, K = 0, L = 0, nb = 0, batch = 0;
+  int nviews = 0, H = 0, W = 0, K = 0, L = 0, nb = 0;
+  int vb = 0;  // views per transform batch (the batch is vb * K kappa rows)
   float dlam = 0.0f, pw = 0.0f, D = 0.0f, su = 0.0f;
-  float *g2 = nullptr, *g3 = nullptr, *g4 = nullptr, *dfa = nullptr, *dba = nullptr;
+  float *g2 = nullptr, *dfa = nullptr, *dba = nullptr;
+  float* g3 = nullptr;  // kappa rows [views rounded up to whole batches][K][L]; [W, L) zero
+  float* g4 = nullptr;  // one batch of transformed rows [vb][K][L]
   int *dfj = nullptr, *dbk = nullptr;
-  float *hpad = nullptr, *dhim = nullptr;
-  cufftComplex* hspec = nullptr;
+  float* dhim = nullptr;
+  cufftComplex* hspec = nullptr;  // one batch of spectra
   cufftHandle pf = 0, pi = 0;
   ~fcb_katsevich_plan()
   {
     if (pf) cufftDestroy(pf);
     if (pi) cufftDestroy(pi);
     cudaFree(g2); cudaFree(g3); cudaFree(g4); cudaFree(dfa); cudaFree(dba); cudaFree(dfj);
-    cudaFree(dbk); cudaFree(hpad); cudaFree(hspec); cudaFree(dhim);
+    cudaFree(dbk); cudaFree(hspec); cudaFree(dhim);
   }
 };
 
@@ -203,6 +272,8 @@ extern "C" int fcb_katsevich_plan_create(int nviews, int H, int W, const float* 
   *out = nullptr;
   if (!angles || nviews < 2 || H < 2 || W < 2 || !(D > 0) || !(pw > 0) || pitch == 0.0f)
     return set_error(FCB_ERR_INVALID, "bad Katsevich filter arguments");
+  if (nviews > 65535 || H > 32768 || (nkappa > 1 && nkappa > 65535))
+    return set_error(FCB_ERR_INVALID, "Katsevich filter sizes above the grid limits (65535 views)");
   // mean angular step; float32 angles of several turns carry ~1e-6 rad of rounding each
   const double dlam = ((double)angles[nviews - 1] - (double)angles[0]) / (nviews - 1);
   for (int t = 1; t < nviews; t++) {
@@ -260,18 +331,27 @@ extern "C" int fcb_katsevich_plan_create(int nviews, int H, int W, const float* 
   auto* pl = new fcb_katsevich_plan();
   pl->nviews = nviews; pl->H = H; pl->W = W; pl->K = K; pl->L = L; pl->nb = nb;
   pl->dlam = (float)dlam; pl->pw = pw; pl->D = D; pl->su = (float)su;
-  const long long rows = (long long)nviews * K;
-  pl->batch = (int)std::min<long long>(rows, std::max<long long>(1, (256ll << 20) / (8ll * L)));
-  const size_t nhw = (size_t)nviews * H * W, nkw = (size_t)nviews * K * W;
+  // transform batches of whole views, up to 256 MiB of spectra each (larger batches gain
+  // nothing per transform and make the cuFFT plans and buffers slower to create); the
+  // kappa-row array is rounded up to whole batches and zeroed once (padding columns and rows
+  // are never written)
+  pl->vb = (int)std::min<long long>(nviews, std::max<long long>(1, (256ll << 20) / (8ll * nb * K)));
+  const long long rows_alloc = (long long)((nviews + pl->vb - 1) / pl->vb) * pl->vb * K;
+  const long long batch = (long long)pl->vb * K;
+  const size_t nhw = (size_t)nviews * H * W;
   int rc = FCB_OK;
   do {
-    if (cudaMalloc(&pl->g2, nhw * 4) || cudaMalloc(&pl->g3, nkw * 4) || cudaMalloc(&pl->g4, nkw * 4) ||
+    if (cudaMalloc(&pl->g2, nhw * 4) || cudaMalloc(&pl->g3, (size_t)rows_alloc * L * 4) ||
+        cudaMalloc(&pl->g4, (size_t)batch * L * 4) ||
         cudaMalloc(&pl->dfa, fa.size() * 4) || cudaMalloc(&pl->dba, ba.size() * 4) ||
         cudaMalloc(&pl->dfj, fj0.size() * 4) || cudaMalloc(&pl->dbk, bk0.size() * 4) ||
-        cudaMalloc(&pl->hpad, (size_t)pl->batch * L * 4) ||
-        cudaMalloc(&pl->hspec, (size_t)pl->batch * nb * sizeof(cufftComplex)) || cudaMalloc(&pl->dhim, nb * 4)) {
+        cudaMalloc(&pl->hspec, (size_t)batch * nb * sizeof(cufftComplex)) || cudaMalloc(&pl->dhim, nb * 4)) {
       cudaGetLastError();
       rc = set_error(FCB_ERR_NOMEM, "Katsevich filter scratch");
+      break;
+    }
+    if (cudaMemset(pl->g3, 0, (size_t)rows_alloc * L * 4) != cudaSuccess) {
+      rc = set_error(FCB_ERR_CUDA, "Katsevich scratch initialisation failed");
       break;
     }
     if (cudaMemcpy(pl->dfa, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice) ||
@@ -283,8 +363,8 @@ extern "C" int fcb_katsevich_plan_create(int nviews, int H, int W, const float* 
       break;
     }
     int n1[1] = {L};
-    if (cufftPlanMany(&pl->pf, 1, n1, nullptr, 1, L, nullptr, 1, nb, CUFFT_R2C, pl->batch) != CUFFT_SUCCESS ||
-        cufftPlanMany(&pl->pi, 1, n1, nullptr, 1, nb, nullptr, 1, L, CUFFT_C2R, pl->batch) != CUFFT_SUCCESS) {
+    if (cufftPlanMany(&pl->pf, 1, n1, nullptr, 1, L, nullptr, 1, nb, CUFFT_R2C, (int)batch) != CUFFT_SUCCESS ||
+        cufftPlanMany(&pl->pi, 1, n1, nullptr, 1, nb, nullptr, 1, L, CUFFT_C2R, (int)batch) != CUFFT_SUCCESS) {
       rc = set_error(FCB_ERR_CUDA, "cufftPlanMany failed");
       break;
     }
@@ -303,35 +383,45 @@ extern "C" int fcb_katsevich_plan_execute(fcb_katsevich_plan* pl, const float* i
   if (!pl || !in || !out) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const int nviews = pl->nviews, H = pl->H, W = pl->W, K = pl->K, L = pl->L, nb = pl->nb;
-  const size_t nhw = (size_t)nviews * H * W, nkw = (size_t)nviews * K * W;
-  kats_deriv_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(in, pl->g2, nviews, H, W, pl->dlam,
-                                                                   pl->pw, pl->D, pl->su);
-  kats_rebin_fwd_kernel<<<(unsigned)((nkw + 255) / 256), 256, 0, st>>>(pl->g2, pl->g3, pl->dfj, pl->dfa,
-                                                                       nviews, H, W, K);
+  // 16-byte vector accesses need 4 | W and 16-byte aligned caller buffers (the plan's own are)
+  const bool v4 = (W % 4) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) == 0 &&
+                  (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+  const int cpt = v4 ? 4 : 1;
+  const unsigned bx_hw = (unsigned)(((long long)H * (W / cpt) + 255) / 256);
+  const unsigned bx_kw = (unsigned)(((long long)K * (W / cpt) + 255) / 256);
+  if (v4) {
+    kats_deriv_kernel<4><<<dim3(bx_hw, nviews), 256, 0, st>>>(in, pl->g2, nviews, H, W, pl->dlam, pl->pw, pl->D, pl->su);
+    kats_rebin_fwd_kernel<4><<<dim3(bx_kw, nviews), 256, 0, st>>>(pl->g2, pl->g3, pl->dfj, pl->dfa, H, W, K, L);
+  } else {
+    kats_deriv_kernel<1><<<dim3(bx_hw, nviews), 256, 0, st>>>(in, pl->g2, nviews, H, W, pl->dlam, pl->pw, pl->D, pl->su);
+    kats_rebin_fwd_kernel<1><<<dim3(bx_kw, nviews), 256, 0, st>>>(pl->g2, pl->g3, pl->dfj, pl->dfa, H, W, K, L);
+  }
+  auto rebin_bwd = [&](const float* rows, int t0, int nv, float scale) {
+    if (v4) kats_rebin_bwd_kernel<4><<<dim3(bx_hw, nv), 256, 0, st>>>(rows, out, pl->dbk, pl->dba, H, W, K, L, scale, t0);
+    else kats_rebin_bwd_kernel<1><<<dim3(bx_hw, nv), 256, 0, st>>>(rows, out, pl->dbk, pl->dba, H, W, K, L, scale, t0);
+  };
   // the published Hilbert transform runs along increasing u; along w it changes sign when u = -w
   const char* direct = getenv("FCB_KATS_DIRECT_HILBERT");
   if (direct && direct[0] == '1') {
-    kats_hilbert_kernel<<<(unsigned)((size_t)nviews * K), 256, W * sizeof(float), st>>>(pl->g3, pl->g4, W,
-                                                                                        pl->su);
+    kats_hilbert_kernel<<<(unsigned)((size_t)nviews * K), 256, W * sizeof(float), st>>>(pl->g3, W, L, pl->su);
+    rebin_bwd(pl->g3, 0, nviews, 1.0f);
   } else {
     if (cufftSetStream(pl->pf, st) != CUFFT_SUCCESS || cufftSetStream(pl->pi, st) != CUFFT_SUCCESS)
       return set_error(FCB_ERR_CUDA, "cufftSetStream failed");
     const float scale = pl->su / (float)L;
-    const long long rows = (long long)nviews * K;
-    const int batch = pl->batch;
-    for (long long r0 = 0; r0 < rows; r0 += batch) {
-      const int nr = (int)std::min<long long>(batch, rows - r0);
-      kats_pad_kernel<<<(unsigned)(((long long)batch * L + 255) / 256), 256, 0, st>>>(pl->g3, pl->hpad, r0, nr, W, L);
-      if (nr < batch)
-        FCB_CUDA_TRY(cudaMemsetAsync(pl->hpad + (size_t)nr * L, 0, (size_t)(batch - nr) * L * 4, st));
-      if (cufftExecR2C(pl->pf, pl->hpad, pl->hspec) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecR2C failed");
-      kats_spec_kernel<<<(unsigned)(((long long)nr * nb + 255) / 256), 256, 0, st>>>(pl->hspec, pl->dhim, nr, nb);
-      if (cufftExecC2R(pl->pi, pl->hspec, pl->hpad) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecC2R failed");
-      kats_crop_kernel<<<(unsigned)(((long long)nr * W + 255) / 256), 256, 0, st>>>(pl->hpad, pl->g4, r0, nr, W, L, scale);
+    const int vb = pl->vb;
+    // per batch of whole views: R2C of the zero-padded kappa rows, multiplication by the
+    // kernel's spectrum, C2R into g4 (the padding in g3 stays zero), backward rebinning of
+    // the batch's views with the 1/L normalisation and the direction sign
+    for (int t0 = 0; t0 < nviews; t0 += vb) {
+      const int nv = std::min(vb, nviews - t0);
+      if (cufftExecR2C(pl->pf, pl->g3 + (size_t)t0 * K * L, pl->hspec) != CUFFT_SUCCESS)
+        return set_error(FCB_ERR_CUDA, "cufftExecR2C failed");
+      kats_spec_kernel<<<(unsigned)((long long)nv * K), 256, 0, st>>>(pl->hspec, pl->dhim, nb);
+      if (cufftExecC2R(pl->pi, pl->hspec, pl->g4) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecC2R failed");
+      rebin_bwd(pl->g4, t0, nv, scale);
     }
   }
-  kats_rebin_bwd_kernel<<<(unsigned)((nhw + 255) / 256), 256, 0, st>>>(pl->g4, out, pl->dbk, pl->dba, nviews, H,
-                                                                      W, K);
   FCB_CUDA_TRY(cudaGetLastError());
   return ok();
 }

@@ -236,8 +236,9 @@ int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, 
                                 void* stream);
 
 /* The same filter as a reusable plan for one helix and detector: kappa-line tables, the
- * Hilbert kernel's spectrum, cuFFT plans and intermediate buffers made once (about
- * 4 x nviews x 2H x W floats of device memory); execute is stream-ordered, allocates nothing
+ * Hilbert kernel's spectrum, cuFFT plans and intermediate buffers made once (nviews x H x W
+ * floats plus nviews x nkappa x 2W floats of zero-padded kappa rows, plus 0.5 GiB of transform
+ * batches); execute is stream-ordered, allocates nothing
  * and does not synchronise.  One execute at a time per plan. */
 typedef struct fcb_katsevich_plan fcb_katsevich_plan;
 int fcb_katsevich_plan_create(int nviews, int H, int W, const float* angles, float D, float pw,
