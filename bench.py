@@ -107,7 +107,8 @@ def run_case(args):
     proj-512: the staged, unstaged and texture projectors on 512^3, 90 views, 768x512
     detector (0.5 GB volume);
     conv-256: one unrolled step's convolutions at 256^3 x 16 BF16 channels (0.54 GB per
-    activation): forward, input gradient (tensor cores) and weight gradient;
+    activation): forward (three kernel forms) and weight gradient (tensor cores and the
+    CUDA-core kernel), all on tcgen05 except the last;
     katsevich: the helical PI-window backprojection (512x512x384, 4640 views; 1.3 GB);
     pipeline: every other kernel once at a moderate size, inputs above L2 where the workload
     allows: phantom, FDK filter (ramp + Shepp-Logan), Katsevich filter, projector adjoint,
@@ -216,10 +217,18 @@ def run_case(args):
                     os.environ.pop("FCB_CONV_SIMPLE", None)
             return run
 
+        def wgrad_simt():
+            os.environ["FCB_WGRAD_SIMT"] = "1"
+            try:
+                return nn.conv3d16_wgrad(x, x)
+            finally:
+                os.environ.pop("FCB_WGRAD_SIMT", None)
+
         for name, fn in (("fwd", lambda: nn.conv3d16(x, wk, b, relu=True)),
                          ("fwd_one_tile_per_cta", fwd_variant("1")),
                          ("fwd_persistent_no_row_reuse", fwd_variant("2")),
-                         ("wgrad", lambda: nn.conv3d16_wgrad(x, x))):
+                         ("wgrad", lambda: nn.conv3d16_wgrad(x, x)),
+                         ("wgrad_cuda_cores", wgrad_simt)):
             for _ in range(args.warmup):
                 fn()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

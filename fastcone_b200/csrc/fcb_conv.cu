@@ -15,8 +15,9 @@
 // ReLU and store.
 //
 // The same kernels compute the input gradient (transposed, tap-flipped weights, prepared by
-// the caller).  conv3d16p_kernel is the persistent, pipelined form used by default.  The weight gradient, a 6912-entry reduction over all voxels, runs on the
-// CUDA cores (fcb_conv3d16_wgrad_device).
+// the caller); conv3d16r_kernel (row reuse) is the default form.  The weight gradient, a
+// 6912-entry reduction over all voxels, runs on the tensor cores too
+// (conv3d16_wgrad_tc_kernel, BF16 dY) with a CUDA-core kernel for FP32 dY and comparison.
 #include <stdlib.h>
 #include <string.h>
 
@@ -687,6 +688,302 @@ __global__ void __launch_bounds__(256) conv3d16_wgrad_kernel(const WgradParams P
   for (int t = 0; t < 27; t++) atomicAdd(P.dw + (t * 16 + co) * 16 + ci, acc[t]);
 }
 
+// Weight gradient on the tensor cores (BF16 dY).  dW[t][co][ci] = sum over voxels v of
+// dY[v][co] X[v + off(t)][ci] is a GEMM whose reduction dimension K is the voxels, 16 per
+// MMA.  For one input row r = (dz, dy) and u = the X voxels x0-1 .. x0+142 of a 128-voxel
+// tile (9 K-steps of 16):
+//   D_r[s*16 + co][ci] = sum_u A[s*16 + co][u] * X_r[u][ci],   A[s*16 + co][u] = dY[u + 1 - s][co]
+// with dY taken as zero outside the tile: rows s = 0, 1, 2 of D_r are the taps dx = s of row
+// r (v = u + 1 - s runs over the tile).  The three dy rows of one dz sit in consecutive
+// shared-memory slots, so one MMA per (K-step, dz) covers them: M = 128 (rows 0-47 used),
+// N = 48 (dy, ci), K = 16 -- 27 MMAs per tile give all 27 taps.  A lives in tensor memory:
+// warps 0-1 write the three shifted copies of the tile's dY (lane = s*16 + co, 16-bit voxel
+// pairs packed per 32-bit column) with tcgen05.st from the staged dY row; B is the staged X
+// rows, MN-major straight from the activation layout (8 channels of one voxel = one 16-byte
+// core-matrix row).  TMEM: 3 accumulators of 48 columns (144) + WGT_ABUF A buffers of 72.
+// A CTA walks chunks of CVR_YCH consecutive y rows of one (x tile, z) column; each tile loads
+// its 3 new X rows into a ring of WGT_RING positions per dz, rows at positions 0 and 1 also
+// into positions WGT_RING and WGT_RING + 1, so that rows y-1, y, y+1 always occupy three
+// consecutive slots (a uniform N stride for B); dY rows are staged WGT_LEAD deep;
+//   warp 2 (one lane): TMA producer, up to WGT_LEAD tiles ahead of the MMAs;
+//   warps 0-1:         A writers (per tile), then the epilogue: TMEM lanes 0-47 of the
+//                      accumulators -> dW (FP32 atomics, once per CTA);
+//   warp 3 (one lane): MMA issuer, commits to the tile's done barrier.
+// Dynamic shared memory above half an SM's keeps one CTA per SM (512-column allocation).
+constexpr int WGT_THREADS = 128;
+constexpr int WGT_KSTEPS = 9;                        // 144 voxels u per tile
+constexpr int WGT_XROW = 148;                        // staged X voxels per row (from x0 - 2)
+constexpr int WGT_RB = 2432;                         // one channel half of a staged X row, 128-B multiple
+static_assert(WGT_XROW * 16 <= WGT_RB && (WGT_KSTEPS * 16 + 1) * 16 <= WGT_XROW * 16, "X row slot");
+constexpr int WGT_DY_BYTES = 2048;                   // one channel half of 128 dY voxels (TMA box)
+constexpr int WGT_DYH = 2432;                        // its slot: 8 zero voxels, the box, 16 zero voxels
+// Pipeline depth: X rows in a ring of WGT_RING positions per dz, so the producer runs up to
+// WGT_LEAD = WGT_RING - 2 tiles ahead of the MMAs; as many dY stages; WGT_ABUF A buffers.
+constexpr int WGT_RING = 8;
+constexpr int WGT_LEAD = WGT_RING - 2;
+constexpr int WGT_ABUF = 3;
+constexpr int WGT_DY = WGT_LEAD * 2 * WGT_DYH;       // dY stages x 2 halves
+constexpr int WGT_XPOS = WGT_RING + 2;               // ring positions + the two duplicates
+constexpr int WGT_X = 3 * WGT_XPOS * 2 * WGT_RB;     // X row ring
+constexpr int WGT_BAR = WGT_DY + WGT_X;
+constexpr int WGT_NBAR = 2 * WGT_RING + WGT_ABUF + 1;
+constexpr int WGT_SMEM_USED = WGT_BAR + 8 * WGT_NBAR + 16;
+static_assert(WGT_DYH >= (8 + CV_TILE + 16) * 16 && WGT_DYH % 128 == 0 && WGT_DY % 128 == 0, "dY slots");
+constexpr int WGT_SMEM = 200 * 1024;                 // > half an SM: one CTA per SM
+static_assert(WGT_SMEM_USED <= WGT_SMEM, "wgrad shared memory");
+constexpr uint32_t WGT_ACOL = 144;                   // first A column (after the 9 accumulators)
+constexpr uint32_t WGT_ACOLS = WGT_KSTEPS * 8;       // 72 columns per A buffer
+static_assert(WGT_ACOL + WGT_ABUF * WGT_ACOLS <= 512, "TMEM columns");
+
+struct WgradTcParams {
+  float* dw;
+  int nx, ny, nz, tiles_x, pairs;
+  uint32_t xbox_bytes;
+  int* status;
+};
+
+namespace tc {
+// D(tmem) (+)= A(tmem) * B(smem desc), BF16 inputs, FP32 accumulator.
+__device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.u32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// 32 lanes x 8 consecutive 32-bit columns from registers: thread i writes lane (base + i).
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8])
+{
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+               "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+}  // namespace tc
+
+__global__ void __launch_bounds__(WGT_THREADS, 1) conv3d16_wgrad_tc_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                                         const __grid_constant__ CUtensorMap dymap,
+                                                                         const __grid_constant__ WgradTcParams P,
+                                                                         int nchunks)
+{
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* DY = smem;
+  unsigned char* X = smem + WGT_DY;
+  uint64_t* rows_full = reinterpret_cast<uint64_t*>(smem + WGT_BAR);  // [WGT_RING] per tile
+  uint64_t* tile_done = rows_full + WGT_RING;                           // [WGT_RING] per tile
+  uint64_t* a_full = tile_done + WGT_RING;                              // [WGT_ABUF] A buffer written
+  uint64_t* fin = a_full + WGT_ABUF;                                    // every MMA of the CTA done
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+  volatile int* failed_flag = reinterpret_cast<volatile int*>(tslot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ych = (P.ny + CVR_YCH - 1) / CVR_YCH;
+
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < WGT_RING; q++) {
+      dev::mbar_init(&rows_full[q], 1);
+      dev::mbar_init(&tile_done[q], 1);
+    }
+    for (int b = 0; b < WGT_ABUF; b++) dev::mbar_init(&a_full[b], 2);
+    dev::mbar_init(fin, 1);
+    *failed_flag = 0;
+    dev::fence_mbar_init();
+  }
+  // the dY slots' margins (voxels x0-8 .. x0-1 and x0+128 .. x0+143) stay zero: dY outside
+  // the tile, which the shifted copies must not see
+  for (int q = threadIdx.x; q < 2 * WGT_LEAD * 24; q += blockDim.x) {
+    const int slot = q / 24, v = q % 24;
+    reinterpret_cast<uint4*>(DY + slot * WGT_DYH)[v < 8 ? v : 128 + v] = make_uint4(0, 0, 0, 0);
+  }
+  if (warp == 3) {
+    tc::tmem_alloc(tslot, 512);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t taddr = *tslot;
+
+  auto chunk_of = [&](int c, int& x0, int& z, int& y0, int& y1) {
+    const int yc = c % ych, col = c / ych;
+    x0 = (col % P.tiles_x) * CV_TILE;
+    z = col / P.tiles_x;
+    y0 = yc * CVR_YCH;
+    y1 = min(P.ny, y0 + CVR_YCH);
+  };
+  int last = -1;  // tiles this CTA handles, minus one
+  for (int c = blockIdx.x; c < nchunks; c += gridDim.x) {
+    int x0, z, y0, y1;
+    chunk_of(c, x0, z, y0, y1);
+    last += y1 - y0;
+  }
+
+  if (warp == 2) {
+    // ---------------------------------------------------------------- TMA producer
+    if (lane == 0) {
+      dev::tma_prefetch(&xmap);
+      dev::tma_prefetch(&dymap);
+      int i = 0, issued = 0;
+      bool failed = false;
+      for (int c = blockIdx.x; c < nchunks && !failed; c += gridDim.x) {
+        int x0, z, y0, y1;
+        chunk_of(c, x0, z, y0, y1);
+        for (int y = y0; y < y1; y++, i++) {
+          const bool start = y == y0;
+          // the X slot refilled now (row y + 1) was last read by tile i - WGT_LEAD, every slot
+          // at a new chunk by tile i-1; the dY stage by the A writers of tile i - WGT_LEAD,
+          // which finished before its MMAs
+          const int wt = start ? i - 1 : i - WGT_LEAD;
+          if (wt >= 0 && !dev::mbar_wait(&tile_done[wt % WGT_RING], (wt / WGT_RING) & 1)) {
+            dev::record_status(P.status, DEV_TIMEOUT);
+            *failed_flag = 1;
+            failed = true;
+            break;
+          }
+          const int r0 = start ? -1 : 1;  // new rows y + r0 .. y + 1
+          int ncopies = 0;
+          for (int dy = r0; dy <= 1; dy++) ncopies += ((y + dy) & (WGT_RING - 1)) < 2 ? 2 : 1;
+          uint64_t* full = &rows_full[i % WGT_RING];
+          dev::mbar_arrive_expect_tx(full, (uint32_t)(3 * ncopies) * 2u * P.xbox_bytes + 2u * WGT_DY_BYTES);
+          for (int dz = 0; dz < 3; dz++)
+            for (int dy = r0; dy <= 1; dy++) {
+              const int yy = y + dy, pos = yy & (WGT_RING - 1);
+              for (int dup = 0; dup < (pos < 2 ? 2 : 1); dup++) {
+                unsigned char* slot = X + (dz * WGT_XPOS + pos + dup * WGT_RING) * 2 * WGT_RB;
+                for (int kh = 0; kh < 2; kh++)
+                  tc::tma_load_5d(slot + kh * WGT_RB, &xmap, full, 0, P.pairs ? (x0 >> 1) - 1 : x0 - 1, kh, yy,
+                                  z + dz - 1);
+              }
+            }
+          unsigned char* dst = DY + (i % WGT_LEAD) * 2 * WGT_DYH + 128;  // after the 8 zero voxels
+          for (int kh = 0; kh < 2; kh++)
+            tc::tma_load_5d(dst + kh * WGT_DYH, &dymap, full, 0, P.pairs ? (x0 >> 1) : x0, kh, y, z);
+          issued = i + 1;
+        }
+      }
+      for (int j = max(0, issued - WGT_RING); j < issued; j++)
+        dev::mbar_wait(&rows_full[j % WGT_RING], (j / WGT_RING) & 1, 100000000ull);
+    }
+  } else if (warp == 3) {
+    // ---------------------------------------------------------------- MMA issuer
+    if (lane == 0) {
+      const uint32_t xbase = dev::smem_u32(X);
+      // M = 128 (rows 0-47 used), N = 48, A K-major in TMEM, B MN-major in shared memory
+      constexpr uint32_t IDESC = tc::idesc_bf16(CV_TILE, 48) | (1u << 16);
+      int i = 0;
+      bool failed = false;
+      for (int c = blockIdx.x; c < nchunks && !failed; c += gridDim.x) {
+        int x0, z, y0, y1;
+        chunk_of(c, x0, z, y0, y1);
+        for (int y = y0; y < y1; y++, i++) {
+          if (!dev::mbar_wait(&rows_full[i % WGT_RING], (i / WGT_RING) & 1) ||
+              !dev::mbar_wait(&a_full[i % WGT_ABUF], (i / WGT_ABUF) & 1)) {
+            dev::record_status(P.status, DEV_TIMEOUT);
+            *failed_flag = 1;
+            failed = true;
+            break;
+          }
+          tc::fence_after();
+          // MN-major B over the slots of rows y-1, y, y+1 of one dz: N core matrices (dy, ci
+          // half) every WGT_RB bytes (SBO), K core matrices of 8 voxels every 128 bytes (LBO);
+          // a K-step of 16 voxels moves the start address by 256 B (16 in the descriptor's
+          // address field, which stays below 2^14 inside shared memory)
+          uint64_t bd[3];
+          const int p0 = (y - 1) & (WGT_RING - 1);
+#pragma unroll
+          for (int dz = 0; dz < 3; dz++)
+            bd[dz] = tc::smem_desc(xbase + (dz * WGT_XPOS + p0) * 2 * WGT_RB + P.pairs * 16, 128, WGT_RB);
+          const uint32_t aaddr = taddr + WGT_ACOL + (uint32_t)(i % WGT_ABUF) * WGT_ACOLS;
+          for (int ks = 0; ks < WGT_KSTEPS; ks++) {
+            const uint32_t acc = (i > 0 || ks > 0) ? 1u : 0u;
+#pragma unroll
+            for (int dz = 0; dz < 3; dz++)
+              tc::mma_bf16_ts(taddr + (uint32_t)(dz * 48), aaddr + (uint32_t)(ks * 8), bd[dz] + (uint64_t)(ks * 16),
+                              IDESC, acc);
+          }
+          tc::mma_commit(&tile_done[i % WGT_RING]);
+        }
+      }
+      // one phase that completes when every MMA issued here has (or at once if none was)
+      if (i > 0) tc::mma_commit(fin);
+      else dev::mbar_arrive(fin);
+    }
+  } else {
+    // ---------------------------------------------------------------- A writers (warps 0-1)
+    const int m = warp * 32 + lane;  // TMEM lane = s * 16 + co
+    const int s = m >> 4, co = m & 15;
+    const int se = s < 3 ? s : 2;    // lanes 48-63 (unused rows of D) copy s = 2
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    int i = 0;
+    bool failed = false;
+    for (int c = blockIdx.x; c < nchunks && !failed; c += gridDim.x) {
+      int x0, z, y0, y1;
+      chunk_of(c, x0, z, y0, y1);
+      for (int y = y0; y < y1; y++, i++) {
+        // the dY row of tile i is staged, and the A buffer's previous readers (the MMAs of
+        // tile i - WGT_ABUF) are done
+        bool ok = dev::mbar_wait(&rows_full[i % WGT_RING], (i / WGT_RING) & 1);
+        const int pt = i - WGT_ABUF;
+        if (ok && pt >= 0) ok = dev::mbar_wait(&tile_done[pt % WGT_RING], (pt / WGT_RING) & 1);
+        if (!__all_sync(0xffffffffu, ok)) {
+          if (lane == 0) {
+            dev::record_status(P.status, DEV_TIMEOUT);
+            *failed_flag = 1;
+          }
+          failed = true;
+          break;
+        }
+        tc::fence_after();
+        // A[u] = dY[x0 + rel], rel = 16 ks + k - s: slot voxel rel + 8 (zero outside the tile)
+        const unsigned short* dyb = reinterpret_cast<const unsigned short*>(
+            DY + (i % WGT_LEAD) * 2 * WGT_DYH + (co >> 3) * WGT_DYH + (8 - se) * 16) + (co & 7);
+        const uint32_t acol = WGT_ACOL + (uint32_t)(i % WGT_ABUF) * WGT_ACOLS;
+#pragma unroll 1
+        for (int ks = 0; ks < WGT_KSTEPS; ks++) {
+          const unsigned short* p = dyb + ks * 16 * 8;
+          uint32_t pk[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) pk[j] = (uint32_t)p[(2 * j) * 8] | ((uint32_t)p[(2 * j + 1) * 8] << 16);
+          tc::tmem_st8(taddr + lane_base + acol + (uint32_t)(ks * 8), pk);
+        }
+        tc::tmem_wait_st();
+        tc::fence_before();
+        __syncwarp();
+        if (lane == 0) dev::mbar_arrive(&a_full[i % WGT_ABUF]);
+      }
+    }
+    // ---------------------------------------------------------------- epilogue
+    if (last >= 0) {
+      const bool done = __all_sync(0xffffffffu, dev::mbar_wait(fin, 0)) != 0;
+      tc::fence_after();
+      if (done && !*failed_flag) {
+        for (int r = 0; r < 9; r++) {
+          uint32_t v[16];
+          tc::tmem_ld16(taddr + lane_base + (uint32_t)(r * 16), v);
+          if (s < 3) {
+            float* d = P.dw + ((r * 3 + s) * 16 + co) * 16;
+#pragma unroll
+            for (int q = 0; q < 16; q++) atomicAdd(d + q, __uint_as_float(v[q]));
+          }
+        }
+      } else if (!done && lane == 0) {
+        dev::record_status(P.status, DEV_TIMEOUT);
+      }
+    }
+  }
+  // every MMA issued must be complete before the columns are released
+  if (warp == 3 && lane == 0 && last >= 0) dev::mbar_wait(fin, 0, 100000000ull);
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 3) {
+    tc::fence_after();
+    tc::tmem_dealloc(taddr, 512);
+  }
+}
+
 }  // namespace fcb
 
 using namespace fcb;
@@ -754,6 +1051,39 @@ extern "C" int fcb_conv3d16_wgrad_device(const void* x, const void* dy, int dyTy
   if (!x || !dy || !dw || nx <= 0 || ny <= 0 || nz <= 0 || (dyType != FCB_F32 && dyType != FCB_BF16))
     return set_error(FCB_ERR_INVALID, "bad conv3d wgrad arguments");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  // BF16 dY: tensor cores (FCB_WGRAD_SIMT=1 selects the CUDA-core kernel for comparison)
+  const char* simt = getenv("FCB_WGRAD_SIMT");
+  if (dyType == FCB_BF16 && !(simt && simt[0] == '1')) {
+    if (((uintptr_t)x & 15) || ((uintptr_t)dy & 15))
+      return set_error(FCB_ERR_INVALID, "conv3d wgrad buffers must be 16-byte aligned");
+    const bool pairs = nx % 2 == 0;
+    const uint64_t dims[5] = {pairs ? 16u : 8u, (uint64_t)(pairs ? nx / 2 : nx), 2, (uint64_t)ny, (uint64_t)nz};
+    const uint64_t strides[4] = {pairs ? 32u : 16u, 16ull * nx, 32ull * nx, 32ull * nx * ny};
+    const uint32_t xbox[5] = {pairs ? 16u : 8u, pairs ? (uint32_t)WGT_XROW / 2 : (uint32_t)WGT_XROW - 2, 1, 1, 1};
+    const uint32_t dybox[5] = {pairs ? 16u : 8u, pairs ? (uint32_t)CV_TILE / 2 : (uint32_t)CV_TILE, 1, 1, 1};
+    CUtensorMap xmap, dymap;
+    FCB_TRY(encode_tmap(&xmap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(x), dims, strides, xbox));
+    FCB_TRY(encode_tmap(&dymap, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(dy), dims, strides, dybox));
+    int* status = nullptr;
+    FCB_TRY(device_status_ptr(&status));
+    WgradTcParams T;
+    T.dw = dw;
+    T.nx = nx; T.ny = ny; T.nz = nz;
+    T.tiles_x = (nx + CV_TILE - 1) / CV_TILE;
+    T.pairs = pairs ? 1 : 0;
+    T.xbox_bytes = xbox[0] * xbox[1] * 2;
+    T.status = status;
+    const long long nchunks = (long long)T.tiles_x * nz * ((ny + CVR_YCH - 1) / CVR_YCH);
+    if (nchunks > 0x7fffffffll) return set_error(FCB_ERR_RANGE, "conv3d volume too large");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    FCB_CUDA_TRY(cudaFuncSetAttribute(conv3d16_wgrad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, WGT_SMEM));
+    const int grid = (int)std::min<long long>(nchunks, sms);
+    conv3d16_wgrad_tc_kernel<<<grid, WGT_THREADS, WGT_SMEM, st>>>(xmap, dymap, T, (int)nchunks);
+    FCB_CUDA_TRY(cudaGetLastError());
+    return ok();
+  }
   WgradParams P;
   P.x = reinterpret_cast<const __nv_bfloat16*>(x);
   P.dy = dy;

@@ -4,8 +4,9 @@ Activations are BF16 volumes of 16 channels in the kernels' channel-half-major l
 ``[nz, ny, 2, nx, 8]`` (channel c at ``[:, :, c // 8, :, c % 8]``; ``to_layout`` /
 ``from_layout`` convert from / to ``[16, nz, ny, nx]``); a layer with fewer channels is
 zero-padded to 16 (the kernels' fixed width).  Forward and input gradient run the
-tensor-core kernel (``fcb_conv3d16_device``), the weight gradient the CUDA-core reduction
-(``fcb_conv3d16_wgrad_device``); master weights stay FP32 and are rounded to BF16 per call.
+tensor-core kernel (``fcb_conv3d16_device``), the weight gradient the tensor-core reduction
+over voxels (``fcb_conv3d16_wgrad_device`` with BF16 dY); master weights stay FP32 and are
+rounded to BF16 per call.
 """
 from __future__ import annotations
 

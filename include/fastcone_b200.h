@@ -258,7 +258,9 @@ int fcb_conv3d16_device(const void* x, const void* w, const float* bias, void* y
                         int ny, int nz, int relu, void* stream);
 
 /* Weight gradient of fcb_conv3d16_device: dw[t][co][ci] += sum_v dy[v][co] x[v + tap t][ci]
- * (FP32, accumulated); dy of dyType (FCB_F32 / FCB_BF16), x BF16, both [nz][ny][2][nx][8]. */
+ * (FP32, accumulated); dy of dyType (FCB_F32 / FCB_BF16), x BF16, both [nz][ny][2][nx][8].
+ * BF16 dy runs on the tcgen05 tensor cores (16-byte aligned buffers; FP32 accumulation in
+ * tensor memory, one FP32 atomic add per output and CTA), FP32 dy on the CUDA cores. */
 int fcb_conv3d16_wgrad_device(const void* x, const void* dy, int dyType, float* dw, int nx, int ny,
                               int nz, void* stream);
 

@@ -1,6 +1,8 @@
 """tcgen05 3x3x3 convolution vs torch.nn.functional.conv3d in FP32 on the same BF16-rounded
-inputs (FP32 accumulation both sides: rel-L2 <= 1e-5), input and weight gradients vs torch
-autograd (rel-L2 <= 1e-2 -- the gradient flowing in is rounded to BF16 by design)."""
+inputs (FP32 accumulation both sides: rel-L2 <= 1e-5), the tcgen05 weight gradient vs
+torch's in FP32 on the same BF16 inputs (rel-L2 <= 2e-4: sums over up to 5e5 voxels in a
+different order), input and weight gradients vs torch autograd (rel-L2 <= 1e-2 -- the
+gradient flowing in is rounded to BF16 by design)."""
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -103,3 +105,34 @@ def test_persistent_conv_equals_one_tile_per_cta(shape, monkeypatch):
     torch.cuda.synchronize()
     assert torch.equal(y1, y2)
     assert torch.equal(y3, y2)
+
+
+@pytest.mark.parametrize("shape", [(20, 17, 130), (3, 5, 7), (6, 70, 128), (37, 41, 300), (1, 1, 5), (9, 33, 257)])
+def test_wgrad_tensor_cores_vs_torch(shape, monkeypatch):
+    """The tcgen05 weight gradient (BF16 x and dY, FP32 accumulation) against torch's FP32
+    weight gradient on the same values and against the CUDA-core kernel: odd and even x
+    extents (single-voxel and voxel-pair boxes), partial x tiles, chunks longer than 32
+    rows, and fewer tiles than SMs."""
+    import torch
+
+    from fastcone_b200 import nn, ops
+
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x = _act(shape, g, torch.bfloat16)
+    gy = _act(shape, g, torch.bfloat16)
+    monkeypatch.delenv("FCB_WGRAD_SIMT", raising=False)
+    dw = nn.conv3d16_wgrad(x, gy)
+    ops.sync_status()
+    xr = nn.from_layout(x).float().unsqueeze(0)
+    gr = nn.from_layout(gy).float().unsqueeze(0)
+    tf32 = torch.backends.cudnn.allow_tf32
+    torch.backends.cudnn.allow_tf32 = False
+    try:
+        ref = torch.nn.grad.conv3d_weight(xr, (16, 16, 3, 3, 3), gr, padding=1)
+    finally:
+        torch.backends.cudnn.allow_tf32 = tf32
+    assert _rel(nn.from_kernel_weights(dw), ref) < 2e-4, _rel(nn.from_kernel_weights(dw), ref)
+    monkeypatch.setenv("FCB_WGRAD_SIMT", "1")
+    dw2 = nn.conv3d16_wgrad(x, gy)
+    torch.cuda.synchronize()
+    assert _rel(dw2, dw) < 2e-4
