@@ -1,0 +1,74 @@
+"""Speed against the reference's OWN CUDA path on the same B200 (oracle/_ref: the reference
+sources compiled unmodified, texture references mapped onto texture objects), through the
+same host-buffer entry point (GPU_CB_K_backproject's arguments, fastcone.backproject), on
+the small circular FDK problem: 128^3 voxels, 180 views, 192x128 detector, D = 500,
+pw = 0.5 (3.77e8 voxel-view updates).  Both calls include their host<->device copies and
+set-up; the timings (best of 3 after a warm-up) are printed with -s.
+
+The 1024^3 / 1440-view comparison runs the same way when FCB_TIME_REFERENCE_LARGE=1 (the
+reference's host-side caching takes tens of seconds there; off by default)."""
+import os
+import time
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _need_ref():
+    if O.reflib() is None:
+        pytest.skip("oracle/_ref/libfastcone_ref.so not built")
+
+
+def _best(fn, reps):
+    fn()
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        best = min(best, time.perf_counter() - t0)
+    return best
+
+
+def _compare(vol_xyz, det_wh, nviews, D, pw, reps):
+    from fastcone_b200 import fastcone as fc
+
+    norm = np.full(nviews, 1.0 / nviews, np.float32)
+    pb = O.make_problem(vol_xyz, det_wh, nviews, D=D, pw=pw, norm=norm)
+    proj = np.random.default_rng(0).random(pb.proj_shape, dtype=np.float32)
+    upd = float(np.prod(vol_xyz)) * nviews
+
+    def ours():
+        vol = np.zeros(pb.vol_shape_zyx, np.float32)
+        fc.backproject(vol, proj, pb.angles, pb.D, pb.hMid, norm=norm, kernelMode=2, pixelWidth=pb.pw)
+        return vol
+
+    def ref():
+        return O.reflib_backproject(pb, proj, kernel_mode=2)
+
+    t_ours = _best(ours, reps)
+    t_ref = _best(ref, reps)
+    err = O.rel_l2(ours(), ref())
+    print(f"\n{vol_xyz} x {nviews} views: ours {t_ours * 1e3:.1f} ms ({upd / t_ours / 1e9:.1f} GUPS), "
+          f"reference CUDA path {t_ref * 1e3:.1f} ms ({upd / t_ref / 1e9:.1f} GUPS), "
+          f"ratio {t_ref / t_ours:.1f}, rel-L2 {err:.2e}")
+    return t_ours, t_ref, err
+
+
+def test_faster_than_reference_cuda_path_small_fdk():
+    _need_ref()
+    t_ours, t_ref, err = _compare((128, 128, 128), (192, 128), 180, 500.0, 0.5, reps=3)
+    assert err < 1e-3
+    assert t_ours < t_ref
+
+
+@pytest.mark.skipif(os.environ.get("FCB_TIME_REFERENCE_LARGE") != "1",
+                    reason="the 1024^3 comparison runs with FCB_TIME_REFERENCE_LARGE=1")
+def test_faster_than_reference_cuda_path_large_fdk():
+    _need_ref()
+    t_ours, t_ref, err = _compare((1024, 1024, 1024), (1536, 1024), 1440, 2000.0, 0.8, reps=1)
+    assert err < 1e-3
+    assert t_ours < t_ref
