@@ -982,8 +982,19 @@ int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void
       if (piw) FCB_TRY((launch_fdk<float, 32, true, false>(pl, map, chunk, tz0, tz1, st)));
       else FCB_TRY((launch_fdk<float, 32, false, false>(pl, map, chunk, tz0, tz1, st)));
     } else if (pl->ptype == FCB_F32 && pl->nz_tile == 16) {
-      if (piw) FCB_TRY((launch_fdk<float, 16, true, true>(pl, map, chunk, tz0, tz1, st)));
-      else FCB_TRY((launch_fdk<float, 16, false, true>(pl, map, chunk, tz0, tz1, st)));
+      // FCB_FDK_MINB=4/5: register caps for 4 or 5 CTAs per SM (occupancy experiments)
+      const char* mb = getenv("FCB_FDK_MINB");
+      const int minb = mb ? atoi(mb) : 0;
+      if (minb == 5) {
+        if (piw) FCB_TRY((launch_fdk<float, 16, true, true, 5>(pl, map, chunk, tz0, tz1, st)));
+        else FCB_TRY((launch_fdk<float, 16, false, true, 5>(pl, map, chunk, tz0, tz1, st)));
+      } else if (minb == 4) {
+        if (piw) FCB_TRY((launch_fdk<float, 16, true, true, 4>(pl, map, chunk, tz0, tz1, st)));
+        else FCB_TRY((launch_fdk<float, 16, false, true, 4>(pl, map, chunk, tz0, tz1, st)));
+      } else {
+        if (piw) FCB_TRY((launch_fdk<float, 16, true, true>(pl, map, chunk, tz0, tz1, st)));
+        else FCB_TRY((launch_fdk<float, 16, false, true>(pl, map, chunk, tz0, tz1, st)));
+      }
     } else if (pl->ptype == FCB_F32 && pl->nz_tile == 64) {
       if (piw) FCB_TRY((launch_fdk<float, 64, true, true>(pl, map, chunk, tz0, tz1, st)));
       else FCB_TRY((launch_fdk<float, 64, false, true>(pl, map, chunk, tz0, tz1, st)));

@@ -136,3 +136,35 @@ def test_wgrad_tensor_cores_vs_torch(shape, monkeypatch):
     dw2 = nn.conv3d16_wgrad(x, gy)
     torch.cuda.synchronize()
     assert _rel(dw2, dw) < 2e-4
+
+
+def test_conv_forward_and_gradients_vs_cpu_fp64():
+    """Forward, input gradient and weight gradient of the tcgen05 kernels against torch on
+    the CPU in FP64, on the same BF16 values (the kernels accumulate in FP32: rel-L2 <= 1e-5).
+    The input gradient is the forward kernel with tap-flipped, transposed weights, as the
+    autograd function runs it."""
+    import torch
+    import torch.nn.functional as F
+
+    from fastcone_b200 import nn, ops
+
+    g = torch.Generator(device="cuda").manual_seed(11)
+    shape = (10, 12, 70)
+    x = _act(shape, g, torch.bfloat16)
+    gy = _act(shape, g, torch.bfloat16)
+    w = (torch.randn(16, 16, 3, 3, 3, device="cuda", generator=g) * 0.1).to(torch.bfloat16)
+    wk = nn.to_kernel_weights(w.float()).to(torch.bfloat16).contiguous()
+    y = nn.conv3d16(x, wk, None, relu=False, out_dtype=torch.float32)
+    gx = nn.conv3d16(gy, wk.flip(0).transpose(1, 2).contiguous(), None, relu=False, out_dtype=torch.float32)
+    dw = nn.conv3d16_wgrad(x, gy)
+    ops.sync_status()
+
+    xc = nn.from_layout(x).double().cpu().unsqueeze(0)
+    gc = nn.from_layout(gy).double().cpu().unsqueeze(0)
+    wc = w.double().cpu()
+    y_ref = F.conv3d(xc, wc, padding=1)
+    gx_ref = torch.nn.grad.conv3d_input(xc.shape, wc, gc, padding=1)
+    dw_ref = torch.nn.grad.conv3d_weight(xc, wc.shape, gc, padding=1)
+    assert _rel(nn.from_layout(y).cpu().unsqueeze(0).double(), y_ref) < 1e-5
+    assert _rel(nn.from_layout(gx).cpu().unsqueeze(0).double(), gx_ref) < 1e-5
+    assert _rel(nn.from_kernel_weights(dw).cpu().double(), dw_ref) < 1e-5
