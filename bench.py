@@ -506,6 +506,18 @@ def main():
         e1.record(st)
         torch.cuda.synchronize()
         proj_res[name] = nsamp / (e0.elapsed_time(e1) / 3 / 1e3) / 1e9
+        if meth != _lib.PROJ_TEXTURE:
+            # the matched transpose of the same plan (the autograd backward), same samples
+            av = torch.zeros_like(pv)
+            pplan.adjoint(pp, av)
+            torch.cuda.synchronize()
+            e0.record(st)
+            for _ in range(3):
+                pplan.adjoint(pp, av)
+            e1.record(st)
+            torch.cuda.synchronize()
+            proj_res[name + "_adjoint"] = nsamp / (e0.elapsed_time(e1) / 3 / 1e3) / 1e9
+            del av
         del pplan
     del pv, pp
 
