@@ -461,14 +461,16 @@ __global__ void __launch_bounds__(PB_THREADS, 1) project_brick_kernel(
 // both orientations flush coalesced.  Samples whose taps leave the brick scatter straight
 // to global memory.  Weights are those of project_adjoint_kernel; the pair with the brick
 // projector passes the dot-product test to rounding.
-__global__ void __launch_bounds__(256) project_adjoint_brick_kernel(const __grid_constant__ PjParams P,
-                                                                    float* vol, float* volT)
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) project_adjoint_brick_kernel(const __grid_constant__ PjParams P,
+                                                                          float* vol, float* volT, int vec4)
 {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float* brick = reinterpret_cast<float*>(smem_raw);
   const int nb = P.BC * PB_BD * P.BZ;
   int* range = reinterpret_cast<int*>(smem_raw + (size_t)nb * 4);
   int4* org = reinterpret_cast<int4*>(range + 4);
+  int* box = reinterpret_cast<int*>(org + 1);  // cells touched in the slab: c, d, z min / max
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int v = blockIdx.z;
   const PjView& V = P.v[v];
@@ -518,10 +520,15 @@ __global__ void __launch_bounds__(256) project_adjoint_brick_kernel(const __grid
       int c0, z0, nc, nzz;
       brick_extent(B, a, -1.0f, (float)ndom, c0, z0, nc, nzz);
       org[0] = make_int4(c0, a, z0, 0);
+      box[0] = box[2] = box[4] = INT_MAX;
+      box[1] = box[3] = box[5] = INT_MIN;
     }
     __syncthreads();
     const int4 o = org[0];
     const int alo = a, ahi = a + PB_T - 1;
+    // first and last brick cell of this ray in the slab: a straight line's cells lie in
+    // the box they span
+    int fc = INT_MAX, fd = 0, fz = 0, lc = 0, ld = 0, lz = 0;
     while (m <= m1) {
       const float mf = (float)m;
       const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
@@ -532,6 +539,14 @@ __global__ void __launch_bounds__(256) project_adjoint_brick_kernel(const __grid
       if ((unsigned)ic < (unsigned)(P.BC - 1) && (unsigned)id < (unsigned)PB_T &&
           (unsigned)iz < (unsigned)(P.BZ - 1)) {
         float* b0 = brick + ((size_t)iz * PB_BD + id) * P.BC + ic;
+        if (fc == INT_MAX) {
+          fc = ic;
+          fd = id;
+          fz = iz;
+        }
+        lc = ic;
+        ld = id;
+        lz = iz;
         const int ox = xd ? P.BC : 1, oy = xd ? 1 : P.BC, oz = P.BC * PB_BD;
 #pragma unroll
         for (int q = 0; q < 8; q++) {
@@ -549,8 +564,49 @@ __global__ void __launch_bounds__(256) project_adjoint_brick_kernel(const __grid
       }
       m++;
     }
+    if (vec4) {
+      const bool hit = fc != INT_MAX;
+      const int v[6] = {hit ? min(fc, lc) : INT_MAX, hit ? max(fc, lc) : INT_MIN,
+                        hit ? min(fd, ld) : INT_MAX, hit ? max(fd, ld) : INT_MIN,
+                        hit ? min(fz, lz) : INT_MAX, hit ? max(fz, lz) : INT_MIN};
+#pragma unroll
+      for (int q = 0; q < 6; q++) {
+        const int r = (q & 1) ? __reduce_max_sync(0xffffffffu, v[q]) : __reduce_min_sync(0xffffffffu, v[q]);
+        if (lane == 0 && ((q & 1) ? r != INT_MIN : r != INT_MAX)) {
+          if (q & 1) atomicMax(&box[q], r);
+          else atomicMin(&box[q], r);
+        }
+      }
+    }
     __syncthreads();
-    // flush: brick element (c, dd, zz) -> voxel; y-fastest buffer for x-dominant bundles
+    // flush: brick element (c, dd, zz) -> voxel; y-fastest buffer for x-dominant bundles.
+    // vec4: four cross-axis neighbours per step (16-byte shared loads and global float4
+    // atomics): the brick's cross origin and extent are multiples of 4 and so are the
+    // volume's x and y extents, so a group is wholly inside or outside the volume
+    if (vec4) {
+      // only the box of touched cells (their +1 corners included); the rest is zero
+      float4* b4 = reinterpret_cast<float4*>(brick);
+      const int cg0 = box[0] >> 2, ncg = ((box[1] + 1) >> 2) - cg0 + 1;
+      const int d0 = box[2], ndd = box[3] + 2 - box[2], z0b = box[4], nzb = box[5] + 2 - box[4];
+      const int ngr = box[0] == INT_MAX ? 0 : ncg * ndd * nzb;
+      for (int gi = threadIdx.x; gi < ngr; gi += blockDim.x) {
+        const int cg = cg0 + gi % ncg, rr = gi / ncg;
+        const int dd = d0 + rr % ndd, zz = z0b + rr / ndd;
+        const int e = (zz * PB_BD + dd) * P.BC + cg * 4;
+        const int e4 = e >> 2;
+        const float4 val = b4[e4];
+        if (val.x == 0.0f && val.y == 0.0f && val.z == 0.0f && val.w == 0.0f) continue;
+        b4[e4] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const int c = cg * 4;
+        const int gc = o.x + c, gd = a + dd, gz = o.z + zz;
+        const int X = xd ? gd : gc, Y = xd ? gc : gd;
+        if (X < 0 || Y < 0 || gz < 0 || X >= nx || Y >= ny || gz >= nz) continue;
+        if (xd) atomicAdd(reinterpret_cast<float4*>(volT + (size_t)gz * sz + (size_t)X * ny + Y), val);
+        else atomicAdd(reinterpret_cast<float4*>(vol + (size_t)gz * sz + (size_t)Y * nx + X), val);
+      }
+      __syncthreads();
+      continue;
+    }
     for (int e = threadIdx.x; e < nb; e += blockDim.x) {
       const float val = brick[e];
       if (val == 0.0f) continue;
@@ -684,16 +740,24 @@ int brick_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, const floa
 int brick_adjoint_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, float* vol, float* vt,
                          int nx, int ny, int nz, cudaStream_t st)
 {
-  const size_t smem = (size_t)bs.BC * PB_BD * bs.BZ * 4 + 16 + 16;
+  const size_t smem = (size_t)bs.BC * PB_BD * bs.BZ * 4 + 16 + 16 + 32;
   if (smem > 200 * 1024) return set_error(FCB_ERR_RANGE, "adjoint brick exceeds shared memory");
   FCB_CUDA_TRY(cudaMemsetAsync(vt, 0, (size_t)nx * ny * nz * sizeof(float), st));
-  FCB_CUDA_TRY(cudaFuncSetAttribute(project_adjoint_brick_kernel,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // 16-byte flush groups: 4 | nx, 4 | ny and both volumes 16-byte aligned (FCB_PROJ_FLUSH4=0
+  // selects the element-wise flush, for comparison)
+  const char* f4 = getenv("FCB_PROJ_FLUSH4");
+  const int vec4 = (nx % 4 == 0 && ny % 4 == 0 && (uintptr_t)vol % 16 == 0 && (uintptr_t)vt % 16 == 0 &&
+                    !(f4 && f4[0] == '0')) ? 1 : 0;
+  // registers for 5 resident CTAs (the shared-memory limit of the usual brick) unless
+  // FCB_PROJ_ADJ_MINB=4 lets the kernel keep its working set without spills
+  const char* mb = getenv("FCB_PROJ_ADJ_MINB");
+  auto kern = (mb && mb[0] == '4') ? project_adjoint_brick_kernel<4> : project_adjoint_brick_kernel<5>;
+  FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (PjParams& P : chunks) {
     P.BC = bs.BC;
     P.BZ = bs.BZ;
     dim3 grid((P.WH0 + PB_W - 1) / PB_W, (P.WH1 + PB_H - 1) / PB_H, P.nviews);
-    project_adjoint_brick_kernel<<<grid, 256, smem, st>>>(P, vol, vt);
+    kern<<<grid, 256, smem, st>>>(P, vol, vt, vec4);
     FCB_CUDA_TRY(cudaGetLastError());
   }
   dim3 tg((nx + 31) / 32, (ny + 31) / 32, nz);
