@@ -306,6 +306,34 @@ __global__ void project_brick_extent_kernel(const __grid_constant__ PjParams P, 
   }
 }
 
+// Packed FP32 pairs (sm_100 f32x2 arithmetic): two samples of one ray per instruction, each
+// lane doing exactly the scalar operation of tri_of / tri_lerp.
+typedef unsigned long long pj_u64;
+__device__ __forceinline__ pj_u64 pj_pk(float lo, float hi)
+{
+  pj_u64 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void pj_up(pj_u64 v, float& lo, float& hi)
+{
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ pj_u64 pj_sub(pj_u64 a, pj_u64 b)
+{
+  pj_u64 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ pj_u64 pj_fma(pj_u64 a, pj_u64 b, pj_u64 c)
+{
+  pj_u64 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+// lerp of both lanes: a + t (b - a), as fmaf(t, b - a, a)
+__device__ __forceinline__ pj_u64 pj_lerp(pj_u64 t, pj_u64 a, pj_u64 b) { return pj_fma(t, pj_sub(b, a), a); }
+
 __device__ __forceinline__ float lds32(uint32_t a)
 {
   float v;
@@ -342,6 +370,45 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
     const int alo = o.y, ahi = o.y + PB_T - 1;
     const uint32_t stb = sbase + (uint32_t)st * (uint32_t)P.stage_bytes;
     while (m <= m1) {
+      if (m + 1 <= m1) {
+        // samples m and m+1 in f32x2 lanes, when both are inside the slab and the brick
+        const pj_u64 mm = pj_pk((float)m, (float)(m + 1));
+        float x0, x1, y0, y1, z0, z1;
+        pj_up(pj_fma(mm, pj_pk(d[0], d[0]), pj_pk(s[0], s[0])), x0, x1);
+        pj_up(pj_fma(mm, pj_pk(d[1], d[1]), pj_pk(s[1], s[1])), y0, y1);
+        pj_up(pj_fma(mm, pj_pk(d[2], d[2]), pj_pk(s[2], s[2])), z0, z1);
+        const float fx0 = floorf(x0), fx1 = floorf(x1), fy0 = floorf(y0), fy1 = floorf(y1);
+        const float fz0 = floorf(z0), fz1 = floorf(z1);
+        const int i0 = (int)fx0, i1 = (int)fx1, j0 = (int)fy0, j1 = (int)fy1, k0 = (int)fz0, k1 = (int)fz1;
+        const int d0 = XD ? i0 : j0, d1 = XD ? i1 : j1;
+        const int c0 = (XD ? j0 : i0) - o.x, c1 = (XD ? j1 : i1) - o.x;
+        const int e0 = d0 - alo, e1 = d1 - alo, q0 = k0 - o.z, q1 = k1 - o.z;
+        if ((unsigned)c0 < (unsigned)BC1 && (unsigned)e0 < (unsigned)PB_T && (unsigned)q0 < (unsigned)BZ1 &&
+            (unsigned)c1 < (unsigned)BC1 && (unsigned)e1 < (unsigned)PB_T && (unsigned)q1 < (unsigned)BZ1) {
+          const pj_u64 ta = pj_sub(pj_pk(x0, x1), pj_pk(fx0, fx1));
+          const pj_u64 tb = pj_sub(pj_pk(y0, y1), pj_pk(fy0, fy1));
+          const pj_u64 tc = pj_sub(pj_pk(z0, z1), pj_pk(fz0, fz1));
+          const uint32_t p0 = stb + (uint32_t)q0 * planeb + (uint32_t)e0 * rowb + (uint32_t)c0 * 4u;
+          const uint32_t p1 = stb + (uint32_t)q1 * planeb + (uint32_t)e1 * rowb + (uint32_t)c1 * 4u;
+          const pj_u64 v000 = pj_pk(lds32(p0), lds32(p1));
+          const pj_u64 v100 = pj_pk(lds32(p0 + ox), lds32(p1 + ox));
+          const pj_u64 v010 = pj_pk(lds32(p0 + oy), lds32(p1 + oy));
+          const pj_u64 v110 = pj_pk(lds32(p0 + ox + oy), lds32(p1 + ox + oy));
+          const pj_u64 v001 = pj_pk(lds32(p0 + planeb), lds32(p1 + planeb));
+          const pj_u64 v101 = pj_pk(lds32(p0 + planeb + ox), lds32(p1 + planeb + ox));
+          const pj_u64 v011 = pj_pk(lds32(p0 + planeb + oy), lds32(p1 + planeb + oy));
+          const pj_u64 v111 = pj_pk(lds32(p0 + planeb + ox + oy), lds32(p1 + planeb + ox + oy));
+          const pj_u64 x00 = pj_lerp(ta, v000, v100), x10 = pj_lerp(ta, v010, v110);
+          const pj_u64 x01 = pj_lerp(ta, v001, v101), x11 = pj_lerp(ta, v011, v111);
+          const pj_u64 yy0 = pj_lerp(tb, x00, x10), yy1 = pj_lerp(tb, x01, x11);
+          float r0, r1;
+          pj_up(pj_lerp(tc, yy0, yy1), r0, r1);
+          acc += r0;
+          acc += r1;
+          m += 2;
+          continue;
+        }
+      }
       const float mf = (float)m;
       const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
       const int idom = XD ? t.i : t.j;
