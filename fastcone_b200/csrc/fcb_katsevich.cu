@@ -61,9 +61,18 @@ __device__ __forceinline__ void stv(float* __restrict__ p, const float (&v)[CPT]
   else *p = v[0];
 }
 
+// Reciprocals of the step sizes, computed once on the host: the kernel multiplies instead
+// of dividing (no per-element IEEE division).
+struct KatsDerivConst {
+  float idl, hidl;   // 1 / dlam, 1 / (2 dlam)
+  float idu, hidu;   // 1 / du, 1 / (2 du), du = su pw
+  float ipw, hipw;   // 1 / pw, 1 / (2 pw)
+  float pw, D, iD, su;
+};
+
 template <int CPT>
 __global__ void kats_deriv_kernel(const float* __restrict__ g, float* __restrict__ g2, int n, int H,
-                                  int W, float dlam, float pw, float D, float su)
+                                  int W, const KatsDerivConst K)
 {
   const int Wq = W / CPT;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -81,19 +90,18 @@ __global__ void kats_deriv_kernel(const float* __restrict__ g, float* __restrict
   } else if (t == 0) {
     ldv<CPT>(g + o + plane, a);
 #pragma unroll
-    for (int k = 0; k < CPT; k++) dl[k] = (a[k] - c[k]) / dlam;
+    for (int k = 0; k < CPT; k++) dl[k] = (a[k] - c[k]) * K.idl;
   } else if (t == n - 1) {
     ldv<CPT>(g + o - plane, b);
 #pragma unroll
-    for (int k = 0; k < CPT; k++) dl[k] = (c[k] - b[k]) / dlam;
+    for (int k = 0; k < CPT; k++) dl[k] = (c[k] - b[k]) * K.idl;
   } else {
     ldv<CPT>(g + o + plane, a);
     ldv<CPT>(g + o - plane, b);
 #pragma unroll
-    for (int k = 0; k < CPT; k++) dl[k] = (a[k] - b[k]) / (2.0f * dlam);
+    for (int k = 0; k < CPT; k++) dl[k] = (a[k] - b[k]) * K.hidl;
   }
   // dg/du with u_i = su * (i - W/2) pw; e = the row from column i0 - 1 to i0 + CPT
-  const float du = su * pw;
   float e[CPT + 2];
   e[0] = i0 > 0 ? g[o - 1] : 0.0f;
 #pragma unroll
@@ -103,9 +111,9 @@ __global__ void kats_deriv_kernel(const float* __restrict__ g, float* __restrict
   for (int k = 0; k < CPT; k++) {
     const int i = i0 + k;
     if (W == 1) dgu[k] = 0.0f;
-    else if (i == 0) dgu[k] = (e[k + 2] - e[k + 1]) / du;
-    else if (i == W - 1) dgu[k] = (e[k + 1] - e[k]) / du;
-    else dgu[k] = (e[k + 2] - e[k]) / (2.0f * du);
+    else if (i == 0) dgu[k] = (e[k + 2] - e[k + 1]) * K.idu;
+    else if (i == W - 1) dgu[k] = (e[k + 1] - e[k]) * K.idu;
+    else dgu[k] = (e[k + 2] - e[k]) * K.hidu;
   }
   if (H == 1) {
 #pragma unroll
@@ -113,23 +121,24 @@ __global__ void kats_deriv_kernel(const float* __restrict__ g, float* __restrict
   } else if (j == 0) {
     ldv<CPT>(g + o + W, a);
 #pragma unroll
-    for (int k = 0; k < CPT; k++) dgv[k] = (a[k] - c[k]) / pw;
+    for (int k = 0; k < CPT; k++) dgv[k] = (a[k] - c[k]) * K.ipw;
   } else if (j == H - 1) {
     ldv<CPT>(g + o - W, b);
 #pragma unroll
-    for (int k = 0; k < CPT; k++) dgv[k] = (c[k] - b[k]) / pw;
+    for (int k = 0; k < CPT; k++) dgv[k] = (c[k] - b[k]) * K.ipw;
   } else {
     ldv<CPT>(g + o + W, a);
     ldv<CPT>(g + o - W, b);
 #pragma unroll
-    for (int k = 0; k < CPT; k++) dgv[k] = (a[k] - b[k]) / (2.0f * pw);
+    for (int k = 0; k < CPT; k++) dgv[k] = (a[k] - b[k]) * K.hipw;
   }
-  const float v = (float)(j - H / 2) * pw;
+  const float v = (float)(j - H / 2) * K.pw;
 #pragma unroll
   for (int k = 0; k < CPT; k++) {
-    const float u = su * (float)(i0 + k - W / 2) * pw;
-    const float g1 = dl[k] + ((u * u + D * D) / D) * dgu[k] + (u * v / D) * dgv[k];
-    r[k] = g1 * (D * rsqrtf(u * u + D * D + v * v));
+    const float u = K.su * (float)(i0 + k - W / 2) * K.pw;
+    const float q2 = u * u + K.D * K.D;
+    const float g1 = dl[k] + (q2 * K.iD) * dgu[k] + (u * v * K.iD) * dgv[k];
+    r[k] = g1 * (K.D * rsqrtf(q2 + v * v));
   }
   stv<CPT>(g2 + o, r);
 }
@@ -389,11 +398,25 @@ extern "C" int fcb_katsevich_plan_execute(fcb_katsevich_plan* pl, const float* i
   const int cpt = v4 ? 4 : 1;
   const unsigned bx_hw = (unsigned)(((long long)H * (W / cpt) + 255) / 256);
   const unsigned bx_kw = (unsigned)(((long long)K * (W / cpt) + 255) / 256);
+  KatsDerivConst KC;
+  {
+    const double dl = pl->dlam, du = (double)pl->su * pl->pw, pw = pl->pw, D = pl->D;
+    KC.idl = (float)(1.0 / dl);
+    KC.hidl = (float)(0.5 / dl);
+    KC.idu = (float)(1.0 / du);
+    KC.hidu = (float)(0.5 / du);
+    KC.ipw = (float)(1.0 / pw);
+    KC.hipw = (float)(0.5 / pw);
+    KC.pw = pl->pw;
+    KC.D = pl->D;
+    KC.iD = (float)(1.0 / D);
+    KC.su = pl->su;
+  }
   if (v4) {
-    kats_deriv_kernel<4><<<dim3(bx_hw, nviews), 256, 0, st>>>(in, pl->g2, nviews, H, W, pl->dlam, pl->pw, pl->D, pl->su);
+    kats_deriv_kernel<4><<<dim3(bx_hw, nviews), 256, 0, st>>>(in, pl->g2, nviews, H, W, KC);
     kats_rebin_fwd_kernel<4><<<dim3(bx_kw, nviews), 256, 0, st>>>(pl->g2, pl->g3, pl->dfj, pl->dfa, H, W, K, L);
   } else {
-    kats_deriv_kernel<1><<<dim3(bx_hw, nviews), 256, 0, st>>>(in, pl->g2, nviews, H, W, pl->dlam, pl->pw, pl->D, pl->su);
+    kats_deriv_kernel<1><<<dim3(bx_hw, nviews), 256, 0, st>>>(in, pl->g2, nviews, H, W, KC);
     kats_rebin_fwd_kernel<1><<<dim3(bx_kw, nviews), 256, 0, st>>>(pl->g2, pl->g3, pl->dfj, pl->dfa, H, W, K, L);
   }
   auto rebin_bwd = [&](const float* rows, int t0, int nv, float scale) {

@@ -75,12 +75,14 @@ class BackprojectPlan:
         return vol
 
     def __del__(self):
-        if getattr(self, "_h", None) and self._h.value:
+        # also runs at interpreter exit, when module globals may already be gone
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._h = None
             try:
-                lib().fcb_bp_plan_destroy(self._h)
+                lib().fcb_bp_plan_destroy(h)
             except Exception:
                 pass
-            self._h = ctypes.c_void_p()
 
 
 def project(vol: torch.Tensor, geom: ConeGeometry, method: int = _lib.PROJ_EXPLICIT,
@@ -138,12 +140,14 @@ class ProjectPlan:
         return vol
 
     def __del__(self):
-        if getattr(self, "_h", None) and self._h.value:
+        # also runs at interpreter exit, when module globals may already be gone
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._h = None
             try:
-                lib().fcb_proj_plan_destroy(self._h)
+                lib().fcb_proj_plan_destroy(h)
             except Exception:
                 pass
-            self._h = ctypes.c_void_p()
 
 
 def project_adjoint(proj: torch.Tensor, geom: ConeGeometry, vol: torch.Tensor | None = None) -> torch.Tensor:
@@ -206,12 +210,14 @@ class FilterPlan:
         return out
 
     def __del__(self):
-        if getattr(self, "_h", None) and self._h.value:
+        # also runs at interpreter exit, when module globals may already be gone
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._h = None
             try:
-                lib().fcb_filter_plan_destroy(self._h)
+                lib().fcb_filter_plan_destroy(h)
             except Exception:
                 pass
-            self._h = ctypes.c_void_p()
 
 
 def katsevich_filter(proj: torch.Tensor, geom: ConeGeometry, n_kappa: int = 0,
@@ -252,12 +258,14 @@ class KatsevichPlan:
         return out
 
     def __del__(self):
-        if getattr(self, "_h", None) and self._h.value:
+        # also runs at interpreter exit, when module globals may already be gone
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._h = None
             try:
-                lib().fcb_katsevich_plan_destroy(self._h)
+                lib().fcb_katsevich_plan_destroy(h)
             except Exception:
                 pass
-            self._h = ctypes.c_void_p()
 
 
 def katsevich_reconstruct(proj: torch.Tensor, geom: ConeGeometry, n_kappa: int = 0,
