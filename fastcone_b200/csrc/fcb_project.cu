@@ -201,8 +201,9 @@ __global__ void __launch_bounds__(256) project_explicit_kernel(const __grid_cons
 // Explicit FP32 trilinear sampling from volume bricks staged in shared memory by TMA.
 // A CTA owns a bundle of 32 x 8 rays (detector pixels) of one view.  Its rays share the
 // source, so the bundle is a thin frustum; the CTA walks it along the dominant axis of its
-// central ray (x or y) in slabs of PB_T planes, and a producer warp stages, per slab, the
-// brick of voxels the frustum can touch there -- PB_T + 1 dominant planes x BC cross
+// central ray (x or y) in slabs of T planes (12, or 8 where the brick would otherwise keep
+// occupancy low), and a producer warp stages, per slab, the
+// brick of voxels the frustum can touch there -- T + 1 dominant planes x BC cross
 // voxels x BZ z-planes -- with one 3-D TMA load (zero fill outside the volume) into a ring
 // of `stages` buffers.  Eight consumer warps (one detector row each, lanes along the row)
 // then take every sample of their ray inside the slab from shared memory.  For x-dominant
@@ -217,8 +218,6 @@ __global__ void __launch_bounds__(256) project_explicit_kernel(const __grid_cons
 constexpr int PB_W = 32, PB_H = 8;              // rays per CTA: 32 pixels x 8 rows
 constexpr int PB_CWARPS = PB_H;                 // one consumer warp per detector row
 constexpr int PB_THREADS = (PB_CWARPS + 1) * 32;
-constexpr int PB_T = 12;                        // dominant planes per slab
-constexpr int PB_BD = PB_T + 1;                 // dominant planes per brick
 
 struct Bundle {
   float s[3];     // source (local voxel-index coordinates)
@@ -245,9 +244,10 @@ __device__ __forceinline__ void bundle_of(const PjView& V, int bw0, int bh0, Bun
   B.sgn = (B.xdom ? c[0] : c[1]) > 0.0f ? 1 : -1;
 }
 
-// Brick of the slab whose samples have floor(dominant) in [a, a + PB_T - 1]: the frustum's
-// cross / z range between the dominant planes a and a + PB_T (clipped to [lo, hi]), plus
+// Brick of the slab whose samples have floor(dominant) in [a, a + T - 1]: the frustum's
+// cross / z range between the dominant planes a and a + T (clipped to [lo, hi]), plus
 // the +1 trilinear neighbour; the cross origin is aligned down to 4 voxels (16-byte TMA rule).
+template <int T>
 __device__ __forceinline__ void brick_extent(const Bundle& B, int a, float lo, float hi, int& c0,
                                              int& z0, int& needc, int& needz)
 {
@@ -255,7 +255,7 @@ __device__ __forceinline__ void brick_extent(const Bundle& B, int a, float lo, f
   const bool xd = B.xdom != 0;
   const float sD = xd ? B.s[0] : B.s[1], sC = xd ? B.s[1] : B.s[0];
   float cmin = 3.0e38f, cmax = -3.0e38f, zmin = 3.0e38f, zmax = -3.0e38f;
-  const float p0 = fmaxf((float)a, lo), p1 = fminf((float)(a + PB_T), hi);
+  const float p0 = fmaxf((float)a, lo), p1 = fminf((float)(a + T), hi);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const float dD = xd ? B.d[q][0] : B.d[q][1], dC = xd ? B.d[q][1] : B.d[q][0];
@@ -277,6 +277,7 @@ __device__ __forceinline__ void brick_extent(const Bundle& B, int a, float lo, f
 }
 
 // Pre-pass: the largest brick over every (view, bundle, slab start) sizes the staged box.
+template <int T>
 __global__ void project_brick_extent_kernel(const __grid_constant__ PjParams P, int bx, int by,
                                             int* out)
 {
@@ -289,9 +290,9 @@ __global__ void project_brick_extent_kernel(const __grid_constant__ PjParams P, 
     Bundle B;
     bundle_of(P.v[v], (b % bx) * PB_W, (b / bx) * PB_H, B);
     const int ndom = B.xdom ? P.nx : P.ny;
-    for (int a = -PB_T; a <= ndom; a++) {
+    for (int a = -T; a <= ndom; a++) {
       int c0, z0, nc, nz;
-      brick_extent(B, a, -1.0f, (float)ndom, c0, z0, nc, nz);
+      brick_extent<T>(B, a, -1.0f, (float)ndom, c0, z0, nc, nz);
       mc = max(mc, nc);
       mz = max(mz, nz);
     }
@@ -346,7 +347,7 @@ __device__ __forceinline__ float lds32(uint32_t a)
 // contiguous axis is y, its middle axis x).  Returns the ray sum; a timed-out wait records
 // the status and returns what was summed (the caller's store then carries a partial sum
 // that the status flags).
-template <bool XD>
+template <bool XD, int T>
 __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char* smem_raw,
                                                uint64_t* full, uint64_t* empty, const int4* origin,
                                                int nsl, int sgn, const float s[3], const float d[3],
@@ -354,7 +355,7 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
 {
   const int lane = threadIdx.x & 31;
   const uint32_t sbase = dev::smem_u32(smem_raw);
-  const uint32_t rowb = (uint32_t)P.BC * 4u, planeb = rowb * (uint32_t)PB_BD;
+  const uint32_t rowb = (uint32_t)P.BC * 4u, planeb = rowb * (uint32_t)(T + 1);
   const uint32_t ox = XD ? rowb : 4u, oy = XD ? 4u : rowb;
   const int BC1 = P.BC - 1, BZ1 = P.BZ - 1;
   float acc = 0.0f;
@@ -367,7 +368,7 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
       return acc;
     }
     const int4 o = origin[st];
-    const int alo = o.y, ahi = o.y + PB_T - 1;
+    const int alo = o.y, ahi = o.y + T - 1;
     const uint32_t stb = sbase + (uint32_t)st * (uint32_t)P.stage_bytes;
     while (m <= m1) {
       if (m + 1 <= m1) {
@@ -383,8 +384,8 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
         const int d0 = XD ? i0 : j0, d1 = XD ? i1 : j1;
         const int c0 = (XD ? j0 : i0) - o.x, c1 = (XD ? j1 : i1) - o.x;
         const int e0 = d0 - alo, e1 = d1 - alo, q0 = k0 - o.z, q1 = k1 - o.z;
-        if ((unsigned)c0 < (unsigned)BC1 && (unsigned)e0 < (unsigned)PB_T && (unsigned)q0 < (unsigned)BZ1 &&
-            (unsigned)c1 < (unsigned)BC1 && (unsigned)e1 < (unsigned)PB_T && (unsigned)q1 < (unsigned)BZ1) {
+        if ((unsigned)c0 < (unsigned)BC1 && (unsigned)e0 < (unsigned)T && (unsigned)q0 < (unsigned)BZ1 &&
+            (unsigned)c1 < (unsigned)BC1 && (unsigned)e1 < (unsigned)T && (unsigned)q1 < (unsigned)BZ1) {
           const pj_u64 ta = pj_sub(pj_pk(x0, x1), pj_pk(fx0, fx1));
           const pj_u64 tb = pj_sub(pj_pk(y0, y1), pj_pk(fy0, fy1));
           const pj_u64 tc = pj_sub(pj_pk(z0, z1), pj_pk(fz0, fz1));
@@ -415,7 +416,7 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
       if (sgn > 0 ? idom > ahi : idom < alo) break;
       const int ic = (XD ? t.j : t.i) - o.x, id = idom - alo, iz = t.k - o.z;
       float val;
-      if ((unsigned)ic < (unsigned)BC1 && (unsigned)id < (unsigned)PB_T && (unsigned)iz < (unsigned)BZ1) {
+      if ((unsigned)ic < (unsigned)BC1 && (unsigned)id < (unsigned)T && (unsigned)iz < (unsigned)BZ1) {
         // taps outside the volume are the brick's zero fill
         const uint32_t p = stb + (uint32_t)iz * planeb + (uint32_t)id * rowb + (uint32_t)ic * 4u;
         val = tri_lerp(t, lds32(p), lds32(p + ox), lds32(p + oy), lds32(p + ox + oy), lds32(p + planeb),
@@ -432,7 +433,7 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
   return acc;
 }
 
-template <int MINB>
+template <int MINB, int T>
 __global__ void __launch_bounds__(PB_THREADS, MINB) project_brick_kernel(
     const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmT,
     const __grid_constant__ PjParams P)
@@ -482,14 +483,14 @@ __global__ void __launch_bounds__(PB_THREADS, MINB) project_brick_kernel(
   }
   __syncthreads();
   const int fmin = range[0], fmax = range[1];
-  const int nsl = fmax >= fmin ? (fmax - fmin) / PB_T + 1 : 0;
+  const int nsl = fmax >= fmin ? (fmax - fmin) / T + 1 : 0;
 
   if (warp == PB_CWARPS) {
     // ------------------------------------------------------------- producer warp
     if (lane != 0) return;
     const CUtensorMap* tm = B.xdom ? &tmT : &tmV;
     dev::tma_prefetch(tm);
-    const uint32_t bytes = (uint32_t)(P.BC * PB_BD * P.BZ * 4);
+    const uint32_t bytes = (uint32_t)(P.BC * (T + 1) * P.BZ * 4);
     int issued = 0;
     bool failed = false;
     for (int k = 0; k < nsl; k++) {
@@ -498,9 +499,9 @@ __global__ void __launch_bounds__(PB_THREADS, MINB) project_brick_kernel(
         failed = true;
         break;
       }
-      const int a = B.sgn > 0 ? fmin + k * PB_T : fmax - PB_T + 1 - k * PB_T;
+      const int a = B.sgn > 0 ? fmin + k * T : fmax - T + 1 - k * T;
       int c0, z0, nc, nz;
-      brick_extent(B, a, -1.0f, (float)ndom, c0, z0, nc, nz);
+      brick_extent<T>(B, a, -1.0f, (float)ndom, c0, z0, nc, nz);
       origin[st] = make_int4(c0, a, z0, 0);
       dev::mbar_arrive_expect_tx(&full[st], bytes);
       dev::tma_load_3d(smem_raw + (size_t)st * P.stage_bytes, tm, &full[st], c0, a, z0);
@@ -515,8 +516,8 @@ __global__ void __launch_bounds__(PB_THREADS, MINB) project_brick_kernel(
   }
 
   // --------------------------------------------------------------- consumer warps
-  const float acc = xd ? brick_consume<true>(P, smem_raw, full, empty, origin, nsl, B.sgn, s, d, m0, m1)
-                       : brick_consume<false>(P, smem_raw, full, empty, origin, nsl, B.sgn, s, d, m0, m1);
+  const float acc = xd ? brick_consume<true, T>(P, smem_raw, full, empty, origin, nsl, B.sgn, s, d, m0, m1)
+                       : brick_consume<false, T>(P, smem_raw, full, empty, origin, nsl, B.sgn, s, d, m0, m1);
   if (pix) P.proj[((size_t)(P.view0 + v) * P.WH1 + hl) * P.WH0 + wl] += V.wt * acc;
   count_samples(P.samples, m1 - m0 + 1);
 }
@@ -529,13 +530,13 @@ __global__ void __launch_bounds__(PB_THREADS, MINB) project_brick_kernel(
 // both orientations flush coalesced.  Samples whose taps leave the brick scatter straight
 // to global memory.  Weights are those of project_adjoint_kernel; the pair with the brick
 // projector passes the dot-product test to rounding.
-template <int MINB>
+template <int MINB, int T>
 __global__ void __launch_bounds__(256, MINB) project_adjoint_brick_kernel(const __grid_constant__ PjParams P,
                                                                           float* vol, float* volT, int vec4)
 {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   float* brick = reinterpret_cast<float*>(smem_raw);
-  const int nb = P.BC * PB_BD * P.BZ;
+  const int nb = P.BC * (T + 1) * P.BZ;
   int* range = reinterpret_cast<int*>(smem_raw + (size_t)nb * 4);
   int4* org = reinterpret_cast<int4*>(range + 4);
   int* box = reinterpret_cast<int*>(org + 1);  // cells touched in the slab: c, d, z min / max
@@ -579,21 +580,21 @@ __global__ void __launch_bounds__(256, MINB) project_adjoint_brick_kernel(const 
   }
   __syncthreads();
   const int fmin = range[0], fmax = range[1];
-  const int nsl = fmax >= fmin ? (fmax - fmin) / PB_T + 1 : 0;
+  const int nsl = fmax >= fmin ? (fmax - fmin) / T + 1 : 0;
   const size_t sy = nx, sz = (size_t)nx * ny;
   int m = m0;
   for (int k = 0; k < nsl; k++) {
-    const int a = B.sgn > 0 ? fmin + k * PB_T : fmax - PB_T + 1 - k * PB_T;
+    const int a = B.sgn > 0 ? fmin + k * T : fmax - T + 1 - k * T;
     if (threadIdx.x == 0) {
       int c0, z0, nc, nzz;
-      brick_extent(B, a, -1.0f, (float)ndom, c0, z0, nc, nzz);
+      brick_extent<T>(B, a, -1.0f, (float)ndom, c0, z0, nc, nzz);
       org[0] = make_int4(c0, a, z0, 0);
       box[0] = box[2] = box[4] = INT_MAX;
       box[1] = box[3] = box[5] = INT_MIN;
     }
     __syncthreads();
     const int4 o = org[0];
-    const int alo = a, ahi = a + PB_T - 1;
+    const int alo = a, ahi = a + T - 1;
     // first and last brick cell of this ray in the slab: a straight line's cells lie in
     // the box they span
     int fc = INT_MAX, fd = 0, fz = 0, lc = 0, ld = 0, lz = 0;
@@ -604,9 +605,9 @@ __global__ void __launch_bounds__(256, MINB) project_adjoint_brick_kernel(const 
       if (B.sgn > 0 ? idom > ahi : idom < alo) break;
       const int ic = (xd ? t.j : t.i) - o.x, id = idom - alo, iz = t.k - o.z;
       const float ab[2] = {1.0f - t.a, t.a}, bb[2] = {1.0f - t.b, t.b}, cb[2] = {1.0f - t.c, t.c};
-      if ((unsigned)ic < (unsigned)(P.BC - 1) && (unsigned)id < (unsigned)PB_T &&
+      if ((unsigned)ic < (unsigned)(P.BC - 1) && (unsigned)id < (unsigned)T &&
           (unsigned)iz < (unsigned)(P.BZ - 1)) {
-        float* b0 = brick + ((size_t)iz * PB_BD + id) * P.BC + ic;
+        float* b0 = brick + ((size_t)iz * (T + 1) + id) * P.BC + ic;
         if (fc == INT_MAX) {
           fc = ic;
           fd = id;
@@ -615,7 +616,7 @@ __global__ void __launch_bounds__(256, MINB) project_adjoint_brick_kernel(const 
         lc = ic;
         ld = id;
         lz = iz;
-        const int ox = xd ? P.BC : 1, oy = xd ? 1 : P.BC, oz = P.BC * PB_BD;
+        const int ox = xd ? P.BC : 1, oy = xd ? 1 : P.BC, oz = P.BC * (T + 1);
 #pragma unroll
         for (int q = 0; q < 8; q++) {
           const float w = ab[q & 1] * bb[(q >> 1) & 1] * cb[(q >> 2) & 1];
@@ -660,7 +661,7 @@ __global__ void __launch_bounds__(256, MINB) project_adjoint_brick_kernel(const 
       for (int gi = threadIdx.x; gi < ngr; gi += blockDim.x) {
         const int cg = cg0 + gi % ncg, rr = gi / ncg;
         const int dd = d0 + rr % ndd, zz = z0b + rr / ndd;
-        const int e = (zz * PB_BD + dd) * P.BC + cg * 4;
+        const int e = (zz * (T + 1) + dd) * P.BC + cg * 4;
         const int e4 = e >> 2;
         const float4 val = b4[e4];
         if (val.x == 0.0f && val.y == 0.0f && val.z == 0.0f && val.w == 0.0f) continue;
@@ -680,7 +681,7 @@ __global__ void __launch_bounds__(256, MINB) project_adjoint_brick_kernel(const 
       if (val == 0.0f) continue;
       brick[e] = 0.0f;
       const int c = e % P.BC, r = e / P.BC;
-      const int dd = r % PB_BD, zz = r / PB_BD;
+      const int dd = r % (T + 1), zz = r / (T + 1);
       const int gc = o.x + c, gd = a + dd, gz = o.z + zz;
       const int X = xd ? gd : gc, Y = xd ? gc : gd;
       if (X < 0 || Y < 0 || gz < 0 || X >= nx || Y >= ny || gz >= nz) continue;
@@ -734,6 +735,7 @@ struct BrickSetup {
   bool ok = false;
   int BC = 0, BZ = 0, stages = 0, stage_bytes = 0;
   int minb = 1;  // resident CTAs per SM the kernel's registers are capped for (1 or 3)
+  int T = 12;    // dominant planes per slab (8 or 12)
   size_t smem = 0;
 };
 
@@ -746,43 +748,58 @@ int brick_setup(const std::vector<PjParams>& chunks, int nx, int ny, cudaStream_
   int* scratch = nullptr;
   FCB_TRY(device_status_ptr(&scratch));
   int* need = scratch + 3;  // [3..4]: brick extents ([1..2] belong to the backprojector)
-  FCB_CUDA_TRY(cudaMemsetAsync(need, 0, 2 * sizeof(int), st));
-  for (const PjParams& P : chunks) {
-    const int bx = (P.WH0 + PB_W - 1) / PB_W, by = (P.WH1 + PB_H - 1) / PB_H;
-    const long long total = (long long)P.nviews * bx * by;
-    project_brick_extent_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(P, bx, by, need);
-    FCB_CUDA_TRY(cudaGetLastError());
+  // Slab depth: 12 dominant planes where three CTAs with two brick buffers fit in an SM's
+  // shared memory, else 8 (a brick about a third smaller; on the 256^3 / 360-view geometry
+  // two CTAs fit instead of one: 21.3 ms per pass instead of 29.8).  FCB_PROJ_SLAB=8|12
+  // fixes it.
+  const char* se = getenv("FCB_PROJ_SLAB");
+  const int forced = se ? atoi(se) : 0;
+  for (int T : {12, 8}) {
+    if (forced && forced != T) continue;
+    FCB_CUDA_TRY(cudaMemsetAsync(need, 0, 2 * sizeof(int), st));
+    for (const PjParams& P : chunks) {
+      const int bx = (P.WH0 + PB_W - 1) / PB_W, by = (P.WH1 + PB_H - 1) / PB_H;
+      const long long total = (long long)P.nviews * bx * by;
+      const unsigned g = (unsigned)((total + 255) / 256);
+      if (T == 12) project_brick_extent_kernel<12><<<g, 256, 0, st>>>(P, bx, by, need);
+      else project_brick_extent_kernel<8><<<g, 256, 0, st>>>(P, bx, by, need);
+      FCB_CUDA_TRY(cudaGetLastError());
+    }
+    int h[2] = {0, 0};
+    FCB_CUDA_TRY(cudaMemcpyAsync(h, need, sizeof h, cudaMemcpyDeviceToHost, st));
+    FCB_CUDA_TRY(cudaStreamSynchronize(st));
+    const int BC = std::max(4, (h[0] + 3) & ~3), BZ = std::max(2, h[1]);
+    if (BC > 128 || BZ > 64) continue;  // a wide cone: bricks would not pay
+    const int box = BC * (T + 1) * BZ * 4;
+    const int stage_bytes = (box + 127) & ~127;
+    auto smem_of = [&](int n) {
+      return (size_t)n * stage_bytes + n * (2 * sizeof(uint64_t) + sizeof(int4)) + 16;
+    };
+    // Two buffers and registers capped for three resident CTAs where three such CTAs fit
+    // (512^3 / 90 views: 41.6 ms against 47.1 ms with three buffers and two CTAs);
+    // otherwise up to four buffers in 96 KB.
+    const bool three = 3 * (smem_of(2) + 1024) <= 228 * 1024;
+    if (T == 12 && !three && !forced) continue;  // try the shallower slab
+    int stages = std::max(2, std::min(4, (96 * 1024) / stage_bytes)), minb = 1;
+    if (three) {
+      stages = 2;
+      minb = 3;
+    }
+    // tuning knobs: FCB_PROJ_STAGES=2..6 buffers, FCB_PROJ_MINB=1|3 register cap
+    if (const char* e = getenv("FCB_PROJ_STAGES")) stages = std::max(2, std::min(6, atoi(e)));
+    if (const char* e = getenv("FCB_PROJ_MINB")) minb = e[0] == '3' ? 3 : 1;
+    const size_t smem = smem_of(stages);
+    if (smem > 200 * 1024) continue;
+    bs->ok = true;
+    bs->T = T;
+    bs->BC = BC;
+    bs->BZ = BZ;
+    bs->stages = stages;
+    bs->minb = minb;
+    bs->stage_bytes = stage_bytes;
+    bs->smem = smem;
+    return FCB_OK;
   }
-  int h[2] = {0, 0};
-  FCB_CUDA_TRY(cudaMemcpyAsync(h, need, sizeof h, cudaMemcpyDeviceToHost, st));
-  FCB_CUDA_TRY(cudaStreamSynchronize(st));
-  const int BC = std::max(4, (h[0] + 3) & ~3), BZ = std::max(2, h[1]);
-  if (BC > 128 || BZ > 64) return FCB_OK;  // a wide cone: bricks would not pay
-  const int box = BC * PB_BD * BZ * 4;
-  const int stage_bytes = (box + 127) & ~127;
-  auto smem_of = [&](int st) {
-    return (size_t)st * stage_bytes + st * (2 * sizeof(uint64_t) + sizeof(int4)) + 16;
-  };
-  // Two buffers and registers capped for three resident CTAs where three such CTAs fit in an
-  // SM's shared memory (measured at 512^3 / 90 views: 41.6 ms against 47.1 ms with three
-  // buffers and two CTAs); otherwise up to four buffers in 96 KB.
-  int stages = std::max(2, std::min(4, (96 * 1024) / stage_bytes)), minb = 1;
-  if (3 * (smem_of(2) + 1024) <= 228 * 1024) {
-    stages = 2;
-    minb = 3;
-  }
-  // tuning knobs: FCB_PROJ_STAGES=2..6 buffers, FCB_PROJ_MINB=1|3 register cap
-  if (const char* e = getenv("FCB_PROJ_STAGES")) stages = std::max(2, std::min(6, atoi(e)));
-  if (const char* e = getenv("FCB_PROJ_MINB")) minb = e[0] == '3' ? 3 : 1;
-  const size_t smem = smem_of(stages);
-  if (smem > 200 * 1024) return FCB_OK;
-  bs->ok = true;
-  bs->BC = BC;
-  bs->BZ = BZ;
-  bs->stages = stages;
-  bs->minb = minb;
-  bs->stage_bytes = stage_bytes;
-  bs->smem = smem;
   return FCB_OK;
 }
 
@@ -797,12 +814,13 @@ int brick_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, const floa
   FCB_CUDA_TRY(cudaGetLastError());
   CUtensorMap mv, mt;
   FCB_TRY(encode_tmap_3d(&mv, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, const_cast<float*>(vol), nx, ny, nz,
-                         (uint64_t)nx * 4, (uint64_t)nx * ny * 4, bs.BC, PB_BD, bs.BZ));
+                         (uint64_t)nx * 4, (uint64_t)nx * ny * 4, bs.BC, bs.T + 1, bs.BZ));
   FCB_TRY(encode_tmap_3d(&mt, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, vt, ny, nx, nz, (uint64_t)ny * 4,
-                         (uint64_t)nx * ny * 4, bs.BC, PB_BD, bs.BZ));
+                         (uint64_t)nx * ny * 4, bs.BC, bs.T + 1, bs.BZ));
   int* status = nullptr;
   FCB_TRY(device_status_ptr(&status));
-  auto pkern = bs.minb == 3 ? project_brick_kernel<3> : project_brick_kernel<1>;
+  auto pkern = bs.T == 12 ? (bs.minb == 3 ? project_brick_kernel<3, 12> : project_brick_kernel<1, 12>)
+                          : (bs.minb == 3 ? project_brick_kernel<3, 8> : project_brick_kernel<1, 8>);
   FCB_CUDA_TRY(cudaFuncSetAttribute(pkern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)bs.smem));
   for (PjParams& P : chunks) {
@@ -822,7 +840,7 @@ int brick_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, const floa
 int brick_adjoint_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, float* vol, float* vt,
                          int nx, int ny, int nz, cudaStream_t st)
 {
-  const size_t smem = (size_t)bs.BC * PB_BD * bs.BZ * 4 + 16 + 16 + 32;
+  const size_t smem = (size_t)bs.BC * (bs.T + 1) * bs.BZ * 4 + 16 + 16 + 32;
   if (smem > 200 * 1024) return set_error(FCB_ERR_RANGE, "adjoint brick exceeds shared memory");
   FCB_CUDA_TRY(cudaMemsetAsync(vt, 0, (size_t)nx * ny * nz * sizeof(float), st));
   // 16-byte flush groups: 4 | nx, 4 | ny and both volumes 16-byte aligned (FCB_PROJ_FLUSH4=0
@@ -833,7 +851,9 @@ int brick_adjoint_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, fl
   // registers for 5 resident CTAs (the shared-memory limit of the usual brick) unless
   // FCB_PROJ_ADJ_MINB=4 lets the kernel keep its working set without spills
   const char* mb = getenv("FCB_PROJ_ADJ_MINB");
-  auto kern = (mb && mb[0] == '4') ? project_adjoint_brick_kernel<4> : project_adjoint_brick_kernel<5>;
+  const bool m4 = mb && mb[0] == '4';
+  auto kern = bs.T == 12 ? (m4 ? project_adjoint_brick_kernel<4, 12> : project_adjoint_brick_kernel<5, 12>)
+                         : (m4 ? project_adjoint_brick_kernel<4, 8> : project_adjoint_brick_kernel<5, 8>);
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (PjParams& P : chunks) {
     P.BC = bs.BC;
