@@ -741,20 +741,24 @@ struct BrickSetup {
 
 // Sizes the bricks for the views of `chunks` (pre-pass on `st`, synchronises `st`).
 // ok == false when the volume rows are not 16-byte multiples or the bricks do not fit.
-int brick_setup(const std::vector<PjParams>& chunks, int nx, int ny, cudaStream_t st, BrickSetup* bs)
+int brick_setup(const std::vector<PjParams>& chunks, int nx, int ny, cudaStream_t st, BrickSetup* bs,
+                bool for_adjoint = false)
 {
   bs->ok = false;
   if (nx % 4 != 0 || ny % 4 != 0 || getenv("FCB_PROJ_NOBRICK")) return FCB_OK;
   int* scratch = nullptr;
   FCB_TRY(device_status_ptr(&scratch));
   int* need = scratch + 3;  // [3..4]: brick extents ([1..2] belong to the backprojector)
-  // Slab depth: 12 dominant planes where three CTAs with two brick buffers fit in an SM's
-  // shared memory, else 8 (a brick about a third smaller; on the 256^3 / 360-view geometry
-  // two CTAs fit instead of one: 21.3 ms per pass instead of 29.8).  FCB_PROJ_SLAB=8|12
-  // fixes it.
+  // Slab depth, forward: the deepest of 12, 8 and 6 dominant planes with which three CTAs of
+  // two brick buffers fit in an SM's shared memory, else 6 (on the 256^3 / 360-view
+  // geometry 6 planes give three CTAs instead of one: 19.9 ms per pass instead of 29.7).
+  // The transpose holds one brick and flushes it per slab; 8 planes suit it on both
+  // measured geometries.  FCB_PROJ_SLAB=6|8|12 fixes the depth.
   const char* se = getenv("FCB_PROJ_SLAB");
   const int forced = se ? atoi(se) : 0;
-  for (int T : {12, 8}) {
+  const int order_fwd[3] = {12, 8, 6}, order_adj[3] = {8, 6, 6};
+  for (int oi = 0; oi < 3; oi++) {
+    const int T = for_adjoint ? order_adj[oi] : order_fwd[oi];
     if (forced && forced != T) continue;
     FCB_CUDA_TRY(cudaMemsetAsync(need, 0, 2 * sizeof(int), st));
     for (const PjParams& P : chunks) {
@@ -762,7 +766,8 @@ int brick_setup(const std::vector<PjParams>& chunks, int nx, int ny, cudaStream_
       const long long total = (long long)P.nviews * bx * by;
       const unsigned g = (unsigned)((total + 255) / 256);
       if (T == 12) project_brick_extent_kernel<12><<<g, 256, 0, st>>>(P, bx, by, need);
-      else project_brick_extent_kernel<8><<<g, 256, 0, st>>>(P, bx, by, need);
+      else if (T == 8) project_brick_extent_kernel<8><<<g, 256, 0, st>>>(P, bx, by, need);
+      else project_brick_extent_kernel<6><<<g, 256, 0, st>>>(P, bx, by, need);
       FCB_CUDA_TRY(cudaGetLastError());
     }
     int h[2] = {0, 0};
@@ -771,6 +776,14 @@ int brick_setup(const std::vector<PjParams>& chunks, int nx, int ny, cudaStream_
     const int BC = std::max(4, (h[0] + 3) & ~3), BZ = std::max(2, h[1]);
     if (BC > 128 || BZ > 64) continue;  // a wide cone: bricks would not pay
     const int box = BC * (T + 1) * BZ * 4;
+    if (for_adjoint) {
+      if ((size_t)box + 80 > 200 * 1024) continue;
+      bs->ok = true;
+      bs->T = T;
+      bs->BC = BC;
+      bs->BZ = BZ;
+      return FCB_OK;
+    }
     const int stage_bytes = (box + 127) & ~127;
     auto smem_of = [&](int n) {
       return (size_t)n * stage_bytes + n * (2 * sizeof(uint64_t) + sizeof(int4)) + 16;
@@ -779,7 +792,7 @@ int brick_setup(const std::vector<PjParams>& chunks, int nx, int ny, cudaStream_
     // (512^3 / 90 views: 41.6 ms against 47.1 ms with three buffers and two CTAs);
     // otherwise up to four buffers in 96 KB.
     const bool three = 3 * (smem_of(2) + 1024) <= 228 * 1024;
-    if (T == 12 && !three && !forced) continue;  // try the shallower slab
+    if (oi < 2 && !three && !forced) continue;  // try a shallower slab
     int stages = std::max(2, std::min(4, (96 * 1024) / stage_bytes)), minb = 1;
     if (three) {
       stages = 2;
@@ -819,8 +832,9 @@ int brick_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, const floa
                          (uint64_t)nx * ny * 4, bs.BC, bs.T + 1, bs.BZ));
   int* status = nullptr;
   FCB_TRY(device_status_ptr(&status));
-  auto pkern = bs.T == 12 ? (bs.minb == 3 ? project_brick_kernel<3, 12> : project_brick_kernel<1, 12>)
-                          : (bs.minb == 3 ? project_brick_kernel<3, 8> : project_brick_kernel<1, 8>);
+  auto pkern = bs.T == 12  ? (bs.minb == 3 ? project_brick_kernel<3, 12> : project_brick_kernel<1, 12>)
+               : bs.T == 8 ? (bs.minb == 3 ? project_brick_kernel<3, 8> : project_brick_kernel<1, 8>)
+                           : (bs.minb == 3 ? project_brick_kernel<3, 6> : project_brick_kernel<1, 6>);
   FCB_CUDA_TRY(cudaFuncSetAttribute(pkern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)bs.smem));
   for (PjParams& P : chunks) {
@@ -852,8 +866,9 @@ int brick_adjoint_launch(std::vector<PjParams>& chunks, const BrickSetup& bs, fl
   // FCB_PROJ_ADJ_MINB=4 lets the kernel keep its working set without spills
   const char* mb = getenv("FCB_PROJ_ADJ_MINB");
   const bool m4 = mb && mb[0] == '4';
-  auto kern = bs.T == 12 ? (m4 ? project_adjoint_brick_kernel<4, 12> : project_adjoint_brick_kernel<5, 12>)
-                         : (m4 ? project_adjoint_brick_kernel<4, 8> : project_adjoint_brick_kernel<5, 8>);
+  auto kern = bs.T == 12  ? (m4 ? project_adjoint_brick_kernel<4, 12> : project_adjoint_brick_kernel<5, 12>)
+              : bs.T == 8 ? (m4 ? project_adjoint_brick_kernel<4, 8> : project_adjoint_brick_kernel<5, 8>)
+                          : (m4 ? project_adjoint_brick_kernel<4, 6> : project_adjoint_brick_kernel<5, 6>);
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (PjParams& P : chunks) {
     P.BC = bs.BC;
@@ -1057,7 +1072,7 @@ int project_launch(const Problem& pb, int method, const float* vol, float* proj,
   int rc = FCB_OK;
   if (method == FCB_PROJ_EXPLICIT && !compat) {
     BrickSetup bs;
-    FCB_TRY(brick_setup(chunks, nx, ny, st, &bs));
+    FCB_TRY(brick_setup(chunks, nx, ny, st, &bs, adj_vol != nullptr));
     if (bs.ok) {
       float* vt = nullptr;
       FCB_CUDA_TRY(cudaMallocAsync((void**)&vt, (size_t)nx * ny * nz * sizeof(float), st));
@@ -1101,6 +1116,7 @@ struct fcb_proj_plan {
   cudaTextureObject_t tex = 0;
   std::vector<PjParams> chunks;
   BrickSetup bricks;     // explicit method: staged-brick projector, when it applies
+  BrickSetup bricks_adj; // and its transpose's bricks (their own slab depth)
   float* vt = nullptr;   // its y-fastest volume copy
 };
 
@@ -1156,7 +1172,8 @@ extern "C" int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_
   }
   if (method == FCB_PROJ_EXPLICIT) {
     rc = brick_setup(pl->chunks, pl->nx, pl->ny, 0, &pl->bricks);
-    if (rc == FCB_OK && pl->bricks.ok &&
+    if (rc == FCB_OK) rc = brick_setup(pl->chunks, pl->nx, pl->ny, 0, &pl->bricks_adj, true);
+    if (rc == FCB_OK && (pl->bricks.ok || pl->bricks_adj.ok) &&
         cudaMalloc((void**)&pl->vt, (size_t)pl->nx * pl->ny * pl->nz * sizeof(float)) != cudaSuccess) {
       cudaGetLastError();
       rc = set_error(FCB_ERR_NOMEM, "device allocation of the brick projector's volume copy failed");
@@ -1178,13 +1195,13 @@ extern "C" int fcb_proj_plan_execute(fcb_proj_plan* pl, const float* volume, flo
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (adjoint && pl->method == FCB_PROJ_TEXTURE)
     return set_error(FCB_ERR_INVALID, "the adjoint belongs to the explicit projector");
-  if (pl->bricks.ok) {
+  if (adjoint ? pl->bricks_adj.ok : pl->bricks.ok) {
     for (PjParams& P : pl->chunks) {
       P.vol = volume;
       P.proj = proj;
     }
     if (adjoint)
-      FCB_TRY(brick_adjoint_launch(pl->chunks, pl->bricks, const_cast<float*>(volume), pl->vt, pl->nx,
+      FCB_TRY(brick_adjoint_launch(pl->chunks, pl->bricks_adj, const_cast<float*>(volume), pl->vt, pl->nx,
                                    pl->ny, pl->nz, st));
     else
       FCB_TRY(brick_launch(pl->chunks, pl->bricks, volume, pl->vt, pl->nx, pl->ny, pl->nz, st));
