@@ -221,3 +221,37 @@ def test_katsevich_pi_window_vs_f64():
     ref, pairs = O.katsevich_piwin_f64(pb, proj, g.helical_pitch)
     assert pairs > 0
     assert O.rel_l2(got, ref) < 2e-3, O.rel_l2(got, ref)
+
+
+def test_host_driver_staging_of_large_pageable_buffers():
+    """Pageable caller buffers larger than one staging piece (64 MB), with a detector width
+    that is not a multiple of 4 (rows padded on the device): the staged copies through
+    pinned buffers give exactly the result of pinned caller buffers, for the backprojector
+    (volume in and out, projections in) and the projector (projections in and out)."""
+    import ctypes
+
+    import torch
+
+    from fastcone_b200 import _lib
+
+    g, pb = make_case(vol_xyz=(256, 256, 300), det_wh=(250, 300), nviews=240, D=900.0, pw=1.0, seed=4)
+    rng = np.random.default_rng(5)
+    proj = rng.random(g.proj_shape, dtype=np.float32)           # 72 MB
+    vol0 = rng.random(g.vol_shape, dtype=np.float32)            # 79 MB
+    gs = g.struct()
+    L = _lib.lib()
+    outs = []
+    for pinned in (False, True):
+        if pinned:
+            vol = torch.from_numpy(vol0.copy()).pin_memory().numpy()
+            hp = torch.from_numpy(proj.copy()).pin_memory().numpy()
+        else:
+            vol, hp = vol0.copy(), proj.copy()
+        _lib.check(L.fcb_backproject_host(0, ctypes.byref(gs), 2, hp.ctypes.data_as(_lib.c_float_p),
+                                          vol.ctypes.data_as(_lib.c_float_p)))
+        _lib.check(L.fcb_project_host(0, ctypes.byref(gs), _lib.PROJ_EXPLICIT, vol.ctypes.data_as(_lib.c_float_p),
+                                      hp.ctypes.data_as(_lib.c_float_p)))
+        outs.append((vol.copy(), hp.copy()))
+    assert np.array_equal(outs[0][0], outs[1][0])
+    assert np.array_equal(outs[0][1], outs[1][1])
+    assert not np.array_equal(outs[0][0], vol0)
