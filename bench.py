@@ -604,14 +604,20 @@ def main():
 
         call()
         barrier()
-        t0 = time.perf_counter()
-        ke = max(2, args.steps // 2)
+        # each call timed on its own (host clock around the whole call: copies in, kernels,
+        # copies out); the median of the calls, since a single host-side stall (paging,
+        # another process on the host) otherwise moves a two-call mean by a third
+        ke = max(3, args.steps // 2)
+        times = []
         for _ in range(ke):
+            t0 = time.perf_counter()
             call()
-        dt = barrier_max(time.perf_counter() - t0) / ke
+            times.append(time.perf_counter() - t0)
+        dt = barrier_max(float(np.median(times)))
         e2e = {"value": job_updates / dt / 1e9, "unit": UNIT,
                "h2d_bytes_per_step": hproj.numel() * 4 + hvol.numel() * 4,
                "d2h_bytes_per_step": hvol.numel() * 4, "ms_per_step": dt * 1e3,
+               "calls_ms": [round(t * 1e3, 1) for t in times], "statistic": f"median of {ke} calls",
                "path": "GPU_CB_K_backproject (C ABI), pinned host buffers"}
 
     cpu = None

@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -130,22 +131,38 @@ void par_memcpy(void* dst, const void* src, size_t bytes, int nthreads)
   for (std::thread& x : th) x.join();
 }
 
+// The pinned buffers are made on the first staged call and kept until the process exits
+// (3 x 64 MB of page-locked host memory: pinning them per call would cost more than small
+// transfers save); calls that stage take turns on them.
+std::mutex g_pin_mu;
+void* g_pin[3] = {nullptr, nullptr, nullptr};
+
 struct HostStager {
   static constexpr size_t PIECE = (size_t)64 << 20;  // bytes per pinned buffer
+  static constexpr size_t MIN_BYTES = (size_t)64 << 20;  // smaller transfers copy directly
   static constexpr int NBUF = 3;
   void* buf[NBUF] = {nullptr, nullptr, nullptr};
   cudaEvent_t done[NBUF] = {nullptr, nullptr, nullptr};
   bool used[NBUF] = {false, false, false};
   int next = 0, nthreads = 1;
   bool ok = false;
+  std::unique_lock<std::mutex> lock;
 
-  int init()
+  // `bytes`: the pageable traffic of the call; below MIN_BYTES the stager stays off
+  int init(size_t bytes)
   {
+    if (bytes < MIN_BYTES || getenv("FCB_HOST_NOSTAGE")) return FCB_OK;
+    lock = std::unique_lock<std::mutex>(g_pin_mu);
     for (int b = 0; b < NBUF; b++) {
-      if (cudaHostAlloc(&buf[b], PIECE, cudaHostAllocDefault) != cudaSuccess ||
-          cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) != cudaSuccess) {
+      if (!g_pin[b] && cudaHostAlloc(&g_pin[b], PIECE, cudaHostAllocPortable) != cudaSuccess) {
         cudaGetLastError();
+        g_pin[b] = nullptr;
         return FCB_OK;  // not fatal: the caller falls back to plain copies
+      }
+      buf[b] = g_pin[b];
+      if (cudaEventCreateWithFlags(&done[b], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return FCB_OK;
       }
     }
     unsigned hc = std::thread::hardware_concurrency();
@@ -161,7 +178,6 @@ struct HostStager {
         cudaEventSynchronize(done[b]);
         cudaEventDestroy(done[b]);
       }
-      if (buf[b]) cudaFreeHost(buf[b]);
     }
   }
   int take(int* b)
@@ -329,7 +345,7 @@ extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kern
   // pageable caller buffers (numpy arrays): pinned staging filled by host threads
   HostStager stager;
   const bool proj_pg = is_pageable(projections), vol_pg = is_pageable(volume);
-  if ((proj_pg || vol_pg) && !getenv("FCB_HOST_NOSTAGE")) FCB_TRY(stager.init());
+  FCB_TRY(stager.init((proj_pg ? (size_t)n * H * W * sizeof(float) : 0) + (vol_pg ? 2 * nvox * sizeof(float) : 0)));
   HostStager* pst = proj_pg && stager.ok ? &stager : nullptr;
   HostStager* vst = vol_pg && stager.ok ? &stager : nullptr;
   std::vector<cudaEvent_t> slab_done(nslab, nullptr);
@@ -445,7 +461,7 @@ extern "C" int fcb_project_host(int device, const fcb_geometry* g, int method, c
   // pageable caller buffers (numpy arrays): pinned staging filled by host threads
   HostStager stager;
   const bool proj_pg = is_pageable(projections), vol_pg = is_pageable(volume);
-  if ((proj_pg || vol_pg) && !getenv("FCB_HOST_NOSTAGE")) FCB_TRY(stager.init());
+  FCB_TRY(stager.init((proj_pg ? 2 * np * sizeof(float) : 0) + (vol_pg ? nvox * sizeof(float) : 0)));
   if (proj_pg && stager.ok)
     FCB_TRY(stager.h2d(dproj, projections, np * sizeof(float), xs));
   else
