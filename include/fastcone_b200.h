@@ -135,7 +135,10 @@ typedef struct fcb_geometry {
 } fcb_geometry;
 
 /* Host-buffer versions of GPU_CB_K_backproject / GPU_CB_misalign_project that return
- * the status.  Replaces unit_coneBeamGPU.cu:173-305 and :88-171. */
+ * the status.  Replaces unit_coneBeamGPU.cu:173-305 and :88-171.  Pinned (page-locked)
+ * caller buffers are copied by DMA directly; pageable ones of 64 MB or more go through
+ * three 64 MB pinned buffers that the library makes on the first such call and keeps until
+ * the process exits (calls from several threads take turns on them). */
 int fcb_backproject_host(int device, const fcb_geometry* g, int kernelMode,
                          const float* projections, float* volume);
 int fcb_project_host(int device, const fcb_geometry* g, int method, const float* volume,
