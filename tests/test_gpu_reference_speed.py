@@ -33,26 +33,26 @@ def _best(fn, reps):
     return best
 
 
-def _compare(vol_xyz, det_wh, nviews, D, pw, reps):
+def _compare(vol_xyz, det_wh, nviews, D, pw, reps, mode=2, hmid=None, arc=2 * np.pi):
     from fastcone_b200 import fastcone as fc
 
     norm = np.full(nviews, 1.0 / nviews, np.float32)
-    pb = O.make_problem(vol_xyz, det_wh, nviews, D=D, pw=pw, norm=norm)
+    pb = O.make_problem(vol_xyz, det_wh, nviews, D=D, pw=pw, norm=norm, hmid=hmid, arc=arc)
     proj = np.random.default_rng(0).random(pb.proj_shape, dtype=np.float32)
     upd = float(np.prod(vol_xyz)) * nviews
 
     def ours():
         vol = np.zeros(pb.vol_shape_zyx, np.float32)
-        fc.backproject(vol, proj, pb.angles, pb.D, pb.hMid, norm=norm, kernelMode=2, pixelWidth=pb.pw)
+        fc.backproject(vol, proj, pb.angles, pb.D, pb.hMid, norm=norm, kernelMode=mode, pixelWidth=pb.pw)
         return vol
 
     def ref():
-        return O.reflib_backproject(pb, proj, kernel_mode=2)
+        return O.reflib_backproject(pb, proj, kernel_mode=mode)
 
     t_ours = _best(ours, reps)
     t_ref = _best(ref, reps)
     err = O.rel_l2(ours(), ref())
-    print(f"\n{vol_xyz} x {nviews} views: ours {t_ours * 1e3:.1f} ms ({upd / t_ours / 1e9:.1f} GUPS), "
+    print(f"\n{vol_xyz} x {nviews} views, mode {mode}: ours {t_ours * 1e3:.1f} ms ({upd / t_ours / 1e9:.1f} GUPS), "
           f"reference CUDA path {t_ref * 1e3:.1f} ms ({upd / t_ref / 1e9:.1f} GUPS), "
           f"ratio {t_ref / t_ours:.1f}, rel-L2 {err:.2e}")
     return t_ours, t_ref, err
@@ -70,5 +70,20 @@ def test_faster_than_reference_cuda_path_small_fdk():
 def test_faster_than_reference_cuda_path_large_fdk():
     _need_ref()
     t_ours, t_ref, err = _compare((1024, 1024, 1024), (1536, 1024), 1440, 2000.0, 0.8, reps=1)
+    assert err < 1e-3
+    assert t_ours < t_ref
+
+
+@pytest.mark.skipif(os.environ.get("FCB_TIME_REFERENCE_LARGE") != "1",
+                    reason="the helical comparison runs with FCB_TIME_REFERENCE_LARGE=1")
+def test_faster_than_reference_cuda_path_helical_katsevich():
+    """The helical geometry (512x512x384, 4 turns x 1160 views, 736x64 detector) through the
+    reference's Katsevich backprojection (kernelMode 1: weight U, every view, no PI window --
+    the reference has none) and ours on the same arguments."""
+    _need_ref()
+    n = 4 * 1160
+    hmid = (384 / 2.0 - 0.5 * (n - 1) * (80.0 / 1160) + np.arange(n) * (80.0 / 1160)).astype(np.float32)
+    t_ours, t_ref, err = _compare((512, 512, 384), (736, 64), n, 1140.0, 1.096, reps=1, mode=1, hmid=hmid,
+                                  arc=4 * 2 * np.pi)
     assert err < 1e-3
     assert t_ours < t_ref
