@@ -598,69 +598,86 @@ __device__ __forceinline__ float gen_load(const void* base, int ptype, size_t i)
   return __uint_as_float(((uint32_t)u) << 16);
 }
 
+// One thread per (x, y) column and GEN_NZ consecutive z-voxels of the launch's z-range: the
+// view's matrix rows are read once per column and the x, y parts of the three projective
+// coordinates are shared, so a voxel-view costs one FMA per coordinate.
+constexpr int GEN_NZ = 8;
 __global__ void __launch_bounds__(256) bp_generic_kernel(const __grid_constant__ GenParams P)
 {
-  const long long i = P.vox0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= P.vox0 + P.nvox) return;
-  const int xi = (int)(i % P.nx);
-  const long long r = i / P.nx;
-  const int yi = (int)(r % P.ny), zi = (int)(r / P.ny);
-  const float x = P.ox + xi, y = P.oy + yi, z = P.oz + zi;
-  float acc = 0.0f;
-  const int4* wrow = nullptr;
-  if (P.win) {
-    const int tile = ((zi / P.sv2) * P.nty + yi / P.sv1) * P.ntx + xi / P.sv0;
-    wrow = P.win + (size_t)tile * P.wviews + P.view0;
-  }
+  const long long plane = (long long)P.nx * P.ny;
+  const int zfirst = (int)(P.vox0 / plane), zend = (int)((P.vox0 + P.nvox) / plane);
+  const int ngz = (zend - zfirst + GEN_NZ - 1) / GEN_NZ;
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= plane * ngz) return;
+  const int xi = (int)(t % P.nx);
+  const long long r = t / P.nx;
+  const int yi = (int)(r % P.ny), zg = (int)(r / P.ny);
+  const int zi0 = zfirst + zg * GEN_NZ;
+  const int nzv = min(GEN_NZ, zend - zi0);
+  const float x = P.ox + xi, y = P.oy + yi;
+  float acc[GEN_NZ];
+#pragma unroll
+  for (int k = 0; k < GEN_NZ; k++) acc[k] = 0.0f;
   for (int v = 0; v < P.nviews; v++) {
     const GenView& V = P.v[v];
-    const float uu = fmaf(V.m[0], x, fmaf(V.m[1], y, fmaf(V.m[2], z, V.m[3])));
-    const float vv = fmaf(V.m[4], x, fmaf(V.m[5], y, fmaf(V.m[6], z, V.m[7])));
-    const float ss = fmaf(V.m[8], x, fmaf(V.m[9], y, fmaf(V.m[10], z, V.m[11])));
-    const float rs = 1.0f / ss;
-    const float wl = uu * rs, hl = vv * rs;
-    float wt = V.wt;
-    if (P.wexp >= 1) wt *= V.kappa * rs;
-    if (P.wexp >= 2) wt *= V.kappa * rs;
-    if (wrow) {
-      // the reference's texture window: texel indices clamp to the window edge, texels
-      // outside the caller's data read zero (coneBeamGPU.cu:839-848, :1049-1088)
-      const int4 wb = wrow[v];
-      const float wc = fminf(fmaxf(wl, (float)wb.x - 2.0f), (float)wb.y + 2.0f);
-      const float hc = fminf(fmaxf(hl, (float)wb.z - 2.0f), (float)wb.w + 2.0f);
-      const float fw = floorf(wc), fh = floorf(hc);
-      const float a = wc - fw, b = hc - fh;
-      const int i0 = min(max((int)fw, wb.x), wb.y), i1 = min(max((int)fw + 1, wb.x), wb.y);
-      const int j0 = min(max((int)fh, wb.z), wb.w), j1 = min(max((int)fh + 1, wb.z), wb.w);
-      const size_t vb = (size_t)(P.view0 + v) * P.WH0 * P.WH1;
-      const bool ci0 = i0 >= 0 && i0 < P.WH0, ci1 = i1 >= 0 && i1 < P.WH0;
-      const bool cj0 = j0 >= 0 && j0 < P.WH1, cj1 = j1 >= 0 && j1 < P.WH1;
-      const float t00 = ci0 && cj0 ? gen_load(P.proj, P.ptype, vb + (size_t)j0 * P.WH0 + i0) : 0.f;
-      const float t10 = ci1 && cj0 ? gen_load(P.proj, P.ptype, vb + (size_t)j0 * P.WH0 + i1) : 0.f;
-      const float t01 = ci0 && cj1 ? gen_load(P.proj, P.ptype, vb + (size_t)j1 * P.WH0 + i0) : 0.f;
-      const float t11 = ci1 && cj1 ? gen_load(P.proj, P.ptype, vb + (size_t)j1 * P.WH0 + i1) : 0.f;
-      const float r0 = fmaf(a, t10 - t00, t00), r1 = fmaf(a, t11 - t01, t01);
-      acc = fmaf(wt, fmaf(b, r1 - r0, r0), acc);
-      continue;
-    }
-    if (!(wl > -1.0f && wl < (float)P.WH0 && hl > -1.0f && hl < (float)P.WH1)) continue;
-    const float fw0 = floorf(wl), fh0 = floorf(hl);
-    const int iw = (int)fw0, ih = (int)fh0;
-    const float a = wl - fw0, b = hl - fh0;
+    const float bu = fmaf(V.m[0], x, fmaf(V.m[1], y, V.m[3]));
+    const float bv = fmaf(V.m[4], x, fmaf(V.m[5], y, V.m[7]));
+    const float bs = fmaf(V.m[8], x, fmaf(V.m[9], y, V.m[11]));
+    const float mu = V.m[2], mv = V.m[6], ms = V.m[10];
     const size_t vb = (size_t)(P.view0 + v) * P.WH0 * P.WH1;
-    float t00 = 0.f, t10 = 0.f, t01 = 0.f, t11 = 0.f;
-    if (ih >= 0) {
-      if (iw >= 0) t00 = gen_load(P.proj, P.ptype, vb + (size_t)ih * P.WH0 + iw);
-      if (iw + 1 < P.WH0) t10 = gen_load(P.proj, P.ptype, vb + (size_t)ih * P.WH0 + iw + 1);
+#pragma unroll
+    for (int k = 0; k < GEN_NZ; k++) {
+      if (k >= nzv) break;
+      const int zi = zi0 + k;
+      const float z = P.oz + zi;
+      const float uu = fmaf(mu, z, bu), vv = fmaf(mv, z, bv), ss = fmaf(ms, z, bs);
+      const float rs = 1.0f / ss;
+      const float wl = uu * rs, hl = vv * rs;
+      float wt = V.wt;
+      if (P.wexp >= 1) wt *= V.kappa * rs;
+      if (P.wexp >= 2) wt *= V.kappa * rs;
+      if (P.win) {
+        // the reference's texture window: texel indices clamp to the window edge, texels
+        // outside the caller's data read zero (coneBeamGPU.cu:839-848, :1049-1088)
+        const int tile = ((zi / P.sv2) * P.nty + yi / P.sv1) * P.ntx + xi / P.sv0;
+        const int4 wb = P.win[(size_t)tile * P.wviews + P.view0 + v];
+        const float wc = fminf(fmaxf(wl, (float)wb.x - 2.0f), (float)wb.y + 2.0f);
+        const float hc = fminf(fmaxf(hl, (float)wb.z - 2.0f), (float)wb.w + 2.0f);
+        const float fw = floorf(wc), fh = floorf(hc);
+        const float a = wc - fw, b = hc - fh;
+        const int i0 = min(max((int)fw, wb.x), wb.y), i1 = min(max((int)fw + 1, wb.x), wb.y);
+        const int j0 = min(max((int)fh, wb.z), wb.w), j1 = min(max((int)fh + 1, wb.z), wb.w);
+        const bool ci0 = i0 >= 0 && i0 < P.WH0, ci1 = i1 >= 0 && i1 < P.WH0;
+        const bool cj0 = j0 >= 0 && j0 < P.WH1, cj1 = j1 >= 0 && j1 < P.WH1;
+        const float t00 = ci0 && cj0 ? gen_load(P.proj, P.ptype, vb + (size_t)j0 * P.WH0 + i0) : 0.f;
+        const float t10 = ci1 && cj0 ? gen_load(P.proj, P.ptype, vb + (size_t)j0 * P.WH0 + i1) : 0.f;
+        const float t01 = ci0 && cj1 ? gen_load(P.proj, P.ptype, vb + (size_t)j1 * P.WH0 + i0) : 0.f;
+        const float t11 = ci1 && cj1 ? gen_load(P.proj, P.ptype, vb + (size_t)j1 * P.WH0 + i1) : 0.f;
+        const float r0 = fmaf(a, t10 - t00, t00), r1 = fmaf(a, t11 - t01, t01);
+        acc[k] = fmaf(wt, fmaf(b, r1 - r0, r0), acc[k]);
+        continue;
+      }
+      if (!(wl > -1.0f && wl < (float)P.WH0 && hl > -1.0f && hl < (float)P.WH1)) continue;
+      const float fw0 = floorf(wl), fh0 = floorf(hl);
+      const int iw = (int)fw0, ih = (int)fh0;
+      const float a = wl - fw0, b = hl - fh0;
+      float t00 = 0.f, t10 = 0.f, t01 = 0.f, t11 = 0.f;
+      if (ih >= 0) {
+        if (iw >= 0) t00 = gen_load(P.proj, P.ptype, vb + (size_t)ih * P.WH0 + iw);
+        if (iw + 1 < P.WH0) t10 = gen_load(P.proj, P.ptype, vb + (size_t)ih * P.WH0 + iw + 1);
+      }
+      if (ih + 1 < P.WH1) {
+        if (iw >= 0) t01 = gen_load(P.proj, P.ptype, vb + (size_t)(ih + 1) * P.WH0 + iw);
+        if (iw + 1 < P.WH0) t11 = gen_load(P.proj, P.ptype, vb + (size_t)(ih + 1) * P.WH0 + iw + 1);
+      }
+      const float r0 = fmaf(a, t10 - t00, t00), r1 = fmaf(a, t11 - t01, t01);
+      acc[k] = fmaf(wt, fmaf(b, r1 - r0, r0), acc[k]);
     }
-    if (ih + 1 < P.WH1) {
-      if (iw >= 0) t01 = gen_load(P.proj, P.ptype, vb + (size_t)(ih + 1) * P.WH0 + iw);
-      if (iw + 1 < P.WH0) t11 = gen_load(P.proj, P.ptype, vb + (size_t)(ih + 1) * P.WH0 + iw + 1);
-    }
-    const float r0 = fmaf(a, t10 - t00, t00), r1 = fmaf(a, t11 - t01, t01);
-    acc = fmaf(wt, fmaf(b, r1 - r0, r0), acc);
   }
-  P.vol[i] += acc;
+  const size_t o = ((size_t)zi0 * P.ny + yi) * P.nx + xi;
+#pragma unroll
+  for (int k = 0; k < GEN_NZ; k++)
+    if (k < nzv) P.vol[o + (size_t)k * plane] += acc[k];
 }
 
 }  // namespace fcb
@@ -1054,7 +1071,8 @@ int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void
     P.vox0 = plane * z0;
     P.nvox = plane * (z1 - z0);
     if (P.nvox <= 0) continue;
-    bp_generic_kernel<<<(unsigned)((P.nvox + 255) / 256), 256, 0, st>>>(P);
+    const long long threads = plane * ((z1 - z0 + GEN_NZ - 1) / GEN_NZ);
+    bp_generic_kernel<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(P);
     FCB_CUDA_TRY(cudaGetLastError());
   }
   return ok();
