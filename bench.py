@@ -95,7 +95,8 @@ def parse():
                     help="N>1: independent volumes per rank (weak scaling) or one volume in z-slabs "
                          "(strong scaling)")
     ap.add_argument("--case", default=None,
-                    choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "conv-256", "katsevich", "pipeline"],
+                    choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "conv-256", "katsevich", "pipeline",
+                             "misaligned-256"],
                     help="profiling case: run only this kernel on a reduced workload (no JSON line)")
     return ap.parse_args()
 
@@ -110,6 +111,8 @@ def run_case(args):
     activation): forward (three kernel forms) and weight gradient (tensor cores and the
     CUDA-core kernel), all on tcgen05 except the last;
     katsevich: the helical PI-window backprojection (512x512x384, 4640 views; 1.3 GB);
+    misaligned-256: the general-matrix backprojector (a misaligned detector, unweighted) on
+    256^3 / 360 views / 384x256 through a plan, CUDA events over the timed calls;
     pipeline: every other kernel once at a moderate size, inputs above L2 where the workload
     allows: phantom, FDK filter (ramp + Shepp-Logan), Katsevich filter, projector adjoint,
     misaligned (generic) backprojection, reference-window backprojection and projection,
@@ -171,6 +174,26 @@ def run_case(args):
             res[name] = (time.perf_counter() - t0) * 1e3
         os.environ.pop("FCB_KATS_DIRECT_HILBERT", None)
         print(json.dumps(res))
+    elif args.case == "misaligned-256":
+        import dataclasses
+
+        from fastcone_b200 import configs
+
+        gd = configs.diff_batch()
+        gm = dataclasses.replace(gd, misalignments=np.array([1.5, -0.5, 2.0, 0.01, -0.01, 0.02], np.float32))
+        proj = torch.randn(gd.proj_shape, device=dev)
+        plan = ops.BackprojectPlan(gm, mode=_lib.MODE_UNWEIGHTED)
+        vol = torch.zeros(gm.vol_shape, device=dev)
+        for _ in range(args.warmup):
+            plan(proj, vol)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            plan(proj, vol)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        print(json.dumps({"case": args.case, "ms": ms, "GUPS": 256 ** 3 * 360 / ms / 1e6}))
     elif args.case == "pipeline":
         import dataclasses
 
