@@ -165,7 +165,7 @@ __device__ __forceinline__ void tma_prefetch(const CUtensorMap* map)
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
-// 3-D tiled TMA load (no multicast) completing on `bar`.
+// 3-D tiled TMA load into this CTA's own shared memory, completing on `bar`.
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar,
                                             int c0, int c1, int c2)
 {

@@ -12,7 +12,7 @@ backprojector (kernelMode 0, the reference's iterative-reconstruction backprojec
 R = 1/(A 1), C = 1/(B 1).  Each CNN_k has 3 layers (2->16->16->1 channels, 3^3 kernels,
 ReLU between) on the tcgen05 convolution kernels with BF16 weights/activations and FP32
 accumulation; its last layer starts at zero, so the untrained network is exactly FDK + 8
-SIRT steps (the fallback it is judged against).  The SIRT step g_k enters the network as
+SIRT steps (the fallback it is compared with).  The SIRT step g_k enters the network as
 data: training back-propagates through the CNNs and the x_k path, not through A and B.
 
 Attenuation: phantom densities U(0.1, 1.0) scaled by MU_PER_VOXEL = 0.025 per voxel, which
