@@ -37,6 +37,7 @@ DET = (1536, 1024)
 NVIEWS = 1440
 VOXEL_MM, PITCH_MM, SOD_MM, SDD_MM = 0.25, 0.4, 500.0, 1000.0
 FDK_BYTES_PER_UPDATE = {"f32": 16, "bf16": 8}  # bilinear gather: 4 detector samples
+WORKLOAD = "circular FDK backprojection 1024^3 voxels, 1440 views, 1536x1024 detector, FP32 filtered projections"
 
 
 # DRAM bytes per FDK launch (1024^3, 180 views per launch): ncu dram__bytes_read.sum +
@@ -369,49 +370,90 @@ def geometry():
     return g.with_norm(np.full(NVIEWS, 1.0 / NVIEWS, np.float32))
 
 
-def cpu_baseline(g, target_s=12.0):
+class CpuReferencePath:
     """Reference path (texture-emulating restatement of Fastcone's FDK kernel, sub-problem
-    tiling and windows) on this host's cores, on a bounded sample: whole detector-height
-    columns of voxels (all z, all views) at random (x, y); returns GUPS and the sample."""
-    import numpy as np
+    tiling and windows) on this host's cores, over bounded samples of the workload: whole
+    columns of voxels (all z, all views) at random (x, y).  `calibrate` sizes one sample for a
+    target duration; `sample` times one."""
 
-    from oracle import oracle as O
+    def __init__(self, g, seed=0):
+        import numpy as np
 
-    pb = O.make_problem(VOL, DET, NVIEWS, D=g.D, pw=g.pw, angles=g.angles, hmid=g.hmid, norm=g.norm)
-    rng = np.random.default_rng(0)
-    proj = rng.standard_normal((NVIEWS, DET[1], DET[0]), dtype=np.float32)
-    cores = os.cpu_count() or 1
+        from oracle import oracle as O
 
-    def run(ncols):
-        xy = rng.integers(0, VOL[0], size=(ncols, 2))
+        self.O = O
+        self.pb = O.make_problem(VOL, DET, NVIEWS, D=g.D, pw=g.pw, angles=g.angles, hmid=g.hmid, norm=g.norm)
+        self.rng = np.random.default_rng(seed)
+        self.proj = self.rng.standard_normal((NVIEWS, DET[1], DET[0]), dtype=np.float32)
+        self.cores = os.cpu_count() or 1
+        self.ncols = 2
+
+    def sample(self, ncols=None):
+        """Backproject `ncols` random voxel columns; returns (seconds, voxel-view updates)."""
+        import numpy as np
+
+        ncols = ncols or self.ncols
+        xy = self.rng.integers(0, VOL[0], size=(ncols, 2))
         z = np.arange(VOL[2])
         pts = np.stack([np.repeat(xy[:, 0], VOL[2]), np.repeat(xy[:, 1], VOL[2]), np.tile(z, ncols)], 1)
+        pts = pts.astype(np.int32)
         t0 = time.perf_counter()
-        O.ref_backproject_points(pb, proj, pts.astype(np.int32), kernel_mode=2, texq=1)
+        self.O.ref_backproject_points(self.pb, self.proj, pts, kernel_mode=2, texq=1)
         return time.perf_counter() - t0, len(pts) * NVIEWS
 
-    dt, upd = run(2)
-    ncols = max(2, int(2 * target_s / max(dt, 1e-3)))
-    dt, upd = run(ncols)
-    return {"value": upd / dt / 1e9, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{ncols} random (x,y) columns x {VOL[2]} z x {NVIEWS} views = {upd:.3g} updates "
-                      f"of the 1024^3 / 1440-view FDK, texture-emulating reference path "
-                      f"(oracle/fc_oracle.c), {dt:.1f} s"}
+    def calibrate(self, target_s):
+        dt, _ = self.sample(2)
+        self.ncols = max(2, int(2 * target_s / max(dt, 1e-3)))
+        return self.ncols
+
+    def describe(self, dt, upd, nsamples=1):
+        return (f"{nsamples} x {self.ncols} random (x,y) columns x {VOL[2]} z x {NVIEWS} views = {upd:.3g} "
+                f"updates of the 1024^3 / 1440-view FDK, texture-emulating reference path "
+                f"(oracle/fc_oracle.c, {self.cores} threads), {dt:.1f} s")
+
+
+def cpu_baseline(g, target_s=12.0):
+    """One bounded sample of the CPU reference path (about `target_s` seconds); returns the
+    cpu_baseline object of the JSON line."""
+    ref = CpuReferencePath(g)
+    ref.calibrate(target_s)
+    dt, upd = ref.sample()
+    return {"value": upd / dt / 1e9, "unit": UNIT, "cores": ref.cores, "kind": "port",
+            "sample": ref.describe(dt, upd)}
+
+
+def reference_line(args, g, budget_s=150.0):
+    """The reference arm: W untimed and K timed steps, each step one bounded sample of the
+    workload on the CPU reference path (all host threads), sized so the whole run stays within
+    about `budget_s` seconds; value = the K samples' updates / their total time."""
+    ref = CpuReferencePath(g)
+    per_step = min(12.0, max(1.0, budget_s / max(1, args.steps + args.warmup)))
+    ref.calibrate(per_step)
+    for _ in range(args.warmup):
+        ref.sample()
+    times, upd = [], 0
+    for _ in range(max(1, args.steps)):
+        dt, u = ref.sample()
+        times.append(dt)
+        upd += u
+    total = sum(times)
+    value = upd / total / 1e9
+    sample = ref.describe(total, upd, len(times))
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total / len(times) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "inputs": "host memory (the reference path has no device copy)",
+                       "parallelism": "host threads", "step": "one bounded sample of the workload",
+                       "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": ref.cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    g = geometry()
-    cb = cpu_baseline(g)
-    out = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
-           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-           "config": {"workload": "circular FDK 1024^3, 1440 views, 1536x1024 detector (bounded sample)",
-                      "sample": cb["sample"]},
-           "cpu_baseline": cb,
-           "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(out), flush=True)
+    print(json.dumps(reference_line(args, geometry())), flush=True)
 
 
 def main():
@@ -659,8 +701,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": scaling,
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "circular FDK backprojection 1024^3 voxels, 1440 views, 1536x1024 detector, "
-                               "FP32 filtered projections in HBM",
+        "config": {"workload": WORKLOAD, "inputs": "resident in HBM (value); pinned host buffers (e2e)",
                    "voxel_view_updates_per_step": updates, "D_voxels": g.D, "pw_voxels": g.pw,
                    "l2": "inputs (13.4 GB) larger than L2; no flush", "box": [info["box_w"], info["box_h"]],
                    "parallelism": parallelism},
