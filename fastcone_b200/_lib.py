@@ -25,6 +25,7 @@ FCB_ERR_NOMEM = 3
 FCB_ERR_TIMEOUT = 4
 FCB_ERR_NODEVICE = 5
 FCB_ERR_RANGE = 6
+FCB_ERR_HOST = 7
 
 FCB_F32, FCB_F16, FCB_BF16 = 0, 1, 2
 MODE_UNWEIGHTED, MODE_KATSEVICH, MODE_FDK = 0, 1, 2

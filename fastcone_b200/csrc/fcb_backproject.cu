@@ -1090,18 +1090,20 @@ int bp_plan_z_tile(const fcb_bp_plan* pl) { return pl->nz_tile; }
 
 extern "C" int fcb_bp_plan_create(const fcb_geometry* g, int kernelMode, int projType,
                                   fcb_bp_plan** out)
-{
+try {
   return bp_plan_create_ex(g, kernelMode, projType, FDK_MAXV, out);
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_bp_plan_execute(fcb_bp_plan* pl, const void* proj, float* volume, void* stream)
-{
+try {
   return bp_plan_execute_chunk(pl, -1, proj, volume, reinterpret_cast<cudaStream_t>(stream));
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_bp_plan_info(const fcb_bp_plan* pl, int* boxW, int* boxH, int* launches,
                                 long long* updates)
-{
+try {
   if (!pl) return set_error(FCB_ERR_INVALID, "NULL plan");
   if (boxW) *boxW = pl->path == 1 ? pl->BW : 0;
   if (boxH) *boxH = pl->path == 1 ? pl->BH : 0;
@@ -1109,22 +1111,25 @@ extern "C" int fcb_bp_plan_info(const fcb_bp_plan* pl, int* boxW, int* boxH, int
   if (updates) *updates = pl->updates;
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_bp_plan_destroy(fcb_bp_plan* pl)
-{
+try {
   delete pl;
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_backproject_device(const fcb_geometry* g, int kernelMode, const void* proj,
                                       int projType, float* volume, void* stream)
-{
+try {
   fcb_bp_plan* pl = nullptr;
   FCB_TRY(fcb_bp_plan_create(g, kernelMode, projType, &pl));
   int rc = fcb_bp_plan_execute(pl, proj, volume, stream);
   fcb_bp_plan_destroy(pl);
   return rc;
 }
+FCB_CATCH_STATUS
 
 // =====================================================================================
 // Backprojection without device-memory allocation
@@ -1165,7 +1170,7 @@ static int noalloc_scratch_address(int** out)
 extern "C" int fcb_backproject_device_noalloc(const fcb_geometry* g, int kernelMode,
                                               const void* proj, int projType, float* volume,
                                               void* stream)
-{
+try {
   if (!proj || !volume) return set_error(FCB_ERR_INVALID, "NULL projection or volume pointer");
   if (NOALLOC_NEEDED_INTS > NOALLOC_SCRATCH_INTS)
     return set_error(FCB_ERR_RANGE, "backprojection needs more scratch than the static array holds");
@@ -1186,3 +1191,4 @@ extern "C" int fcb_backproject_device_noalloc(const fcb_geometry* g, int kernelM
   if (status) return set_error(FCB_ERR_RANGE, "a kernel sample fell outside its staging window");
   return ok();
 }
+FCB_CATCH_STATUS

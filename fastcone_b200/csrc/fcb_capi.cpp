@@ -282,7 +282,7 @@ struct HostTrace {
 // windows that change the result run as one slab (their tiling starts at volStart).
 extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kernelMode,
                                     const float* projections, float* volume)
-{
+try {
   if (!g0 || !projections || !volume) return set_error(FCB_ERR_INVALID, "NULL argument");
   HostTrace tr;
   DeviceGuard guard(device);
@@ -437,10 +437,11 @@ extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kern
   }
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_project_host(int device, const fcb_geometry* g, int method, const float* volume,
                                 float* projections)
-{
+try {
   if (!g || !projections || !volume) return set_error(FCB_ERR_INVALID, "NULL argument");
   DeviceGuard guard(device);
   if (guard.rc) return guard.rc;
@@ -481,12 +482,14 @@ extern "C" int fcb_project_host(int device, const fcb_geometry* g, int method, c
   FCB_TRY(collect_device_status(cs));
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_sync_status(void* stream)
-{
+try {
   FCB_TRY(collect_device_status(reinterpret_cast<cudaStream_t>(stream)));
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_last_status(void);
 extern "C" const char* fcb_last_error(void);

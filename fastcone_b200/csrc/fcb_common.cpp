@@ -274,7 +274,7 @@ extern "C" const char* fcb_last_error(void) { return fcb::t_msg.c_str(); }
 // the hull of its corners' images.  Rows [lo, hi) are global detector rows; a view whose
 // footprint misses the detector gets lo = hi = 0.
 extern "C" int fcb_detector_rows(const fcb_geometry* g, int margin, int* rowLo, int* rowHi)
-{
+try {
   using namespace fcb;
   if (!rowLo || !rowHi || margin < 0) return set_error(FCB_ERR_INVALID, "bad detector-rows arguments");
   Problem pb;
@@ -315,3 +315,4 @@ extern "C" int fcb_detector_rows(const fcb_geometry* g, int margin, int* rowLo, 
   }
   return ok();
 }
+FCB_CATCH_STATUS

@@ -990,7 +990,7 @@ using namespace fcb;
 
 extern "C" int fcb_conv3d16_device(const void* x, const void* w, const float* bias, void* y, int yType,
                                    int nx, int ny, int nz, int relu, void* stream)
-{
+try {
   if (!x || !w || !y || nx <= 0 || ny <= 0 || nz <= 0 || (yType != FCB_F32 && yType != FCB_BF16))
     return set_error(FCB_ERR_INVALID, "bad conv3d arguments");
   if (((uintptr_t)x & 15) || ((uintptr_t)w & 15) || ((uintptr_t)y & 15))
@@ -1044,10 +1044,11 @@ extern "C" int fcb_conv3d16_device(const void* x, const void* w, const float* bi
   FCB_CUDA_TRY(cudaGetLastError());
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_conv3d16_wgrad_device(const void* x, const void* dy, int dyType, float* dw, int nx, int ny,
                                          int nz, void* stream)
-{
+try {
   if (!x || !dy || !dw || nx <= 0 || ny <= 0 || nz <= 0 || (dyType != FCB_F32 && dyType != FCB_BF16))
     return set_error(FCB_ERR_INVALID, "bad conv3d wgrad arguments");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
@@ -1097,3 +1098,4 @@ extern "C" int fcb_conv3d16_wgrad_device(const void* x, const void* dy, int dyTy
   FCB_CUDA_TRY(cudaGetLastError());
   return ok();
 }
+FCB_CATCH_STATUS

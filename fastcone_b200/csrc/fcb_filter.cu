@@ -180,7 +180,7 @@ static int filter_response(int W, int window, double gaussScale, int* L, std::ve
 
 extern "C" int fcb_filter_plan_create_ex(int nviews, int H, int W, int outType, int window,
                                          double gaussScale, fcb_filter_plan** out)
-{
+try {
   if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
   *out = nullptr;
   if (nviews <= 0 || H <= 0 || W <= 0) return set_error(FCB_ERR_INVALID, "bad filter sizes");
@@ -223,17 +223,19 @@ extern "C" int fcb_filter_plan_create_ex(int nviews, int H, int W, int outType, 
   *out = pl;
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_filter_plan_create(int nviews, int H, int W, int outType, int window,
                                       fcb_filter_plan** out)
-{
+try {
   return fcb_filter_plan_create_ex(nviews, H, W, outType, window, 0.125, out);
 }
+FCB_CATCH_STATUS
 
 // out = filter(in) as outType; zOrigin (host, nviews floats) is read before the call returns.
 extern "C" int fcb_filter_plan_execute(fcb_filter_plan* pl, const float* in, void* out, float D,
                                        const float* zOrigin, int cosineWeight, void* stream)
-{
+try {
   if (!pl || !in || !out) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
   if (cosineWeight && (!zOrigin || !(D > 0.0f)))
     return set_error(FCB_ERR_INVALID, "cosine weighting needs D > 0 and zOrigin");
@@ -266,17 +268,19 @@ extern "C" int fcb_filter_plan_execute(fcb_filter_plan* pl, const float* in, voi
   FCB_CUDA_TRY(cudaGetLastError());
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_filter_plan_destroy(fcb_filter_plan* pl)
-{
+try {
   delete pl;
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_fdk_filter_device(const float* in, void* out, int outType, int nviews, int H,
                                      int W, float D, const float* zOrigin, int cosineWeight,
                                      int window, void* stream)
-{
+try {
   if (!in || !out || nviews <= 0 || H <= 0 || W <= 0)
     return set_error(FCB_ERR_INVALID, "bad filter arguments");
   if (cosineWeight && (!zOrigin || !(D > 0.0f)))
@@ -291,10 +295,11 @@ extern "C" int fcb_fdk_filter_device(const float* in, void* out, int outType, in
   if (e != cudaSuccess) return set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_phantom_device(float* vol, const int volDim[3], const double* params, int n,
                                   void* stream)
-{
+try {
   if (!vol || !volDim || (n > 0 && !params) || n < 0) return set_error(FCB_ERR_INVALID, "bad phantom arguments");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const long long nv = (long long)volDim[0] * volDim[1] * volDim[2];
@@ -310,3 +315,4 @@ extern "C" int fcb_phantom_device(float* vol, const int volDim[3], const double*
   }
   return ok();
 }
+FCB_CATCH_STATUS

@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <exception>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -31,6 +33,22 @@ int ok();
     int s_ = (expr);             \
     if (s_ != FCB_OK) return s_; \
   } while (0)
+// Every C entry point's body is a function-try-block ending in FCB_CATCH_STATUS: no C++
+// exception (a failed host allocation, a copy thread that could not start) crosses the C
+// boundary; it becomes a status like any other failure.
+#define FCB_CATCH_STATUS                                                    \
+  catch (const std::bad_alloc&)                                             \
+  {                                                                         \
+    return ::fcb::set_error(FCB_ERR_NOMEM, "host memory allocation failed"); \
+  }                                                                         \
+  catch (const std::exception& e)                                           \
+  {                                                                         \
+    return ::fcb::set_error(FCB_ERR_HOST, e.what());                        \
+  }                                                                         \
+  catch (...)                                                               \
+  {                                                                         \
+    return ::fcb::set_error(FCB_ERR_HOST, "unexpected host-side exception"); \
+  }
 
 // Device-side failure bits recorded in the per-device status word.
 enum : int { DEV_TIMEOUT = 1, DEV_RANGE = 2 };

@@ -276,7 +276,7 @@ struct fcb_katsevich_plan {
 extern "C" int fcb_katsevich_plan_create(int nviews, int H, int W, const float* angles, float D,
                                          float pw, float pitch, int nkappa,
                                          fcb_katsevich_plan** out)
-{
+try {
   if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
   *out = nullptr;
   if (!angles || nviews < 2 || H < 2 || W < 2 || !(D > 0) || !(pw > 0) || pitch == 0.0f)
@@ -385,10 +385,11 @@ extern "C" int fcb_katsevich_plan_create(int nviews, int H, int W, const float* 
   *out = pl;
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_katsevich_plan_execute(fcb_katsevich_plan* pl, const float* in, float* out,
                                           void* stream)
-{
+try {
   if (!pl || !in || !out) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const int nviews = pl->nviews, H = pl->H, W = pl->W, K = pl->K, L = pl->L, nb = pl->nb;
@@ -448,17 +449,19 @@ extern "C" int fcb_katsevich_plan_execute(fcb_katsevich_plan* pl, const float* i
   FCB_CUDA_TRY(cudaGetLastError());
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_katsevich_plan_destroy(fcb_katsevich_plan* pl)
-{
+try {
   delete pl;
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_katsevich_filter_device(const float* in, float* out, int nviews, int H, int W,
                                            const float* angles, float D, float pw, float pitch,
                                            int nkappa, void* stream)
-{
+try {
   if (!in || !out) return set_error(FCB_ERR_INVALID, "bad Katsevich filter arguments");
   fcb_katsevich_plan* pl = nullptr;
   FCB_TRY(fcb_katsevich_plan_create(nviews, H, W, angles, D, pw, pitch, nkappa, &pl));
@@ -470,3 +473,4 @@ extern "C" int fcb_katsevich_filter_device(const float* in, float* out, int nvie
   if (e != cudaSuccess) return set_error(FCB_ERR_CUDA, cudaGetErrorString(e));
   return ok();
 }
+FCB_CATCH_STATUS

@@ -1121,7 +1121,7 @@ struct fcb_proj_plan {
 };
 
 extern "C" int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_plan** out)
-{
+try {
   if (!out) return set_error(FCB_ERR_INVALID, "plan output pointer is NULL");
   *out = nullptr;
   if (method != FCB_PROJ_TEXTURE && method != FCB_PROJ_EXPLICIT && method != FCB_PROJ_EXPLICIT_GLOBAL)
@@ -1186,11 +1186,12 @@ extern "C" int fcb_proj_plan_create(const fcb_geometry* g, int method, fcb_proj_
   *out = pl;
   return ok();
 }
+FCB_CATCH_STATUS
 
 // proj += norm * A vol (adjoint == 0), or vol += A^T (norm * proj) (adjoint != 0, explicit only).
 extern "C" int fcb_proj_plan_execute(fcb_proj_plan* pl, const float* volume, float* proj, int adjoint,
                                      void* stream)
-{
+try {
   if (!pl || !volume || !proj) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (adjoint && pl->method == FCB_PROJ_TEXTURE)
@@ -1227,10 +1228,11 @@ extern "C" int fcb_proj_plan_execute(fcb_proj_plan* pl, const float* volume, flo
   }
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_proj_plan_info(const fcb_proj_plan* pl, int* staged, int* brickC, int* brickZ,
                                   int* stages)
-{
+try {
   if (!pl) return set_error(FCB_ERR_INVALID, "NULL plan");
   if (staged) *staged = pl->bricks.ok ? 1 : 0;
   if (brickC) *brickC = pl->bricks.BC;
@@ -1238,9 +1240,10 @@ extern "C" int fcb_proj_plan_info(const fcb_proj_plan* pl, int* staged, int* bri
   if (stages) *stages = pl->bricks.stages;
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_proj_plan_destroy(fcb_proj_plan* pl)
-{
+try {
   if (pl) {
     if (pl->tex) cudaDestroyTextureObject(pl->tex);
     if (pl->arr) cudaFreeArray(pl->arr);
@@ -1249,10 +1252,11 @@ extern "C" int fcb_proj_plan_destroy(fcb_proj_plan* pl)
   }
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_project_device(const fcb_geometry* g, int method, const float* volume,
                                   float* proj, void* stream)
-{
+try {
   if (!volume || !proj) return set_error(FCB_ERR_INVALID, "NULL buffer");
   if (method != FCB_PROJ_TEXTURE && method != FCB_PROJ_EXPLICIT && method != FCB_PROJ_EXPLICIT_GLOBAL)
     return set_error(FCB_ERR_INVALID, "unknown projector method");
@@ -1262,10 +1266,11 @@ extern "C" int fcb_project_device(const fcb_geometry* g, int method, const float
                          reinterpret_cast<cudaStream_t>(stream)));
   return ok();
 }
+FCB_CATCH_STATUS
 
 extern "C" int fcb_project_adjoint_device(const fcb_geometry* g, const float* proj, float* volume,
                                           void* stream)
-{
+try {
   if (!volume || !proj) return set_error(FCB_ERR_INVALID, "NULL buffer");
   Problem pb;
   FCB_TRY(make_problem(g, &pb));
@@ -1273,12 +1278,13 @@ extern "C" int fcb_project_adjoint_device(const fcb_geometry* g, const float* pr
                          reinterpret_cast<cudaStream_t>(stream)));
   return ok();
 }
+FCB_CATCH_STATUS
 
 // Projector with a device-side sample counter (Gsamples accounting for benchmarks).
 extern "C" int fcb_project_device_counted(const fcb_geometry* g, int method, const float* volume,
                                           float* proj, unsigned long long* samples_dev,
                                           void* stream)
-{
+try {
   if (!volume || !proj) return set_error(FCB_ERR_INVALID, "NULL buffer");
   Problem pb;
   FCB_TRY(make_problem(g, &pb));
@@ -1286,3 +1292,4 @@ extern "C" int fcb_project_device_counted(const fcb_geometry* g, int method, con
                          reinterpret_cast<cudaStream_t>(stream)));
   return ok();
 }
+FCB_CATCH_STATUS

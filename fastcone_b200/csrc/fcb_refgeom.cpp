@@ -227,7 +227,7 @@ int ref_windows(const Problem& pb, bool with_misalign, RefWindows* rw)
 extern "C" int fcb_reference_windows(const fcb_geometry* g, int* subVolDim, int* subProjDim,
                                      int* tiles, int* ws, int* hs, int* sweepStart,
                                      int* sweepSteps, int* matters)
-{
+try {
   if (!g) return fcb::set_error(FCB_ERR_INVALID, "NULL geometry");
   fcb::Problem pb;
   FCB_TRY(fcb::make_problem(g, &pb));
@@ -245,3 +245,4 @@ extern "C" int fcb_reference_windows(const fcb_geometry* g, int* subVolDim, int*
   if (matters) { matters[0] = rw.bp_matters ? 1 : 0; matters[1] = rw.proj_matters ? 1 : 0; }
   return fcb::ok();
 }
+FCB_CATCH_STATUS

@@ -34,6 +34,7 @@ extern "C" {
 #define FCB_ERR_TIMEOUT 4   /* a bounded device-side wait gave up (kernel status word) */
 #define FCB_ERR_NODEVICE 5  /* GPUID does not name a CUDA device */
 #define FCB_ERR_RANGE 6     /* geometry outside what a kernel's staging window supports */
+#define FCB_ERR_HOST 7      /* a host-side failure other than memory (e.g. a copy thread) */
 
 /* projection storage types for the device entry points */
 #define FCB_F32 0
