@@ -1,7 +1,11 @@
 """Generates golden vectors for the Python-layer pre-processing by running the reference's
 OWN fastcone.py (fastcone.py:260-319) in this container.
 
-    python tests/golden/make_golden.py [/path/to/reference]
+    python tests/golden/make_golden.py [/path/to/reference] [all|api]
+
+It also records the signatures of the module's public functions (names, kinds and defaults
+of their parameters, fastcone.py:52, :147, :260, :272, :294, :306) in fastcone_api.json; the
+``api`` argument writes only that file.
 
 Three shims, applied to the imported module only, make it runnable on numpy >= 1.12 without
 touching its code: ``np.zeros`` accepts the float shape the reference builds
@@ -33,8 +37,47 @@ def load_reference(ref_dir):
     return mod
 
 
-def main(ref_dir="/root/reference"):
+API_FUNCTIONS = ("project", "backproject", "fbp", "rampfilter", "cosrampfilter", "gaussrampfilter")
+
+
+def describe_default(v):
+    """JSON form of a parameter default (numpy arrays by dtype and values)."""
+    import inspect
+
+    if v is inspect.Parameter.empty:
+        return {"required": True}
+    if isinstance(v, np.ndarray):
+        return {"array": v.tolist(), "dtype": str(v.dtype)}
+    return {"value": v}
+
+
+def api_signatures(mod):
+    """Parameter names, kinds and defaults of the module's public functions."""
+    import inspect
+
+    out = {}
+    for name in API_FUNCTIONS:
+        sig = inspect.signature(getattr(mod, name))
+        out[name] = [{"name": p.name, "kind": p.kind.name, **describe_default(p.default)}
+                     for p in sig.parameters.values()]
+    out["constants"] = {"FLOAT_TYPE": np.dtype(mod.FLOAT_TYPE).name, "INT_TYPE": np.dtype(mod.INT_TYPE).name}
+    return out
+
+
+def write_api(ref):
+    import json
+
+    with open(os.path.join(HERE, "fastcone_api.json"), "w") as f:
+        json.dump(api_signatures(ref), f, indent=1)
+        f.write("\n")
+
+
+def main(ref_dir="/root/reference", what="all"):
     ref = load_reference(ref_dir)
+    write_api(ref)
+    if what == "api":
+        print("API signatures written to", HERE)
+        return
     rng = np.random.default_rng(20240601)
     for name, shape in (("rampfilter_a", (3, 16, 24)), ("rampfilter_b", (2, 9, 37))):
         x = rng.standard_normal(shape).astype(np.float32)
