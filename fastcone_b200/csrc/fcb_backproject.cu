@@ -708,17 +708,25 @@ struct fcb_bp_plan {
 
 namespace {
 
+// Dynamic shared memory of one fdk_tma_kernel CTA: `stages` boxes of BW x BH elements of
+// `es` bytes, a full and an empty barrier and a footprint record per stage, and, for 16-bit
+// storage widened to FP32 (`widen`), two FP32 boxes (layout of fdk_tma_kernel).
+size_t fdk_smem_bytes(int BW, int BH, int stages, size_t es, bool widen)
+{
+  const size_t stage_bytes = ((size_t)BW * BH * es + 127) & ~(size_t)127;
+  size_t smem = stages * stage_bytes + stages * (2 * sizeof(uint64_t) + sizeof(int4));
+  if (widen) {
+    const size_t fbuf = ((size_t)BW * BH * 4 + 127) & ~(size_t)127;
+    smem = ((smem + 127) & ~(size_t)127) + 2 * fbuf;
+  }
+  return smem;
+}
+
 // Launches chunk `chunk` (-1: all) over the z-tile layers [tz0, tz1) of the plan.
 template <typename T, int NZ, bool PIW, bool X2, int MINB = fdk_min_blocks<NZ>()>
 int launch_fdk(fcb_bp_plan* pl, const CUtensorMap& map, int chunk, int tz0, int tz1, cudaStream_t st)
 {
-  const size_t stage_bytes = ((size_t)pl->BW * pl->BH * sizeof(T) + 127) & ~(size_t)127;
-  size_t smem = pl->stages * stage_bytes + pl->stages * (2 * sizeof(uint64_t) + sizeof(int4));
-  if (X2 && sizeof(T) == 2) {
-    // two FP32 buffers for the widened boxes (layout of fdk_tma_kernel)
-    const size_t fbuf = ((size_t)pl->BW * pl->BH * 4 + 127) & ~(size_t)127;
-    smem = ((smem + 127) & ~(size_t)127) + 2 * fbuf;
-  }
+  const size_t smem = fdk_smem_bytes(pl->BW, pl->BH, pl->stages, sizeof(T), X2 && sizeof(T) == 2);
   auto kern = fdk_tma_kernel<T, NZ, PIW, X2, MINB>;
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int c = 0; c < (int)pl->fdk.size(); c++) {
@@ -901,8 +909,19 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
     pl->BH = h[1];
     if (pl->BW < align) pl->BW = align;
     if (pl->BH < 2) pl->BH = 2;
-    if (pl->BW > 256 || pl->BH > 256) {
-      pl->path = 0;  // footprint too large for one TMA box: generic kernel
+    // the largest dynamic shared memory a CTA of this device may opt into
+    int smem_optin = 227 * 1024;  // sm_100
+    if (cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, pl->device) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      smem_optin = 227 * 1024;
+    }
+    const size_t es_box = dtype_size(projType);
+    if (pl->BW > 256 || pl->BH > 256 ||
+        fdk_smem_bytes(pl->BW, pl->BH, 2, es_box, es_box == 2) > (size_t)smem_optin) {
+      // footprint too large for one TMA box, or two staged boxes exceed a CTA's shared
+      // memory (strong magnification: detector pixels much finer than voxels): generic kernel
+      pl->path = 0;
       pl->fdk.clear();
     } else {
       const size_t es = dtype_size(projType);

@@ -109,6 +109,27 @@ def test_plan_reuse_and_info():
     assert O.rel_l2(v.cpu().numpy(), 2 * ref64) < 2e-5
 
 
+def test_fdk_footprint_beyond_shared_memory_runs_generic():
+    """Detector pixels much finer than voxels (pw = 0.14 voxel): a 16x16x32-voxel tile's
+    footprint is about 155 x 225 pixels at 45 degrees, and two staged FP32 boxes of it
+    (2 x 136 KB) exceed a CTA's 227 KB of shared memory, so the plan takes the general-matrix
+    kernel (no staging box) instead of failing at launch; the result equals the FP64 oracle."""
+    import torch
+
+    from fastcone_b200 import ops
+
+    g, pb = make_case(vol_xyz=(48, 48, 48), det_wh=(512, 352), nviews=16, D=1000.0, pw=0.14)
+    proj = np.random.default_rng(9).random(pb.proj_shape, dtype=np.float32)
+    plan = ops.BackprojectPlan(g, mode=2)
+    info = plan.info()
+    assert info["box_w"] == 0 and info["box_h"] == 0, info
+    v = torch.zeros(g.vol_shape, device="cuda")
+    plan(torch.from_numpy(proj).cuda(), v)
+    ops.sync_status()
+    ref64 = O.backproject_f64(pb, proj, kernel_mode=2)
+    assert O.rel_l2(v.cpu().numpy(), ref64) < 3e-5
+
+
 def test_reference_abi_host_buffers():
     """GPU_CB_K_backproject with host buffers (the reference's entry point) == device API."""
     from fastcone_b200 import fastcone as fc
