@@ -179,3 +179,70 @@ def test_windowed_or_reference_geometries_are_refused():
     g = ConeGeometry((8, 8, 8), (10, 10), np.zeros(2), 30.0, 1.0, reference_windows=True)
     with pytest.raises(ValueError):
         slabs.SlabDecomposition(g, 2)
+
+
+def _footprint_rows(g, t, z0, z1):
+    """Floor of the lowest and highest detector row that the voxel centres of planes
+    [z0, z1) reach in view t (FP64 projective map; the 8 corners of the slab's box bound the
+    rows, since h is monotone in z and in the in-plane depth)."""
+    zc = g.vol_xyz[2] // 2
+    xs = np.array([g.vol_start[0], g.vol_end[0] - 1], float) - g.vol_xyz[0] // 2
+    ys = np.array([g.vol_start[1], g.vol_end[1] - 1], float) - g.vol_xyz[1] // 2
+    zs = np.array([z0, z1 - 1], float) - zc
+    a = float(g.angles[t])
+    ca, sa = np.cos(a), np.sin(a)
+    src_z = float(g.hmid[t]) - zc
+    hs = []
+    for x in xs:
+        for y in ys:
+            depth = g.D + x * ca + y * sa
+            for z in zs:
+                # the detector centre rides with the source (row H // 2 at the source's height)
+                hs.append((z - src_z) * g.D / depth / g.pw + g.det_wh[1] // 2)
+    return np.floor(min(hs)), np.floor(max(hs))
+
+
+def test_decomposition_properties_on_random_geometries():
+    """Random circular and helical geometries, sub-volumes and world sizes (more ranks than
+    z tiles included): the slabs partition the sub-volume's planes in rank order in multiples
+    of the alignment, the view runs partition the views, every band lies on the detector,
+    both directions of the exchange agree in size, and every view a slab keeps covers the
+    rows its voxels reach."""
+    hyp = pytest.importorskip("hypothesis")
+    st = hyp.strategies
+
+    from fastcone_b200 import slabs
+    from fastcone_b200.geometry import ConeGeometry
+
+    @hyp.settings(max_examples=40, deadline=None, derandomize=True)
+    @hyp.given(nx=st.integers(4, 24), nz=st.integers(1, 70), zlo=st.integers(0, 10), nviews=st.integers(1, 24),
+               world=st.integers(1, 7), align=st.sampled_from([1, 8, 32]), helical=st.booleans(),
+               D=st.floats(40.0, 400.0), pw=st.floats(0.5, 1.5))
+    def check(nx, nz, zlo, nviews, world, align, helical, D, pw):
+        nzv = nz + zlo + 3
+        H = int(np.ceil(nzv * 1.6 / pw)) + 4
+        W = int(np.ceil(nx * 2.2 / pw)) + 4
+        angles = np.arange(nviews) * (2 * np.pi / max(1, min(nviews, 12)))
+        hmid = np.linspace(0.0, nzv, nviews) if helical else None
+        g = ConeGeometry((nx, nx, nzv), (W, H), angles, D, pw, hmid=hmid, vol_start=(0, 0, zlo),
+                         vol_end=(nx, nx, zlo + nz))
+        dec = slabs.SlabDecomposition(g, world, align=align)
+        planes, views = [], []
+        for r in range(world):
+            z0, z1 = dec.slab(r)
+            assert (z0 - zlo) % align == 0 or z0 == z1
+            planes.extend(range(z0, z1))
+            views.extend(range(*dec.views(r)))
+            b = dec.bands[r]
+            assert np.all(b.lo >= 0) and np.all(b.lo + b.rows <= H)
+            assert sum(dec.split_sizes(s, r) for s in range(world)) == len(b.views) * b.rows * W
+            for i, t in enumerate(b.views):
+                lo, hi = _footprint_rows(g, int(t), z0, z1)
+                # rows the bilinear taps read: floor(h) and floor(h) + 1, clipped to the detector
+                need_lo, need_hi = max(0.0, lo), min(H - 1.0, hi + 1)
+                if need_lo <= need_hi:
+                    assert b.lo[i] <= need_lo and need_hi < b.lo[i] + b.rows, (r, t)
+        assert planes == list(range(zlo, zlo + nz))
+        assert views == list(range(nviews))
+
+    check()
