@@ -36,9 +36,38 @@ CASES = _cases()
 
 @pytest.mark.parametrize("idx", range(len(CASES)))
 def test_windows_match_oracle(idx):
+    pb, mis = CASES[idx]
+    _compare_windows(pb, mis)
+
+
+def test_windows_match_oracle_on_random_geometries():
+    """Random volumes, sub-volumes, detectors, windows, distances, pitches and
+    misalignments: the library's windows, tiles and sweeps equal the oracle's bit for bit."""
+    hyp = pytest.importorskip("hypothesis")
+    st = hyp.strategies
+
+    @hyp.settings(max_examples=60, deadline=None, derandomize=True)
+    @hyp.given(vol=st.tuples(st.integers(4, 90), st.integers(4, 90), st.integers(4, 90)),
+               det=st.tuples(st.integers(8, 200), st.integers(8, 160)), nviews=st.integers(1, 40),
+               D=st.floats(30.0, 600.0), pw=st.floats(0.3, 1.6), sub=st.booleans(), mis=st.booleans(),
+               seed=st.integers(0, 2 ** 16))
+    def check(vol, det, nviews, D, pw, sub, mis, seed):
+        rng = np.random.default_rng(seed)
+        kw = {}
+        if sub:
+            lo = [int(rng.integers(0, max(1, v // 3))) for v in vol]
+            hi = [int(rng.integers(l + 1, v + 1)) for l, v in zip(lo, vol)]
+            kw = dict(volStart=tuple(lo), volEnd=tuple(hi))
+        pb = O.make_problem(vol, det, nviews, D=D, pw=pw, **kw)
+        m = rng.uniform(-1, 1, 6).astype(np.float32) * np.array([2, 2, 2, 0.03, 0.03, 0.03], np.float32) if mis else None
+        _compare_windows(pb, m)
+
+    check()
+
+
+def _compare_windows(pb, mis):
     from fastcone_b200 import ops
 
-    pb, mis = CASES[idx]
     a = O.ref_geometry(pb, mis)
     b = ops.reference_windows(_geom(pb, mis))
     assert np.array_equal(b["subVolDim"], a["subVolDim"])
