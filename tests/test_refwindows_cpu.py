@@ -127,3 +127,33 @@ def test_proj_matters_flag_covers_every_difference(kw):
     diff = O.rel_l2(O.ref_project(pb, vol, texq=0), O.project_f64(pb, vol))
     if diff > 1e-5:
         assert ops.reference_windows(_geom(pb))["proj_matters"], diff
+
+
+def test_flags_never_miss_a_difference_on_random_geometries():
+    """Random small geometries: whenever the reference's windows or sweeps change the
+    backprojection or the projection (oracle, exact weights), the library's bp_matters /
+    proj_matters flag is set, so the reference-compatible kernels run exactly where they
+    are needed or more often, never less."""
+    hyp = pytest.importorskip("hypothesis")
+    st = hyp.strategies
+
+    from fastcone_b200 import ops
+
+    @hyp.settings(max_examples=30, deadline=None, derandomize=True)
+    @hyp.given(vol=st.tuples(st.integers(4, 28), st.integers(4, 28), st.integers(4, 28)),
+               det=st.tuples(st.integers(8, 72), st.integers(8, 56)), nviews=st.integers(1, 10),
+               D=st.floats(30.0, 300.0), pw=st.floats(0.3, 1.5), seed=st.integers(0, 2 ** 16))
+    def check(vol, det, nviews, D, pw, seed):
+        pb = O.make_problem(vol, det, nviews, D=D, pw=pw)
+        rng = np.random.default_rng(seed)
+        flags = ops.reference_windows(_geom(pb))
+        proj = rng.random(pb.proj_shape, dtype=np.float32)
+        for mode in (2, 0):
+            diff = O.rel_l2(O.ref_backproject(pb, proj, kernel_mode=mode, texq=0),
+                            O.backproject_f64(pb, proj, kernel_mode=mode))
+            assert diff <= 1e-5 or flags["bp_matters"], (mode, diff)
+        v = rng.random(vol[::-1], dtype=np.float32)
+        diff = O.rel_l2(O.ref_project(pb, v, texq=0), O.project_f64(pb, v))
+        assert diff <= 1e-5 or flags["proj_matters"], diff
+
+    check()
