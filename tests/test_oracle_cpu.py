@@ -50,6 +50,40 @@ def test_geometry_restatement_matches_reference_host_code(idx):
         assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
 
 
+def test_geometry_restatement_matches_reference_on_random_geometries():
+    """The same comparison on random volumes, sub-volumes, detectors, data windows,
+    distances, pitches, source heights and misalignments."""
+    if O.reflib() is None:
+        pytest.skip("oracle/_ref not built (reference sources unavailable at build time)")
+    hyp = pytest.importorskip("hypothesis")
+    st = hyp.strategies
+
+    @hyp.settings(max_examples=40, deadline=None, derandomize=True)
+    @hyp.given(vol=st.tuples(st.integers(4, 120), st.integers(4, 120), st.integers(4, 120)),
+               det=st.tuples(st.integers(8, 240), st.integers(8, 200)), nviews=st.integers(1, 60),
+               D=st.floats(30.0, 3000.0), pw=st.floats(0.3, 1.6), sub=st.booleans(), win=st.booleans(),
+               mis=st.booleans(), seed=st.integers(0, 2 ** 16))
+    def check(vol, det, nviews, D, pw, sub, win, mis, seed):
+        rng = np.random.default_rng(seed)
+        kw = {}
+        if sub:
+            lo = [int(rng.integers(0, max(1, v // 3))) for v in vol]
+            kw.update(volStart=tuple(lo), volEnd=tuple(int(rng.integers(l + 1, v + 1)) for l, v in zip(lo, vol)))
+        if win:
+            ww, wh = int(rng.integers(4, det[0] + 1)), int(rng.integers(4, det[1] + 1))
+            kw.update(whsize=(ww, wh), woff=rng.integers(0, det[0] - ww + 1, nviews),
+                      hoff=rng.integers(0, det[1] - wh + 1, nviews))
+        pb = O.make_problem(vol, det, nviews, D=D, pw=pw, **kw)
+        pb.hMid[:] = (vol[2] / 2 + rng.uniform(-0.3, 0.3, nviews) * vol[2]).astype(np.float32)
+        m = (rng.uniform(-1, 1, 6) * np.array([2, 2, 2, 0.03, 0.03, 0.03])).astype(np.float32) if mis else None
+        a = O.ref_geometry(pb, m)
+        b = O.reflib_geometry(pb, m)
+        for k in a:
+            assert np.array_equal(np.asarray(a[k]), np.asarray(b[k])), k
+
+    check()
+
+
 def test_fp32_exact_weight_path_agrees_with_fp64():
     rng = np.random.default_rng(0)
     pb = O.make_problem((40, 40, 40), (64, 48), 30, D=150, pw=0.6)
