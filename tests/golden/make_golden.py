@@ -4,8 +4,10 @@ OWN fastcone.py (fastcone.py:260-319) in this container.
     python tests/golden/make_golden.py [/path/to/reference] [all|api]
 
 It also records the signatures of the module's public functions (names, kinds and defaults
-of their parameters, fastcone.py:52, :147, :260, :272, :294, :306) in fastcone_api.json; the
-``api`` argument writes only that file.
+of their parameters, fastcone.py:52, :147, :260, :272, :294, :306) in fastcone_api.json,
+and, in fastcone_calls.json, the C-ABI arguments that its project / backproject pass for
+the calls of api_calls.py (through a recording stand-in for the library); the ``api``
+argument writes only those two files.
 
 Three shims, applied to the imported module only, make it runnable on numpy >= 1.12 without
 touching its code: ``np.zeros`` accepts the float shape the reference builds
@@ -32,7 +34,8 @@ def load_reference(ref_dir):
     spec.loader.exec_module(mod)
     compat = types.ModuleType("numpy_compat")
     compat.__dict__.update(np.__dict__)
-    compat.zeros = lambda shape, *a, **k: np.zeros([int(s) for s in shape], *a, **k)
+    compat.zeros = lambda shape, *a, **k: np.zeros(int(shape) if np.ndim(shape) == 0 else [int(s) for s in shape],
+                                                   *a, **k)
     mod.np = compat
     return mod
 
@@ -64,11 +67,42 @@ def api_signatures(mod):
     return out
 
 
+def record_calls(ref):
+    """Runs the reference's project / backproject on the calls of api_calls.py with a
+    recording stand-in for ctypes.CDLL("libFastcone.so"); returns each call's C-ABI
+    arguments and the proj array afterwards (the projector zeroes column 0)."""
+    import ctypes
+
+    sys.path.insert(0, HERE)
+    import api_calls
+
+    rec = api_calls.Recorder()
+    shim = types.SimpleNamespace(CDLL=lambda name: rec, c_int=ctypes.c_int, c_float=ctypes.c_float,
+                                 POINTER=ctypes.POINTER)
+    real = ref.ctypes
+    ref.ctypes = shim
+    out = []
+    try:
+        for fn, kw in api_calls.calls():
+            vol, proj = api_calls.arrays()
+            rec.calls.clear()
+            getattr(ref, fn)(vol, proj, **kw)
+            (name, args), = rec.calls
+            out.append({"fn": fn, "c_call": api_calls.decode(name, args, vol, proj),
+                        "proj_after": proj.tolist()})
+    finally:
+        ref.ctypes = real
+    return out
+
+
 def write_api(ref):
     import json
 
     with open(os.path.join(HERE, "fastcone_api.json"), "w") as f:
         json.dump(api_signatures(ref), f, indent=1)
+        f.write("\n")
+    with open(os.path.join(HERE, "fastcone_calls.json"), "w") as f:
+        json.dump(record_calls(ref), f)
         f.write("\n")
 
 

@@ -2,9 +2,11 @@
 the reference's fastcone.py (fastcone.py:52, :147, :260, :272, :294, :306) exists here with
 the same parameters in the same order, of the same kinds, with equal defaults (numpy array
 defaults by dtype and values); any parameter added here comes after them and has a default,
-so every call written against the reference binds the same way.  The reference's signatures
-are the committed fixture tests/golden/fastcone_api.json (written by
-tests/golden/make_golden.py from the reference's own module)."""
+so every call written against the reference binds the same way.  And the calls reach the C
+ABI with the arguments the reference's module passes for them.  The reference's signatures
+and recorded C-call arguments are the committed fixtures tests/golden/fastcone_api.json and
+tests/golden/fastcone_calls.json (written by tests/golden/make_golden.py from the
+reference's own module)."""
 import inspect
 import json
 import os
@@ -49,3 +51,36 @@ def test_module_constants_match_reference():
     assert np.dtype(fc.FLOAT_TYPE).name == REF["constants"]["FLOAT_TYPE"]
     assert np.dtype(fc.INT_TYPE).name == REF["constants"]["INT_TYPE"]
 
+
+
+with open(os.path.join(HERE, "golden", "fastcone_calls.json")) as f:
+    CALLS = json.load(f)
+
+
+@pytest.mark.parametrize("idx", range(len(CALLS)))
+def test_c_call_arguments_match_reference(idx, monkeypatch):
+    """The same project / backproject call reaches the C ABI with the arguments the
+    reference's fastcone.py passes (the fixture recorded them through a stand-in library):
+    same entry point, scalars, reversed dimension arrays, offsets, default normalisation and
+    misalignments, pointers to the caller's own vol / proj; and proj afterwards (the
+    projector's column-0 zeroing) is the same."""
+    import sys
+
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import api_calls
+
+    from fastcone_b200 import _lib
+    from fastcone_b200 import fastcone as fc
+
+    rec = api_calls.Recorder()
+    monkeypatch.setattr(fc, "lib", lambda: rec)
+    monkeypatch.setattr(_lib, "check_last", lambda: None)
+    fn, kw = api_calls.calls()[idx]
+    want = CALLS[idx]
+    assert want["fn"] == fn
+    vol, proj = api_calls.arrays()
+    getattr(fc, fn)(vol, proj, **kw)
+    (name, args), = rec.calls
+    got = api_calls.decode(name, args, vol, proj)
+    assert got == want["c_call"]
+    assert proj.tolist() == want["proj_after"]
