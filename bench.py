@@ -382,9 +382,11 @@ class CpuReferencePath:
         from oracle import oracle as O
 
         self.O = O
-        self.pb = O.make_problem(VOL, DET, NVIEWS, D=g.D, pw=g.pw, angles=g.angles, hmid=g.hmid, norm=g.norm)
+        self.vol, self.det, self.nviews = tuple(g.vol_xyz), tuple(g.det_wh), g.nviews
+        self.pb = O.make_problem(self.vol, self.det, self.nviews, D=g.D, pw=g.pw, angles=g.angles, hmid=g.hmid,
+                                 norm=g.norm)
         self.rng = np.random.default_rng(seed)
-        self.proj = self.rng.standard_normal((NVIEWS, DET[1], DET[0]), dtype=np.float32)
+        self.proj = self.rng.standard_normal((self.nviews, self.det[1], self.det[0]), dtype=np.float32)
         self.cores = os.cpu_count() or 1
         self.ncols = 2
 
@@ -393,13 +395,14 @@ class CpuReferencePath:
         import numpy as np
 
         ncols = ncols or self.ncols
-        xy = self.rng.integers(0, VOL[0], size=(ncols, 2))
-        z = np.arange(VOL[2])
-        pts = np.stack([np.repeat(xy[:, 0], VOL[2]), np.repeat(xy[:, 1], VOL[2]), np.tile(z, ncols)], 1)
+        nx, ny, nz = self.vol
+        xy = np.stack([self.rng.integers(0, nx, ncols), self.rng.integers(0, ny, ncols)], 1)
+        z = np.arange(nz)
+        pts = np.stack([np.repeat(xy[:, 0], nz), np.repeat(xy[:, 1], nz), np.tile(z, ncols)], 1)
         pts = pts.astype(np.int32)
         t0 = time.perf_counter()
         self.O.ref_backproject_points(self.pb, self.proj, pts, kernel_mode=2, texq=1)
-        return time.perf_counter() - t0, len(pts) * NVIEWS
+        return time.perf_counter() - t0, len(pts) * self.nviews
 
     def calibrate(self, target_s):
         dt, _ = self.sample(2)
@@ -407,8 +410,9 @@ class CpuReferencePath:
         return self.ncols
 
     def describe(self, dt, upd, nsamples=1):
-        return (f"{nsamples} x {self.ncols} random (x,y) columns x {VOL[2]} z x {NVIEWS} views = {upd:.3g} "
-                f"updates of the 1024^3 / 1440-view FDK, texture-emulating reference path "
+        nx, ny, nz = self.vol
+        return (f"{nsamples} x {self.ncols} random (x,y) columns x {nz} z x {self.nviews} views = {upd:.3g} "
+                f"updates of the {nx}x{ny}x{nz} / {self.nviews}-view FDK, texture-emulating reference path "
                 f"(oracle/fc_oracle.c, {self.cores} threads), {dt:.1f} s")
 
 
