@@ -41,3 +41,21 @@ def test_library_loader_fails_loudly_without_the_build(monkeypatch):
     monkeypatch.setattr(_lib, "LIB_PATH", os.path.join(PKG, "_build", "does_not_exist.so"))
     with pytest.raises(_lib.FastconeError, match="not built"):
         _lib.lib()
+
+
+def test_torch_entry_points_refuse_host_tensors():
+    """The torch API has no CPU path: host tensors are refused before any library call."""
+    import numpy as np
+    import pytest
+    import torch
+
+    from fastcone_b200 import ops
+    from fastcone_b200.geometry import ConeGeometry
+
+    g = ConeGeometry((8, 8, 8), (12, 10), np.linspace(0, 1, 4), 40.0, 1.0)
+    with pytest.raises(ValueError, match="no CPU path"):
+        ops.backproject(torch.zeros(g.proj_shape), g)
+    with pytest.raises(ValueError, match="no CPU path"):
+        ops.project(torch.zeros(g.vol_shape), g)
+    with pytest.raises(ValueError, match="no CPU path"):
+        ops.project_adjoint(torch.zeros(g.proj_shape), g)
