@@ -41,46 +41,163 @@ WORKLOAD = "circular FDK backprojection 1024^3 voxels, 1440 views, 1536x1024 det
 
 
 # DRAM bytes per FDK launch (1024^3, 180 views per launch): ncu dram__bytes_read.sum +
-# dram__bytes_write.sum of every launch of one step of this benchmark (a one-pass capture of
-# `bench.py --steps 1 --warmup 1`), mean over the step's 8 launches; they range from 15.2 GB
-# (views near 0 and 180 degrees) to 68.3 GB (near 90 and 270 degrees), 326 GB per step
-# (profiles/fdk_tma_kernel_fdk-slab.md).
+# dram__bytes_write.sum of every launch of one step of this benchmark, mean over the step's 8
+# launches; they range from 15.2 GB (views near 0 and 180 degrees) to 68.3 GB (near 90 and
+# 270 degrees), 326 GB per step.
 FDK_TRAFFIC_PER_LAUNCH = 40.72e9
 FDK_TRAFFIC_NOTE = "measured by ncu on the 8 launches of one step (mean; 15.2-68.3 GB per launch)"
 
 
-def pi_window_fraction(g, nvox=4096, seed=0):
-    """Fraction of voxel-view pairs inside the Tam-Danielsson window, estimated on random
-    voxels with the window test of the FP64 Katsevich reference (u = sign * w / D, bounds
-    q (pi/2 -+ atan u), q = P / (2 pi) (1 + u^2), lengths in voxels)."""
+def smem_probe(stream, target_s=0.4):
+    """Measured shared-memory load bandwidth of this GPU (fcb_smem_bandwidth: conflict-free
+    ld.shared by every resident thread), for 4-, 8- and 16-byte loads: GB/s of each, from a
+    region of about `target_s` seconds timed with CUDA events."""
+    from fastcone_b200 import _lib
+
+    L = _lib.lib()
+    out = {}
+    for nb in (4, 8, 16):
+        ms, nbytes = ctypes.c_float(), ctypes.c_double()
+        _lib.check(L.fcb_smem_bandwidth(nb, 2000, ctypes.byref(ms), ctypes.byref(nbytes), stream))
+        iters = max(2000, int(2000 * target_s * 1e3 / max(ms.value, 1e-3)))
+        _lib.check(L.fcb_smem_bandwidth(nb, iters, ctypes.byref(ms), ctypes.byref(nbytes), stream))
+        out[f"ld{8 * nb}_GBs"] = nbytes.value / (ms.value / 1e3) / 1e9
+        out[f"ld{8 * nb}_ms"] = ms.value
+    return out
+
+
+def err_stats(got, ref):
+    """Relative L2 and max-abs error of `got` against the FP64 `ref` (the same points), with
+    the largest reference magnitude beside them."""
     import numpy as np
 
-    rng = np.random.default_rng(seed)
-    nz, ny, nx = g.vol_shape
-    xyz = rng.integers(0, [nx, ny, nz], size=(nvox, 3)).astype(np.float64)
-    x = xyz[:, 0:1] - g.vol_xyz[0] // 2
-    y = xyz[:, 1:2] - g.vol_xyz[1] // 2
-    z = xyz[:, 2:3] - g.vol_xyz[2] // 2
-    a = g.angles.astype(np.float64)[None, :]
-    hm = g.hmid.astype(np.float64)[None, :] - g.vol_xyz[2] // 2
-    U = g.D / (g.D + x * np.cos(a) + y * np.sin(a))
-    w = (y * np.cos(a) - x * np.sin(a)) * U
-    h = (z - hm) * U
-    turn = float(g.angles[-1]) - float(g.angles[0])
-    sgn = -1.0 if (turn >= 0) == (g.helical_pitch >= 0) else 1.0
-    u = sgn * w / g.D
-    q = g.helical_pitch / (2 * np.pi) * (1 + u * u)
-    inside = (h <= q * (np.pi / 2 - np.arctan(u))) & (h >= -q * (np.pi / 2 + np.arctan(u)))
-    return float(inside.mean())
+    from oracle import oracle as O
+
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(ref, np.float64)
+    return {"rel_l2": O.rel_l2(got, ref), "max_abs": O.max_abs(got, ref), "ref_max_abs": float(np.abs(ref).max())}
 
 
-def smem_roofline(gather_gbs, clocks):
-    """The binding ceiling of the FDK kernel: 4 ld.shared per voxel-view update, one 128-byte
-    wavefront per warp instruction -> 128 B/clk/SM of gather bytes on 148 SMs."""
-    mhz = clocks.get("sm_mhz") or 1965.0
-    peak = 128.0 * 148 * mhz * 1e6 / 1e9
-    return {"bound": "smem", "achieved": gather_gbs, "peak": peak, "unit": "GB/s", "frac": gather_gbs / peak,
-            "clock_mhz": mhz, "note": "peak = 128 B/clk/SM x 148 SMs x median sampled SM clock"}
+def _gather(vol, pts, g):
+    """GPU volume values at global voxel indices pts (rows x, y, z) of geometry g's sub-volume."""
+    import torch
+
+    s = g.vol_start
+    t = torch.from_numpy(pts.astype("int64")).to(vol.device)
+    return vol[t[:, 2] - s[2], t[:, 1] - s[1], t[:, 0] - s[0]].double().cpu().numpy()
+
+
+def oracle_problem(g):
+    """The oracle's description of geometry g, with the same FP32 distances the library gets."""
+    import numpy as np
+
+    from oracle import oracle as O
+
+    return O.make_problem(g.vol_xyz, g.det_wh, g.nviews, D=float(np.float32(g.D)), pw=float(np.float32(g.pw)),
+                          angles=g.angles, hmid=g.hmid, norm=g.norm, volStart=g.vol_start, volEnd=g.vol_end,
+                          woff=g.woff, hoff=g.hoff, whsize=g.window_wh)
+
+
+def fdk_parity(dev, ncols=256, seed=11, nellip=50):
+    """Error of the large circular FDK backprojection (1024^3, 1440 views, 1536x1024) against
+    the FP64 oracle, with FP32- and with BF16-stored filtered projections (FP32 accumulation
+    both): a seeded 50-ellipsoid phantom projected by the explicit projector, cosine-weighted
+    and Shepp-Logan filtered on the GPU, backprojected over the whole volume; `ncols` random
+    full-z voxel columns are compared with the oracle's FP64 backprojection of the same FP32
+    filtered projections."""
+    import numpy as np
+    import torch
+
+    from fastcone_b200 import _lib, ops
+    from fastcone_b200.phantom import random_ellipsoids
+    from oracle import oracle as O
+
+    g = geometry()
+    vol = ops.phantom(g.vol_xyz, random_ellipsoids(nellip, g.vol_xyz, seed), device=dev)
+    proj = ops.ProjectPlan(g.with_norm(np.ones(g.nviews, np.float32)), _lib.PROJ_EXPLICIT)(vol)
+    del vol
+    ops.FilterPlan(g.proj_shape, window=_lib.FILTER_SHEPPLOGAN)(proj, zorigin=g.hmid, D=g.D, out=proj)
+    pts = O.column_points(g.vol_xyz, g.vol_start, g.vol_end, ncols, seed)
+    res = {"workload": f"{WORKLOAD}; seeded {nellip}-ellipsoid phantom, explicit projector, cosine weight + "
+                       f"Shepp-Logan filter; {ncols} random full-z voxel columns vs the FP64 oracle",
+           "points": int(len(pts))}
+    got = {}
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+        p = proj if dt == torch.float32 else proj.to(dt)
+        v = torch.zeros(g.vol_shape, device=dev)
+        ops.BackprojectPlan(g, mode=_lib.MODE_FDK, dtype=dt)(p, v)
+        ops.sync_status()
+        got[name] = _gather(v, pts, g)
+        del v, p
+    proj_h = proj.cpu().numpy()
+    del proj
+    torch.cuda.empty_cache()
+    ref = O.backproject_points_f64(oracle_problem(g), proj_h, pts, kernel_mode=2)
+    for name in got:
+        res[name] = err_stats(got[name], ref)
+    return res
+
+
+def helix_parity(dev, ncols=128, seed=12, nellip=20):
+    """Error of the helical Katsevich reconstruction's PI-window backprojection (512x512x384,
+    4 turns x 1160 views, 736x64) against the FP64 oracle: a seeded phantom projected by the
+    explicit projector along the helix, Katsevich-filtered on the GPU, backprojected with
+    weight U over each voxel's PI interval; `ncols` random full-z columns compared with the
+    oracle's FP64 PI-window backprojection of the same filtered projections, and their
+    in-window voxel-view pairs counted by the oracle and by fcb_katsevich_pi_pairs."""
+    import dataclasses
+
+    import numpy as np
+    import torch
+
+    from fastcone_b200 import _lib, configs, ops
+    from fastcone_b200.phantom import random_ellipsoids
+    from oracle import oracle as O
+
+    gk = configs.helical_katsevich(pi_window=True)
+    vol = ops.phantom(gk.vol_xyz, random_ellipsoids(nellip, gk.vol_xyz, seed), device=dev)
+    proj = ops.ProjectPlan(gk, _lib.PROJ_EXPLICIT)(vol)
+    del vol
+    pf = ops.KatsevichPlan(gk)(proj)
+    del proj
+    dlam = (float(gk.angles[-1]) - float(gk.angles[0])) / (gk.nviews - 1)
+    g = dataclasses.replace(gk, norm=np.full(gk.nviews, abs(dlam) / (2 * math.pi * gk.D), np.float32))
+    v = torch.zeros(g.vol_shape, device=dev)
+    ops.BackprojectPlan(g, mode=_lib.MODE_KATSEVICH)(pf, v)
+    ops.sync_status()
+    pts = O.column_points(g.vol_xyz, g.vol_start, g.vol_end, ncols, seed)
+    got = _gather(v, pts, g)
+    ref, pairs = O.katsevich_piwin_points_f64(oracle_problem(g), pf.cpu().numpy(), pts, g.helical_pitch)
+    # the same columns' pairs counted on the GPU, one single-column sub-volume at a time
+    nz = g.vol_xyz[2]
+    gpu_pairs = 0
+    for c in range(ncols):
+        x, y = int(pts[c * nz, 0]), int(pts[c * nz, 1])
+        gpu_pairs += pi_pairs(dataclasses.replace(g, vol_start=(x, y, 0), vol_end=(x + 1, y + 1, nz)))
+    # the largest contribution one view can make to a voxel (U at the volume's widest radius):
+    # the kernel decides the window edge in FP32, the oracle in FP64, so a voxel whose edge
+    # falls within rounding of a view may gain or lose that view at its entry and its exit
+    nx, ny = g.vol_xyz[0], g.vol_xyz[1]
+    umax = g.D / (g.D - math.hypot(nx / 2, ny / 2))
+    one_view = float(np.abs(g.norm).max()) * umax * float(pf.abs().max())
+    return {"workload": f"helical 512x512x384, 4 turns x 1160 views, 736x64; seeded {nellip}-ellipsoid "
+                        f"phantom, explicit projector, Katsevich filter, PI-window backprojection; {ncols} "
+                        f"random full-z voxel columns vs the FP64 oracle",
+            "points": int(len(pts)), "f32": err_stats(got, ref), "one_view_max": one_view,
+            "pi_pairs_oracle": pairs, "pi_pairs_gpu": gpu_pairs}
+
+
+def pi_pairs(g):
+    """Exact number of voxel-view pairs of geometry g inside the PI window (on the GPU)."""
+    import torch
+
+    from fastcone_b200 import _lib
+
+    s = g.struct()
+    n = ctypes.c_longlong()
+    _lib.check(_lib.lib().fcb_katsevich_pi_pairs(ctypes.byref(s), ctypes.byref(n),
+                                                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    return int(n.value)
 
 
 def parse():
@@ -92,9 +209,13 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
-    ap.add_argument("--shard", default="replicas", choices=["replicas", "z"],
-                    help="N>1: independent volumes per rank (weak scaling) or one volume in z-slabs "
-                         "(strong scaling)")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the error measurement against the FP64 oracle at the headline and helical sizes")
+    ap.add_argument("--shard", default=None, choices=["replicas", "z", "slabs"],
+                    help="replicas: every rank reconstructs its own volume (weak scaling; the default "
+                         "for one GPU); slabs: one volume in z-slabs, the views spread over the ranks and "
+                         "exchanged as detector-row bands by an NCCL all-to-all (strong scaling; the "
+                         "default for N > 1); z: one volume in z-slabs, every rank holding all views")
     ap.add_argument("--case", default=None,
                     choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "conv-256", "katsevich", "pipeline",
                              "misaligned-256"],
@@ -460,6 +581,109 @@ def run_reference(args, rank, world):
     print(json.dumps(reference_line(args, geometry())), flush=True)
 
 
+def run_slabs(args, rank, world, local):
+    """One 1024^3 volume over `world` GPUs (fastcone_b200.slabs, the mpi_fastcone.backproject
+    replacement): rank r holds views [1440 r / N, 1440 (r + 1) / N) and owns z-slab r; a step
+    is one slabs.backproject -- pack every view's detector-row bands for the slabs they
+    reach, one NCCL all-to-all, unpack, backproject the slab (a plan made once per rank).
+    value = the volume's voxel-view updates / the slowest rank's step time (strong scaling)."""
+    import numpy as np
+    import torch
+
+    from fastcone_b200 import _lib, ops, slabs
+    from fastcone_b200 import dist as fd
+
+    # NCCL's communicator log (one line per rank with nranks) on stderr
+    os.environ.setdefault("NCCL_DEBUG", "INFO")
+    os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    fd.init("nccl", device=dev)
+    g = geometry()
+    dec = slabs.SlabDecomposition(g, world)
+    v0, v1 = dec.views(rank)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    proj = torch.randn((v1 - v0, DET[1], DET[0]), device=dev, generator=gen)
+    vol = torch.zeros(dec.slab_shape(rank), device=dev)
+    gb = dec.band_geometry(rank)
+    plan = ops.BackprojectPlan(gb, mode=_lib.MODE_FDK) if gb is not None else None
+    local_op = lambda band, geom, mode, v: plan(band, v)  # noqa: E731
+
+    def step():
+        slabs.backproject(proj, dec, rank, _lib.MODE_FDK, vol, local_op=local_op)
+
+    for _ in range(args.warmup):
+        step()
+    ops.sync_status()
+    torch.cuda.synchronize()
+    fd.barrier()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        fd.barrier()
+        e0.record(st)
+        for _ in range(args.steps):
+            step()
+        e1.record(st)
+        torch.cuda.synchronize()
+        fd.barrier()
+    ops.sync_status()
+    ms_step = fd.max_over_ranks(e0.elapsed_time(e1), dev) / args.steps
+    updates = VOL[0] * VOL[1] * VOL[2] * NVIEWS
+    value = updates / (ms_step / 1e3) / 1e9
+    band_bytes = sum(dec.split_sizes(s_, d) for s_ in range(world) for d in range(world) if s_ != d) * 4
+    launches = plan.info()["launches"] if plan is not None else 0
+    my_updates = int(np.prod(dec.slab_shape(rank))) * (len(dec.bands[rank].views))
+
+    # end to end: this rank's views from pinned host memory, the slab back to the host
+    hproj = torch.empty(proj.shape, dtype=torch.float32, pin_memory=True)
+    hproj.copy_(proj)
+    hvol = torch.zeros(vol.shape, dtype=torch.float32, pin_memory=True)
+    times = []
+    for _ in range(max(3, args.steps // 2)):
+        fd.barrier()
+        t0 = time.perf_counter()
+        proj.copy_(hproj, non_blocking=True)
+        step()
+        hvol.copy_(vol, non_blocking=True)
+        torch.cuda.synchronize()
+        fd.barrier()
+        times.append(time.perf_counter() - t0)
+    dt = fd.max_over_ranks(float(np.median(times)), dev)
+    e2e = {"value": updates / dt / 1e9, "unit": UNIT, "h2d_bytes_per_step": hproj.numel() * 4,
+           "d2h_bytes_per_step": hvol.numel() * 4, "ms_per_step": dt * 1e3,
+           "statistic": f"median of {len(times)} steps, slowest rank",
+           "path": "slabs.backproject with this rank's views copied in from pinned host memory and its slab "
+                   "copied out (sizes per rank)"}
+    cpu = cpu_baseline(g) if rank == 0 and world == 1 and not args.no_cpu else None
+    hbm, _ = measured_peaks()
+    ach = FDK_BYTES_PER_UPDATE["f32"] * my_updates / (ms_step / 1e3) / 1e9
+    clocks = clk.summary()
+    del plan
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "parallelism": f"z-slabs x{world}, views spread over the ranks, one "
+                                                        f"NCCL all-to-all of detector-row bands per step",
+                   "inputs": "each rank's views resident in HBM (value); pinned host buffers (e2e)",
+                   "band_bytes_exchanged_per_step": band_bytes,
+                   "l2": "inputs larger than L2; no flush"},
+        "gpu_launches": launches * args.steps,
+        "roofline": {"bound": "smem", "achieved": ach, "peak": None, "unit": "GB/s", "frac": None,
+                     "traffic": None, "note": "rank 0's gather bytes (16 B/update) / step time; the "
+                                              "single-GPU line measures the peak and the fraction"},
+        "hbm_peak": hbm, "clocks": clocks, "e2e": e2e, "cpu_baseline": cpu}), flush=True)
+
+
 def main():
     args = parse()
     from fastcone_b200.dist import env_ranks
@@ -470,6 +694,11 @@ def main():
         return
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.shard is None:
+        args.shard = "slabs" if world > 1 else "replicas"
+    if args.shard == "slabs":
+        run_slabs(args, rank, world, local)
         return
     import numpy as np
     import torch
@@ -534,11 +763,18 @@ def main():
     hbm, peak_kind = measured_peaks()
     # per launch: the step's launches split the views; bytes and time both scale with views
     achieved = FDK_BYTES_PER_UPDATE["f32"] * updates / (ms_step / 1e3) / 1e9
+    ms_launch = ms_step / launches_per_step
 
-    # BF16-stored filtered projections (same kernel family, 2-byte gathers)
+    # the binding ceiling, measured on this GPU: conflict-free 32-bit shared-memory loads
+    with ClockSampler(local) as clk_probe:
+        probe = smem_probe(ctypes.c_void_p(st.cuda_stream))
+    probe["clocks"] = clk_probe.summary()
+    smem_peak = probe["ld32_GBs"]
+
+    # BF16-stored filtered projections (same kernel family; taps read as 32-bit pairs)
     proj16 = proj.to(torch.bfloat16)
     plan16 = ops.BackprojectPlan(g, mode=_lib.MODE_FDK, dtype=torch.bfloat16)
-    for _ in range(2):
+    for _ in range(max(2, args.warmup)):
         plan16(proj16, vol)
     torch.cuda.synchronize()
     e0.record(st)
@@ -549,6 +785,7 @@ def main():
     torch.cuda.synchronize()
     ops.sync_status()
     ms16 = barrier_max(e0.elapsed_time(e1)) / k16
+    ach16 = FDK_BYTES_PER_UPDATE["bf16"] * updates / (ms16 / 1e3) / 1e9
     del proj16, plan16
 
     # secondary: forward projector Gsamples/s on 256^3, 360 views, 384 x 256
@@ -618,12 +855,21 @@ def main():
     ms_kf = barrier_max(e0.elapsed_time(e1)) / kk
     del fk, kfp
     dense = gk.vol_shape[0] * gk.vol_shape[1] * gk.vol_shape[2] * gk.nviews
-    frac = pi_window_fraction(gk)
+    pairs = pi_pairs(gk)  # exact, FP64, on the GPU (fcb_katsevich_pi_pairs)
     katsevich = {"workload": "helical 512x512x384, 4 turns x 1160 views, 736x64 detector, PI window",
-                 "ms_per_pass": ms_k, "filter_ms": ms_kf, "dense_GUPS": dense / (ms_k / 1e3) / 1e9,
-                 "pi_window_pairs_fraction": frac, "pi_window_GUPS": frac * dense / (ms_k / 1e3) / 1e9,
-                 "launches": kplan.info()["launches"]}
+                 "ms_per_pass": ms_k, "filter_ms": ms_kf, "dense_pairs": dense,
+                 "dense_equivalent_GUPS": dense / (ms_k / 1e3) / 1e9, "pi_window_pairs": pairs,
+                 "pi_window_GUPS": pairs / (ms_k / 1e3) / 1e9, "launches": kplan.info()["launches"]}
     del pk, vk, kplan
+
+    # parity at the headline and helical configurations (after every timed region): the
+    # oracle is only the checker here
+    parity = None
+    if rank == 0 and not args.no_parity:
+        del proj, vol
+        torch.cuda.empty_cache()
+        parity = {"fdk_1024": fdk_parity(dev), "katsevich_helix": helix_parity(dev)}
+        torch.cuda.empty_cache()
 
     # learned unrolled reconstruction vs SIRT-100 (committed weights), two held-out phantoms
     learned_res = None
@@ -633,26 +879,39 @@ def main():
 
         net = learned.UnrolledNet().to(dev)
         net.load_state_dict(torch.load(wpath, map_location=dev)["model"])
-        r = learned.evaluate(net, configs.learned_sparse(), seeds=[1, 2], sirt_iters=100)
-        mean = lambda k: sum(x[k] for x in r) / len(r)  # noqa: E731
-        sp = [x["speedup_to_sirt_psnr"] for x in r]
+
+        def summary(r, what):
+            mean = lambda k: sum(x[k] for x in r) / len(r)  # noqa: E731
+            return {
+                "phantoms": what,
+                "sirt100_psnr": mean("sirt_psnr"), "sirt100_ssim": mean("sirt_ssim"), "sirt100_s": mean("sirt_time_s"),
+                "learned_psnr": mean("learned_psnr"), "learned_ssim": mean("learned_ssim"),
+                "learned_s": mean("learned_time_s"), "fdk_psnr": mean("fdk_psnr"),
+                "fallback_psnr": mean("no_net_psnr"),
+                "time_to_sirt100_psnr_s": [x["time_to_sirt_psnr_s"] for x in r],
+                "speedup_to_sirt100_psnr": [x["speedup_to_sirt_psnr"] for x in r],
+            }
+
+        gl = configs.learned_sparse()
+        r_in = learned.evaluate(net, gl, seeds=[1, 2], sirt_iters=100)
+        r_out = learned.evaluate(net, gl, seeds=[3, 4], sirt_iters=100, dist=learned.OUT_OF_DISTRIBUTION)
         learned_res = {
-            "workload": "256^3, 90 views, 384x256, Poisson I0=1e4; 8 unrolled steps vs SIRT-100 from zero",
-            "sirt100_psnr": mean("sirt_psnr"), "sirt100_ssim": mean("sirt_ssim"), "sirt100_s": mean("sirt_time_s"),
-            "learned_psnr": mean("learned_psnr"), "learned_ssim": mean("learned_ssim"),
-            "learned_s": mean("learned_time_s"), "fdk_psnr": mean("fdk_psnr"),
-            "fallback_psnr": mean("no_net_psnr"),
-            "time_to_sirt100_psnr_s": [x["time_to_sirt_psnr_s"] for x in r],
-            "speedup_to_sirt100_psnr": sp,
+            "workload": "256^3, 90 views, 384x256; 8 unrolled steps vs SIRT-100 from zero; each method timed "
+                        "as the median of 3 passes after one untimed pass (CUDA events)",
+            "in_distribution": summary(r_in, "training distribution, held-out seeds 1, 2: 10 ellipsoids, "
+                                             "densities U(0.1, 1), Poisson I0 = 1e4"),
+            "out_of_distribution": summary(r_out, "seeds 3, 4: 30 ellipsoids, densities U(0.5, 1.5), "
+                                                  "Poisson I0 = 5e3"),
         }
         del net
         torch.cuda.empty_cache()
 
     # end to end through the reference-facing C entry point, pinned host buffers
     e2e = None
+    if parity is None:
+        del proj, vol
+    torch.cuda.empty_cache()
     if not args.no_e2e:
-        del proj
-        torch.cuda.empty_cache()
         hproj = torch.empty((NVIEWS, DET[1], DET[0]), dtype=torch.float32, pin_memory=True)
         hproj.normal_(generator=torch.Generator().manual_seed(7))
         hvol = torch.zeros(g.vol_shape, dtype=torch.float32, pin_memory=True)
@@ -689,6 +948,31 @@ def main():
                "calls_ms": [round(t * 1e3, 1) for t in times], "statistic": f"median of {ke} calls",
                "path": "GPU_CB_K_backproject (C ABI), pinned host buffers"}
 
+        # the reference's whole FDK path, fastcone.fbp (cosine weight + Shepp-Logan filter +
+        # backprojection, the filtered projections returned into the caller's array), through
+        # the C entry point fcb_fbp_host with the same pinned buffers
+        gs = g.struct()
+
+        def fbp_call():
+            _lib.check(L.fcb_fbp_host(local, ctypes.byref(gs), _lib.FILTER_SHEPPLOGAN, ctypes.c_float(g.D),
+                                      fp(g.hmid), 1, ctypes.c_void_p(hproj.data_ptr()),
+                                      ctypes.c_void_p(hvol.data_ptr())))
+
+        fbp_call()
+        barrier()
+        times = []
+        for _ in range(ke):
+            t0 = time.perf_counter()
+            fbp_call()
+            times.append(time.perf_counter() - t0)
+        dt = barrier_max(float(np.median(times)))
+        e2e["fbp"] = {"value": job_updates / dt / 1e9, "unit": UNIT,
+                      "h2d_bytes_per_step": hproj.numel() * 4 + hvol.numel() * 4,
+                      "d2h_bytes_per_step": hproj.numel() * 4 + hvol.numel() * 4, "ms_per_step": dt * 1e3,
+                      "calls_ms": [round(t * 1e3, 1) for t in times], "statistic": f"median of {ke} calls",
+                      "path": "fcb_fbp_host (C ABI; fastcone.fbp): cosine weight + Shepp-Logan filter on the GPU, "
+                              "filtered views back into the host array, FDK backprojection; pinned host buffers"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(g)
@@ -710,14 +994,27 @@ def main():
                    "l2": "inputs (13.4 GB) larger than L2; no flush", "box": [info["box_w"], info["box_h"]],
                    "parallelism": parallelism},
         "gpu_launches": launches_per_step * args.steps,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": round(FDK_TRAFFIC_PER_LAUNCH),
-                     "note": f"achieved = 16 B/update bilinear gather bytes per launch / launch time "
-                             f"(CUDA events); peak = {peak_kind} HBM copy bandwidth. frac > 1: the gathers "
-                             f"are served from shared memory (TMA-staged boxes), see smem_roofline; "
-                             f"traffic = DRAM bytes per launch, {FDK_TRAFFIC_NOTE}"},
-        "smem_roofline": smem_roofline(achieved, clk_summary),
-        "bf16_storage": {"value": job_updates / (ms16 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms16},
+        "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+                     "frac": achieved / smem_peak, "traffic": round(FDK_TRAFFIC_PER_LAUNCH),
+                     "kernel": "fdk_tma_kernel<float,32,0,1,3>",
+                     "note": f"achieved = 16 B/update (4 FP32 taps, each a 32-bit ld.shared from the "
+                             f"TMA-staged box) x {updates // launches_per_step} updates per launch / the "
+                             f"launch's mean CUDA-event time ({ms_launch:.1f} ms, {launches_per_step} "
+                             f"launches per step); peak = 32-bit shared-memory load bandwidth measured "
+                             f"in this run (fcb_smem_bandwidth, see smem_probe); traffic = DRAM bytes per "
+                             f"launch, {FDK_TRAFFIC_NOTE}"},
+        "hbm": {"achieved": FDK_TRAFFIC_PER_LAUNCH / (ms_launch / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                "frac": FDK_TRAFFIC_PER_LAUNCH / (ms_launch / 1e3) / 1e9 / hbm,
+                "compulsory_bytes_per_step": (NVIEWS * DET[0] * DET[1] + 2 * launches_per_step * updates // NVIEWS) * 4,
+                "note": f"DRAM bytes per launch (ncu) / launch time against the {peak_kind} HBM copy "
+                        f"bandwidth; the gathers are served from shared memory, HBM is not the bound"},
+        "smem_probe": probe,
+        "bf16_storage": {"value": job_updates / (ms16 / 1e3) / 1e9, "unit": UNIT, "ms_per_step": ms16,
+                         "roofline": {"bound": "smem", "achieved": ach16, "peak": smem_peak, "unit": "GB/s",
+                                      "frac": ach16 / smem_peak,
+                                      "note": "8 B/update: two 32-bit ld.shared of tap pairs (BF16 (w, w+1) "
+                                              "per row)"}},
+        "error_vs_fp64": parity,
         "fwd_proj": {"unit": "Gsamples/s", "samples_per_pass": nsamp,
                      "workload": "256^3, 360 views, 384x256 detector",
                      **{k: v for k, v in proj_res.items()}},

@@ -50,6 +50,7 @@ EXPORTED_SYMBOLS = [
     "fcb_filter_plan_destroy",
     "fcb_katsevich_plan_create", "fcb_katsevich_plan_execute", "fcb_katsevich_plan_destroy",
     "fcb_detector_rows",
+    "fcb_bp_plan_set_test_stall", "fcb_katsevich_pi_pairs", "fcb_smem_bandwidth", "fcb_fbp_host",
 ]
 
 
@@ -138,6 +139,11 @@ def lib():
             L.fcb_katsevich_plan_execute.argtypes = [vp, vp, vp, vp]
             L.fcb_katsevich_plan_destroy.argtypes = [vp]
             L.fcb_detector_rows.argtypes = [gp, ctypes.c_int, c_int_p, c_int_p]
+            L.fcb_bp_plan_set_test_stall.argtypes = [vp, ctypes.c_int, ctypes.c_ulonglong]
+            L.fcb_katsevich_pi_pairs.argtypes = [gp, ctypes.POINTER(ctypes.c_longlong), vp]
+            L.fcb_smem_bandwidth.argtypes = [ctypes.c_int, ctypes.c_longlong, c_float_p, c_double_p, vp]
+            L.fcb_fbp_host.argtypes = [ctypes.c_int, gp, ctypes.c_int, ctypes.c_float, c_float_p, ctypes.c_int,
+                                       vp, vp]
             _lib = L
     return _lib
 

@@ -25,6 +25,7 @@ SOURCES = [
     "fcb_filter.cu",
     "fcb_katsevich.cu",
     "fcb_conv.cu",
+    "fcb_probe.cu",
     "fcb_capi.cpp",
 ]
 

@@ -21,7 +21,6 @@
 #include <string.h>
 
 #include <algorithm>
-#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -61,6 +60,13 @@ struct FdkParams {
   float td_a;                   // window half-height scale P / (2 pi pw), pixels
   float td_r;                   // source-axis distance in pixels (D / pw)
   float td_sign;                // +1/-1: sense of the helix relative to the w axis
+  // Bounded waits.  cwait_ns limits each consumer wait for a staged view (2 s by default).
+  // stop_after >= 0 is a test hook: the producer stages only that many views, drains its
+  // copies and leaves, so the consumers' next wait runs out and the kernel reports
+  // DEV_TIMEOUT without any copy still in flight.
+  unsigned long long cwait_ns;
+  int stop_after;
+  int pbufs;                    // 16-bit storage: tap-pair buffers (fdk_pair_kernel)
   FdkView v[FDK_MAXV];
 };
 
@@ -197,23 +203,40 @@ struct Tap<__nv_bfloat16, OFF> {
   static __device__ __forceinline__ float ld(uint32_t a) { return __uint_as_float(lds_u16<OFF * 2>(a) << 16); }
 };
 
-// ---- 16-bit staged boxes widened to FP32 (8 values per 16-byte load)
-template <typename T>
-__device__ __forceinline__ float wide16(uint32_t bits16);
-template <>
-__device__ __forceinline__ float wide16<__nv_bfloat16>(uint32_t b) { return __uint_as_float(b << 16); }
-template <>
-__device__ __forceinline__ float wide16<__half>(uint32_t b)
+// ---- 16-bit tap pairs: a staged 16-bit box rewritten as 32-bit words, word (r, c) holding
+// tap (r, c) in its low half and tap (r, c + 1) in its high half, so that one 32-bit
+// ld.shared gives both horizontal taps of a row
+template <int OFF>
+__device__ __forceinline__ uint32_t lds_b32(uint32_t a)
 {
-  return __half2float(__ushort_as_half((unsigned short)b));
+  uint32_t v;
+  asm volatile("ld.shared.b32 %0, [%1+%2];" : "=r"(v) : "r"(a), "n"(OFF));
+  return v;
 }
 template <typename T>
-__device__ __forceinline__ void widen8(uint4 q, float4& lo, float4& hi)
+struct PairTap;
+template <>
+struct PairTap<__nv_bfloat16> {
+  static __device__ __forceinline__ float lo(uint32_t w) { return __uint_as_float(w << 16); }
+  static __device__ __forceinline__ float hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
+};
+template <>
+struct PairTap<__half> {
+  static __device__ __forceinline__ float lo(uint32_t w)
+  {
+    return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
+  }
+  static __device__ __forceinline__ float hi(uint32_t w)
+  {
+    return __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+  }
+};
+// 8 staged 16-bit taps q (columns c .. c+7) and the first two of the next 16-byte chunk
+// (nx) -> the pair words of columns c .. c+7
+__device__ __forceinline__ void pair8(uint4 q, uint32_t nx, uint4& lo, uint4& hi)
 {
-  lo = make_float4(wide16<T>(q.x & 0xffffu), wide16<T>(q.x >> 16), wide16<T>(q.y & 0xffffu),
-                   wide16<T>(q.y >> 16));
-  hi = make_float4(wide16<T>(q.z & 0xffffu), wide16<T>(q.z >> 16), wide16<T>(q.w & 0xffffu),
-                   wide16<T>(q.w >> 16));
+  lo = make_uint4(q.x, __byte_perm(q.x, q.y, 0x5432), q.y, __byte_perm(q.y, q.z, 0x5432));
+  hi = make_uint4(q.z, __byte_perm(q.z, q.w, 0x5432), q.w, __byte_perm(q.w, nx, 0x5432));
 }
 
 // ---- packed FP32 pairs (sm_100 f32x2 arithmetic): two z-voxels per instruction
@@ -263,11 +286,10 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
 {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int ES = (int)sizeof(T);
-  // 16-bit storage with the pair path: each staged box is widened into one of two FP32
-  // buffers by the consumers, which then interpolate exactly as for FP32 storage
-  constexpr bool CVT = X2 && ES == 2;
-  using TC = typename std::conditional<CVT, float, T>::type;
-  constexpr int ESC = (int)sizeof(TC);
+  // voxel pairs (X2) read FP32 taps; 16-bit storage runs fdk_pair_kernel, or this kernel's
+  // one-tap-at-a-time path (X2 = false) for comparison
+  static_assert(!X2 || ES == 4, "16-bit voxel pairs run in fdk_pair_kernel");
+  constexpr int ESC = ES;  // bytes per position of the box the taps are read from
   const int stage_elems = P.BW * P.BH;
   const int stage_bytes = ((stage_elems * ES) + 127) & ~127;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)P.stages * stage_bytes);
@@ -275,8 +297,6 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   // per stage: box origin w, h; view (-1: end of the list); rows the tile's footprint needs
   int4* origin = reinterpret_cast<int4*>(empty + P.stages);
   const uint32_t smem_base = dev::smem_u32(smem_raw);
-  const int fbuf_bytes = ((stage_elems * 4) + 127) & ~127;
-  const size_t fbuf_off = ((size_t)P.stages * stage_bytes + (size_t)P.stages * 32 + 127) & ~(size_t)127;
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int tx, ty, tz;
@@ -295,12 +315,12 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
     // ------------------------------------------------------------- producer warp
     const uint32_t bytes = (uint32_t)(stage_elems * ES);
     int issued = 0;  // staged views so far (= ring position)
-    bool failed = false;
+    bool failed = false, stalled = false;
     if constexpr (PIW) {
       // the whole warp tests 32 views at a time against the PI window (most views miss a
       // tile of a helical scan); lane 0 stages the ones that reach it, in view order
       if (lane == 0) dev::tma_prefetch(&tmap);
-      for (int vb = 0; vb < P.nviews && !failed; vb += 32) {
+      for (int vb = 0; vb < P.nviews && !failed && !stalled; vb += 32) {
         const int v = vb + lane;
         int w0 = 0, h0 = 0, nw = 0, nh = 0;
         bool need = false;
@@ -311,6 +331,10 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         }
         unsigned mask = __ballot_sync(0xffffffffu, need);
         while (mask) {
+          if (issued == P.stop_after) {  // test hook (uniform over the warp)
+            stalled = true;
+            break;
+          }
           const int l = __ffs(mask) - 1;
           mask &= mask - 1;
           const int sw0 = __shfl_sync(0xffffffffu, w0, l), sh0 = __shfl_sync(0xffffffffu, h0, l);
@@ -340,6 +364,10 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
       if (lane != 0) return;
       dev::tma_prefetch(&tmap);
       for (int v = 0; v < P.nviews; v++) {
+        if (v == P.stop_after) {  // test hook
+          stalled = true;
+          break;
+        }
         int w0, h0, nw, nh;
         fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, w0, h0, nw, nh);
         const int s = issued % P.stages;
@@ -356,7 +384,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         issued++;
       }
     }
-    if (PIW && !failed) {
+    if (PIW && !failed && !stalled) {
       // end of the view list: a slot whose phase completes without data, view -1
       const int s = issued % P.stages;
       if (issued < P.stages || dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
@@ -366,8 +394,8 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         failed = true;
       }
     }
-    if (failed) {
-      dev::record_status(P.status, DEV_TIMEOUT);
+    if (failed || stalled) {
+      if (failed) dev::record_status(P.status, DEV_TIMEOUT);
       // drain: wait (bounded) for the copies still in flight before leaving
       for (int j = max(0, issued - P.stages); j < issued; j++)
         dev::mbar_wait(&full[j % P.stages], (j / P.stages) & 1, 100000000ull);
@@ -398,53 +426,13 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   // window: only views that reach the tile, then an end marker)
   for (int j = 0; PIW || j < P.nviews; j++) {
     const int s = j % P.stages;
-    bool okw = dev::mbar_wait(&full[s], (j / P.stages) & 1);
-    if constexpr (!CVT) {
-      if (!okw) {
-        dev::record_status(P.status, DEV_TIMEOUT);
-        return;
-      }
+    if (!dev::mbar_wait(&full[s], (j / P.stages) & 1, P.cwait_ns)) {
+      dev::record_status(P.status, DEV_TIMEOUT);
+      return;
     }
     const int4 org = origin[s];
     const int v = PIW ? org.z : j;
-    if (!CVT && PIW && v < 0) break;
-    uint32_t fbase = 0;
-    if constexpr (CVT) {
-      // widen the staged 16-bit box into FP32 buffer j & 1 (16-byte chunks: 8 values), free
-      // the stage for the producer, and meet the other consumer warps; the barrier also
-      // makes the outcome of the wait uniform (a warp that timed out leaves with the rest)
-      float* fb = reinterpret_cast<float*>(smem_raw + fbuf_off + (size_t)(j & 1) * fbuf_bytes);
-      const bool real = okw && !(PIW && v < 0);  // the end marker has no data
-      if (real) {
-        const uint4* src = reinterpret_cast<const uint4*>(smem_raw + (size_t)s * stage_bytes);
-        float4* dst = reinterpret_cast<float4*>(fb);
-        // only the rows this tile's footprint reaches (taps stay below row org.w - 1)
-        const int nconv = min(org.w, P.BH) * (P.BW / 8);
-        for (int e = threadIdx.x; e < nconv; e += FDK_CWARPS * 32) {
-          float4 lo, hi;
-          widen8<T>(src[e], lo, hi);
-          dst[2 * e] = lo;
-          dst[2 * e + 1] = hi;
-        }
-      }
-      __syncwarp();
-      if (lane == 0 && real) dev::mbar_arrive(&empty[s]);
-      int all_ok;
-      asm volatile(
-          "{\n\t.reg .pred p, q;\n\t"
-          "setp.ne.u32 p, %1, 0;\n\t"
-          "bar.red.and.pred q, 1, %2, p;\n\t"
-          "selp.u32 %0, 1, 0, q;\n\t}"
-          : "=r"(all_ok)
-          : "r"((uint32_t)okw), "n"(FDK_CWARPS * 32)
-          : "memory");
-      if (!all_ok) {
-        dev::record_status(P.status, DEV_TIMEOUT);
-        return;
-      }
-      if (PIW && v < 0) break;
-      fbase = dev::smem_u32(fb);
-    }
+    if (PIW && v < 0) break;
     const FdkView& V = P.v[v];
 
     const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
@@ -478,8 +466,8 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
     }
 
     // byte address of tap (row r, column iw) = bits(MAGIC + r) * rowb + base
-    const uint32_t base = (CVT ? fbase : smem_base + (uint32_t)s * (uint32_t)stage_bytes) +
-                          (uint32_t)iw * ESC - MAGIC_BITS * rowb;
+    const uint32_t base = smem_base + (uint32_t)s * (uint32_t)stage_bytes + (uint32_t)iw * ESC -
+                          MAGIC_BITS * rowb;
     if constexpr (X2) {
       const u64 MAG2 = pk2(MAGIC, MAGIC);
       const u64 FW2 = pk2(fw, fw);
@@ -495,10 +483,10 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         const uint32_t a0 = (uint32_t)__float_as_uint(t0) * rowb + base;
         const uint32_t a1 = (uint32_t)__float_as_uint(t1) * rowb + base;
         const uint32_t c0 = a0 + rowb, c1 = a1 + rowb;
-        const u64 A = pk2(Tap<TC, 0>::ld(a0), Tap<TC, 0>::ld(a1));
-        const u64 B = pk2(Tap<TC, 1>::ld(a0), Tap<TC, 1>::ld(a1));
-        const u64 C = pk2(Tap<TC, 0>::ld(c0), Tap<TC, 0>::ld(c1));
-        const u64 Dd = pk2(Tap<TC, 1>::ld(c0), Tap<TC, 1>::ld(c1));
+        const u64 A = pk2(Tap<T, 0>::ld(a0), Tap<T, 0>::ld(a1));
+        const u64 B = pk2(Tap<T, 1>::ld(a0), Tap<T, 1>::ld(a1));
+        const u64 C = pk2(Tap<T, 0>::ld(c0), Tap<T, 0>::ld(c1));
+        const u64 Dd = pk2(Tap<T, 1>::ld(c0), Tap<T, 1>::ld(c1));
         const u64 R0 = fma2(FW2, sub2(B, A), A);
         const u64 R1 = fma2(FW2, sub2(Dd, C), C);
         const u64 VAL = fma2(FH, sub2(R1, R0), R0);
@@ -529,10 +517,8 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         acc[k] = fmaf(wk, val, acc[k]);
       }
     }
-    if constexpr (!CVT) {
-      __syncwarp();
-      if (lane == 0) dev::mbar_arrive(&empty[s]);
-    }
+    __syncwarp();
+    if (lane == 0) dev::mbar_arrive(&empty[s]);
   }
 
   if (xl < P.nx && yl < P.ny) {
@@ -553,6 +539,249 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         k0 = k;
         if (zl + k0 < P.nz) out[(size_t)(zl + k0) * plane] += v0;
       }
+    }
+  }
+}
+
+// =====================================================================================
+// 16-bit storage: tap pairs prepared by the producer warp
+// =====================================================================================
+// The FP32 kernel reads four 32-bit taps per update from the staged box.  With 16-bit
+// storage a row's two horizontal taps fit one 32-bit word, but the staged box holds them as
+// (c, c+1) words only for even c.  Here the producer warp, besides issuing the TMA loads,
+// rewrites every landed box into a tap-pair buffer (word (r, c) = taps (r, c) in its low and
+// (r, c + 1) in its high half) and hands it to the consumers through an mbarrier ring, so a
+// consumer reads two words per update and no block-wide barrier separates the views:
+//   TMA stage ring (S boxes of 16-bit taps)  --full[s]-->  producer rewrite
+//   pair ring (NP buffers)  --full2[p] (32 producer lanes)-->  consumers
+//   consumers  --empty2[p] (one arrive per consumer warp)-->  producer
+// The producer itself frees a TMA stage once it has rewritten it.  The views it selects
+// (all, or with the PI window those that reach the tile) end with a marker buffer (view -1).
+template <typename T, int NZ, bool PIW>
+__global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_constant__ CUtensorMap tmap,
+                                                                  const __grid_constant__ FdkParams P)
+{
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  static_assert(sizeof(T) == 2, "16-bit storage");
+  const int S = P.stages, NP = P.pbufs;
+  const int stage_elems = P.BW * P.BH;
+  const int stage_bytes = ((stage_elems * 2) + 127) & ~127;
+  const int pbuf_bytes = ((stage_elems * 4) + 127) & ~127;
+  unsigned char* pairs = smem_raw + (size_t)S * stage_bytes;
+  int4* origin2 = reinterpret_cast<int4*>(pairs + (size_t)NP * pbuf_bytes);  // per pair buffer
+  int4* sorg = origin2 + NP;                                                   // per TMA stage
+  uint64_t* full = reinterpret_cast<uint64_t*>(sorg + S);
+  uint64_t* full2 = full + S;
+  uint64_t* empty2 = full2 + NP;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int tx, ty, tz;
+  fdk_tile(P, P.tile0 + blockIdx.x, tx, ty, tz);
+
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < S; k++) dev::mbar_init(&full[k], 1);
+    for (int k = 0; k < NP; k++) {
+      dev::mbar_init(&full2[k], 32);
+      dev::mbar_init(&empty2[k], FDK_CWARPS);
+    }
+    dev::fence_mbar_init();
+  }
+  __syncthreads();
+
+  if (warp == FDK_CWARPS) {
+    // ------------------------------------------------------------- producer warp
+    if (lane == 0) dev::tma_prefetch(&tmap);
+    const uint32_t bytes = (uint32_t)(stage_elems * 2);
+    // views in order, 32 tested at a time (PI window: those that reach the tile)
+    int vb = -32;
+    unsigned msk = 0;
+    int lw0 = 0, lh0 = 0, lnw = 0, lnh = 0;
+    bool exhausted = false, stalled = false, failed = false;
+    int issued = 0, conv = 0;
+    auto issue_next = [&]() {
+      if (exhausted) return;
+      if (issued == P.stop_after) {  // test hook
+        stalled = exhausted = true;
+        return;
+      }
+      while (msk == 0) {
+        vb += 32;
+        if (vb >= P.nviews) {
+          exhausted = true;
+          return;
+        }
+        const int v = vb + lane;
+        bool need = false;
+        if (v < P.nviews) {
+          float fp[4];
+          fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, lw0, lh0, lnw, lnh, fp);
+          need = PIW ? !fdk_tile_outside_window(P, P.v[v], fp[0], fp[1], fp[2], fp[3]) : true;
+        }
+        msk = __ballot_sync(0xffffffffu, need);
+      }
+      const int l = __ffs(msk) - 1;
+      msk &= msk - 1;
+      const int w0 = __shfl_sync(0xffffffffu, lw0, l), h0 = __shfl_sync(0xffffffffu, lh0, l);
+      const int nw = __shfl_sync(0xffffffffu, lnw, l), nh = __shfl_sync(0xffffffffu, lnh, l);
+      const int s = issued % S;  // free: its previous view has been rewritten
+      if (lane == 0) {
+        if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
+        sorg[s] = make_int4(w0, h0, vb + l, nh);
+        dev::mbar_arrive_expect_tx(&full[s], bytes);
+        dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + vb + l);
+      }
+      __syncwarp();
+      issued++;
+    };
+    for (int k = 0; k < S; k++) issue_next();
+    const int cpr = P.BW / 8;  // 16-byte chunks per row (BW is a multiple of 8)
+    const int nbox = P.BH * cpr;
+    while (conv < issued) {
+      const int s = conv % S, p = conv % NP;
+      bool ok = dev::mbar_wait(&full[s], (conv / S) & 1);
+      if (ok && conv >= NP) ok = dev::mbar_wait(&empty2[p], ((conv / NP) - 1) & 1);
+      if (!__all_sync(0xffffffffu, ok)) {
+        failed = true;
+        break;
+      }
+      const int4 o = sorg[s];
+      // rewrite the rows the tile's footprint reaches (taps stay below row o.w - 1); the word
+      // of a row's last column takes the next row's first tap, which no tap reads (columns
+      // stay below BW - 1)
+      const uint4* src = reinterpret_cast<const uint4*>(smem_raw + (size_t)s * stage_bytes);
+      uint4* dst = reinterpret_cast<uint4*>(pairs + (size_t)p * pbuf_bytes);
+      const int nconv = min(o.w, P.BH) * cpr;
+      for (int e = lane; e < nconv; e += 32) {
+        const uint32_t nx = e + 1 < nbox ? reinterpret_cast<const uint32_t*>(src + e + 1)[0] : 0u;
+        uint4 lo, hi;
+        pair8(src[e], nx, lo, hi);
+        dst[2 * e] = lo;
+        dst[2 * e + 1] = hi;
+      }
+      if (lane == 0) origin2[p] = o;
+      __syncwarp();
+      dev::mbar_arrive(&full2[p]);  // all 32 lanes: their writes are released to the consumers
+      conv++;
+      issue_next();  // stage s is free again
+    }
+    if (failed) {
+      if (lane == 0) {
+        dev::record_status(P.status, DEV_TIMEOUT);
+        // drain: wait (bounded) for the copies still in flight before leaving
+        for (int j = conv; j < issued; j++) dev::mbar_wait(&full[j % S], (j / S) & 1, 100000000ull);
+      }
+      return;
+    }
+    if (stalled) return;  // every issued copy has landed and been handed over
+    // end of the view list: a pair buffer whose phase completes without data, view -1
+    const int p = conv % NP;
+    const bool ok = conv < NP || dev::mbar_wait(&empty2[p], ((conv / NP) - 1) & 1);
+    if (__all_sync(0xffffffffu, ok)) {
+      if (lane == 0) origin2[p] = make_int4(0, 0, -1, 0);
+      __syncwarp();
+      dev::mbar_arrive(&full2[p]);
+    } else if (lane == 0) {
+      dev::record_status(P.status, DEV_TIMEOUT);
+    }
+    return;
+  }
+
+  // --------------------------------------------------------------- consumer warps
+  const int xl = tx * FDK_TX + (warp & 1) * 8 + (lane & 7);
+  const int yl = ty * FDK_TY + (warp >> 1) * 4 + (lane >> 3);
+  const int zl = tz * NZ;
+  const float x = P.ox + (float)xl, y = P.oy + (float)yl, zf = P.oz + (float)zl;
+  const float MAGIC = 12582912.0f;  // 1.5 * 2^23: adding it in round-down mode floors
+  const uint32_t MAGIC_BITS = 0x4B400000u;
+  const uint32_t rowb = (uint32_t)(P.BW * 4);  // bytes per row of a pair buffer
+  const uint32_t pair0 = dev::smem_u32(pairs);
+  constexpr int NACC = NZ / 2;
+  u64 acc2[NACC];
+#pragma unroll
+  for (int k = 0; k < NACC; k++) acc2[k] = 0ull;
+
+  for (int j = 0;; j++) {
+    const int p = j % NP;
+    if (!dev::mbar_wait(&full2[p], (j / NP) & 1, P.cwait_ns)) {
+      dev::record_status(P.status, DEV_TIMEOUT);
+      return;
+    }
+    const int4 org = origin2[p];
+    const int v = org.z;
+    if (v < 0) break;
+    const FdkView& V = P.v[v];
+    const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
+    const float U = __frcp_rn(den);
+    const float wabs = fmaf(fmaf(V.a0, x, V.a1 * y), U, V.wc);
+    float wl = wabs - (float)org.x;
+    float h0 = fmaf(U, fmaf(P.hb, zf, V.e), V.hc) - (float)org.y;
+    float dh = U * P.hb;
+    float wt = V.wt;
+    if (P.wexp >= 1) wt *= U;
+    if (P.wexp >= 2) wt *= U;
+    // memory safety: every tap must stay inside the staged box
+    int iw = __float2int_rd(wl);
+    const float hl = fmaf((float)(NZ - 1), dh, h0);
+    if (iw < 0 || iw > P.BW - 2 || !(h0 >= 0.0f) || !(hl + 0.01f < (float)(P.BH - 1))) {
+      dev::record_status(P.status, DEV_RANGE);
+      iw = 0; wl = 0.0f; h0 = 0.0f; dh = 0.0f; wt = 0.0f;
+    }
+    const float fw = wl - (float)iw;
+    float lo = -3.0e38f, hi = 3.0e38f;  // Tam-Danielsson bounds (local h)
+    if constexpr (PIW) {
+      const float u = (wabs - V.wc) * P.td_sign / P.td_r;
+      const float q = P.td_a * (1.0f + u * u);
+      const float at = atanf(u);
+      const float hsrc = V.hc - (float)org.y;
+      hi = hsrc + q * (1.5707963267948966f - at);
+      lo = hsrc - q * (1.5707963267948966f + at);
+    }
+    // byte address of tap pair (row r, column iw) = bits(MAGIC + r) * rowb + base
+    const uint32_t base = pair0 + (uint32_t)p * (uint32_t)pbuf_bytes + (uint32_t)iw * 4u - MAGIC_BITS * rowb;
+    const u64 MAG2 = pk2(MAGIC, MAGIC);
+    const u64 FW2 = pk2(fw, fw);
+    const u64 WT2 = pk2(wt, wt);
+    const u64 D2 = pk2(2.0f * dh, 2.0f * dh);
+    u64 H = pk2(h0, h0 + dh);
+#pragma unroll
+    for (int k = 0; k < NACC; k++) {
+      const u64 T2 = add2_rm(H, MAG2);
+      const u64 FH = sub2(H, sub2(T2, MAG2));
+      float t0, t1;
+      up2(T2, t0, t1);
+      const uint32_t a0 = (uint32_t)__float_as_uint(t0) * rowb + base;
+      const uint32_t a1 = (uint32_t)__float_as_uint(t1) * rowb + base;
+      const uint32_t p0 = lds_b32<0>(a0), p1 = lds_b32<0>(a1);
+      const uint32_t q0 = lds_b32<0>(a0 + rowb), q1 = lds_b32<0>(a1 + rowb);
+      const u64 A = pk2(PairTap<T>::lo(p0), PairTap<T>::lo(p1));
+      const u64 B = pk2(PairTap<T>::hi(p0), PairTap<T>::hi(p1));
+      const u64 C = pk2(PairTap<T>::lo(q0), PairTap<T>::lo(q1));
+      const u64 Dd = pk2(PairTap<T>::hi(q0), PairTap<T>::hi(q1));
+      const u64 R0 = fma2(FW2, sub2(B, A), A);
+      const u64 R1 = fma2(FW2, sub2(Dd, C), C);
+      const u64 VAL = fma2(FH, sub2(R1, R0), R0);
+      u64 W = WT2;
+      if constexpr (PIW) {
+        float h0k, h1k;
+        up2(H, h0k, h1k);
+        W = pk2((h0k >= lo && h0k <= hi) ? wt : 0.0f, (h1k >= lo && h1k <= hi) ? wt : 0.0f);
+      }
+      acc2[k] = fma2(W, VAL, acc2[k]);
+      H = add2(H, D2);
+    }
+    __syncwarp();
+    if (lane == 0) dev::mbar_arrive(&empty2[p]);
+  }
+
+  if (xl < P.nx && yl < P.ny) {
+    float* out = P.vol + (size_t)yl * P.nx + xl;
+    const size_t plane = (size_t)P.nx * P.ny;
+#pragma unroll
+    for (int k = 0; k < NACC; k++) {
+      float v0, v1;
+      up2(acc2[k], v0, v1);
+      if (zl + 2 * k < P.nz) out[(size_t)(zl + 2 * k) * plane] += v0;
+      if (zl + 2 * k + 1 < P.nz) out[(size_t)(zl + 2 * k + 1) * plane] += v1;
     }
   }
 }
@@ -682,6 +911,51 @@ __global__ void __launch_bounds__(256) bp_generic_kernel(const __grid_constant__
 
 }  // namespace fcb
 
+namespace fcb {
+// =====================================================================================
+// PI-window pair count (FP64)
+// =====================================================================================
+// The voxel-view pairs of a helical Katsevich backprojection that lie inside each voxel's
+// PI interval: the work the PI-window kernel does, counted exactly rather than sampled.
+// The window is the Tam-Danielsson one (Noo, Pack & Heuscher 2003, flat detector through the
+// axis): with U = D / (D + x cos a + y sin a), w = (y cos a - x sin a) U, u = sign * w / D and
+// q = pitch / 2pi * (1 + u^2), voxel z is inside for view a when
+//   -q (pi/2 + atan u) <= (z - hmp) U <= q (pi/2 - atan u).
+// (z - hmp) U grows with z, so a column's inside voxels are one run of z, counted in closed
+// form per (column, view).
+struct PiView {
+  double ca, sa, hmp;
+};
+
+__global__ void pi_pairs_kernel(const PiView* __restrict__ views, int nviews, int nx, int ny,
+                                double x0, double y0, long long zlo, long long zhi, double D,
+                                double pitch, double sgn, unsigned long long* count)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long total = (long long)nx * ny * nviews;
+  unsigned long long c = 0;
+  if (i < total) {
+    const int t = (int)(i % nviews);
+    const long long col = i / nviews;
+    const double x = x0 + (double)(col % nx), y = y0 + (double)(col / nx);
+    const PiView v = views[t];
+    const double U = D / (D + x * v.ca + y * v.sa);
+    const double w = (y * v.ca - x * v.sa) * U;
+    const double u = sgn * w / D;
+    const double q = pitch / (2.0 * M_PI) * (1.0 + u * u);
+    const double at = atan(u);
+    const double zmin = v.hmp + (-q * (0.5 * M_PI + at)) / U;
+    const double zmax = v.hmp + (q * (0.5 * M_PI - at)) / U;
+    // clamp before converting so that far-away runs stay defined
+    const long long k0 = max(zlo, (long long)ceil(fmax(zmin, (double)zlo - 1.0)));
+    const long long k1 = min(zhi - 1, (long long)floor(fmin(zmax, (double)zhi + 1.0)));
+    if (k1 >= k0) c = (unsigned long long)(k1 - k0 + 1);
+  }
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+}  // namespace fcb
+
 // =====================================================================================
 // Plans
 // =====================================================================================
@@ -695,7 +969,7 @@ struct fcb_bp_plan {
   int device = 0;
   int nz_tile = 32;
   int maxv = FDK_MAXV;
-  int BW = 0, BH = 0, stages = 0, wshift = 2;
+  int BW = 0, BH = 0, stages = 0, pbufs = 0, wshift = 2;
   long long updates = 0;
   std::vector<FdkParams> fdk;  // one per view chunk
   std::vector<GenParams> gen;
@@ -709,25 +983,49 @@ struct fcb_bp_plan {
 namespace {
 
 // Dynamic shared memory of one fdk_tma_kernel CTA: `stages` boxes of BW x BH elements of
-// `es` bytes, a full and an empty barrier and a footprint record per stage, and, for 16-bit
-// storage widened to FP32 (`widen`), two FP32 boxes (layout of fdk_tma_kernel).
-size_t fdk_smem_bytes(int BW, int BH, int stages, size_t es, bool widen)
+// `es` bytes, a full and an empty barrier and a footprint record per stage.
+size_t fdk_smem_bytes(int BW, int BH, int stages, size_t es)
 {
   const size_t stage_bytes = ((size_t)BW * BH * es + 127) & ~(size_t)127;
-  size_t smem = stages * stage_bytes + stages * (2 * sizeof(uint64_t) + sizeof(int4));
-  if (widen) {
-    const size_t fbuf = ((size_t)BW * BH * 4 + 127) & ~(size_t)127;
-    smem = ((smem + 127) & ~(size_t)127) + 2 * fbuf;
-  }
-  return smem;
+  return stages * stage_bytes + stages * (2 * sizeof(uint64_t) + sizeof(int4));
+}
+
+// Dynamic shared memory of one fdk_pair_kernel CTA: `stages` boxes of 16-bit taps, `pbufs`
+// tap-pair buffers of BW x BH words, their footprint records and barriers.
+size_t fdk_pair_smem_bytes(int BW, int BH, int stages, int pbufs)
+{
+  const size_t stage_bytes = ((size_t)BW * BH * 2 + 127) & ~(size_t)127;
+  const size_t pbuf_bytes = ((size_t)BW * BH * 4 + 127) & ~(size_t)127;
+  return stages * stage_bytes + pbufs * pbuf_bytes + (size_t)(stages + pbufs) * sizeof(int4) +
+         (size_t)(stages + 2 * pbufs) * sizeof(uint64_t);
 }
 
 // Launches chunk `chunk` (-1: all) over the z-tile layers [tz0, tz1) of the plan.
 template <typename T, int NZ, bool PIW, bool X2, int MINB = fdk_min_blocks<NZ>()>
 int launch_fdk(fcb_bp_plan* pl, const CUtensorMap& map, int chunk, int tz0, int tz1, cudaStream_t st)
 {
-  const size_t smem = fdk_smem_bytes(pl->BW, pl->BH, pl->stages, sizeof(T), X2 && sizeof(T) == 2);
+  const size_t smem = fdk_smem_bytes(pl->BW, pl->BH, pl->stages, sizeof(T));
   auto kern = fdk_tma_kernel<T, NZ, PIW, X2, MINB>;
+  FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  for (int c = 0; c < (int)pl->fdk.size(); c++) {
+    if (chunk >= 0 && c != chunk) continue;
+    FdkParams& P = pl->fdk[c];
+    const int layer = P.tiles_x * P.tiles_y;
+    P.tile0 = tz0 * layer;
+    const int ntiles = (tz1 - tz0) * layer;
+    if (ntiles <= 0) continue;
+    kern<<<ntiles, FDK_THREADS, smem, st>>>(map, P);
+    FCB_CUDA_TRY(cudaGetLastError());
+  }
+  return FCB_OK;
+}
+
+// The same for 16-bit storage on fdk_pair_kernel.
+template <typename T, bool PIW>
+int launch_fdk_pair(fcb_bp_plan* pl, const CUtensorMap& map, int chunk, int tz0, int tz1, cudaStream_t st)
+{
+  const size_t smem = fdk_pair_smem_bytes(pl->BW, pl->BH, pl->stages, pl->pbufs);
+  auto kern = fdk_pair_kernel<T, 32, PIW>;
   FCB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   for (int c = 0; c < (int)pl->fdk.size(); c++) {
     if (chunk >= 0 && c != chunk) continue;
@@ -797,8 +1095,11 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
   // only the FP32 pair path is instantiated for depths other than 32
   const char* sc = getenv("FCB_FDK_SCALAR");
   if (projType != FCB_F32 || (sc && sc[0] == '1')) pl->nz_tile = 32;
-  int smem_budget = 64 * 1024;
-  if (const char* e = getenv("FCB_FDK_SMEM_KB")) smem_budget = std::max(8, std::min(200, atoi(e))) * 1024;
+  int smem_budget = 64 * 1024, pair_budget = 0;
+  if (const char* e = getenv("FCB_FDK_SMEM_KB")) {
+    smem_budget = std::max(8, std::min(200, atoi(e))) * 1024;
+    pair_budget = smem_budget;
+  }
   int rc = make_problem(g, &pl->pb);
   if (rc) { delete pl; return rc; }
   Problem& pb = pl->pb;
@@ -883,6 +1184,8 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
       P.wexp = wexp;
       P.piwin = piwin ? 1 : 0;
       P.td_a = td_a; P.td_r = td_r; P.td_sign = td_sign;
+      P.cwait_ns = 2000000000ull;
+      P.stop_after = -1;
       fill_fdk_views(pb, pl->mode, v0, std::min(pl->maxv, pb.nviews - v0), &P);
       pl->fdk.push_back(P);
     }
@@ -894,7 +1197,11 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
     }
     int* need = scratch + 1;
     const int ntiles = tiles_x * tiles_y * tiles_z;
-    cudaMemsetAsync(need, 0, 2 * sizeof(int), st);
+    if (cudaMemsetAsync(need, 0, 2 * sizeof(int), st) != cudaSuccess) {
+      delete pl;
+      return set_error(FCB_ERR_CUDA, std::string("clearing the footprint maxima: ") +
+                                         cudaGetErrorString(cudaGetLastError()));
+    }
     for (const FdkParams& P : pl->fdk) {
       const long long total = (long long)ntiles * P.nviews;
       const int blocks = (int)((total + 255) / 256);
@@ -916,26 +1223,31 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
       cudaGetLastError();
       smem_optin = 227 * 1024;
     }
-    const size_t es_box = dtype_size(projType);
-    if (pl->BW > 256 || pl->BH > 256 ||
-        fdk_smem_bytes(pl->BW, pl->BH, 2, es_box, es_box == 2) > (size_t)smem_optin) {
+    const size_t min_smem = projType == FCB_F32 ? fdk_smem_bytes(pl->BW, pl->BH, 2, 4)
+                                                : fdk_pair_smem_bytes(pl->BW, pl->BH, 2, 2);
+    if (pl->BW > 256 || pl->BH > 256 || min_smem > (size_t)smem_optin) {
       // footprint too large for one TMA box, or two staged boxes exceed a CTA's shared
       // memory (strong magnification: detector pixels much finer than voxels): generic kernel
       pl->path = 0;
       pl->fdk.clear();
-    } else {
-      const size_t es = dtype_size(projType);
-      const size_t stage_bytes = (((size_t)pl->BW * pl->BH * es) + 127) & ~(size_t)127;
-      // 16-bit storage also keeps two FP32 buffers of the widened box in the budget
-      const size_t wide = es == 2 ? 2 * ((((size_t)pl->BW * pl->BH * 4) + 127) & ~(size_t)127) : 0;
-      int st = (int)(((size_t)smem_budget > wide + 2 * stage_bytes ? smem_budget - wide : 2 * stage_bytes) /
-                     stage_bytes);
+    } else if (projType == FCB_F32) {
+      const size_t stage_bytes = (((size_t)pl->BW * pl->BH * 4) + 127) & ~(size_t)127;
+      const int st = (int)((size_t)smem_budget / stage_bytes);
       pl->stages = std::max(2, std::min(8, st));
+    } else {
+      // 16-bit storage (fdk_pair_kernel): two TMA stages of 16-bit taps and as many tap-pair
+      // buffers (2..4) as the budget holds; the budget (74 KB unless set) keeps 3 CTAs per SM
+      pl->stages = 2;
+      const int budget = pair_budget > 0 ? pair_budget : 74 * 1024;
+      int np = 2;
+      while (np < 4 && fdk_pair_smem_bytes(pl->BW, pl->BH, 2, np + 1) <= (size_t)budget) np++;
+      pl->pbufs = np;
+    }
+    if (pl->path == 1)
       for (FdkParams& P : pl->fdk) {
-        P.BW = pl->BW; P.BH = pl->BH; P.stages = pl->stages;
+        P.BW = pl->BW; P.BH = pl->BH; P.stages = pl->stages; P.pbufs = pl->pbufs;
         P.status = scratch;
       }
-    }
   }
   if (pl->path == 0) {
     const int gmax = std::min(GEN_MAXV, pl->maxv);
@@ -1049,11 +1361,11 @@ int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void
       if (piw) FCB_TRY((launch_fdk<__nv_bfloat16, 32, true, false>(pl, map, chunk, tz0, tz1, st)));
       else FCB_TRY((launch_fdk<__nv_bfloat16, 32, false, false>(pl, map, chunk, tz0, tz1, st)));
     } else if (pl->ptype == FCB_F16) {
-      if (piw) FCB_TRY((launch_fdk<__half, 32, true, true>(pl, map, chunk, tz0, tz1, st)));
-      else FCB_TRY((launch_fdk<__half, 32, false, true>(pl, map, chunk, tz0, tz1, st)));
+      if (piw) FCB_TRY((launch_fdk_pair<__half, true>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk_pair<__half, false>(pl, map, chunk, tz0, tz1, st)));
     } else {
-      if (piw) FCB_TRY((launch_fdk<__nv_bfloat16, 32, true, true>(pl, map, chunk, tz0, tz1, st)));
-      else FCB_TRY((launch_fdk<__nv_bfloat16, 32, false, true>(pl, map, chunk, tz0, tz1, st)));
+      if (piw) FCB_TRY((launch_fdk_pair<__nv_bfloat16, true>(pl, map, chunk, tz0, tz1, st)));
+      else FCB_TRY((launch_fdk_pair<__nv_bfloat16, false>(pl, map, chunk, tz0, tz1, st)));
     }
     return ok();
   }
@@ -1132,6 +1444,21 @@ try {
 }
 FCB_CATCH_STATUS
 
+extern "C" int fcb_bp_plan_set_test_stall(fcb_bp_plan* pl, int stopAfterViews,
+                                          unsigned long long consumerWaitNs)
+try {
+  if (!pl) return set_error(FCB_ERR_INVALID, "NULL plan");
+  if (pl->path != 1) return set_error(FCB_ERR_INVALID, "the plan does not use the staged kernel");
+  if (consumerWaitNs == 0 || consumerWaitNs > 2000000000ull)
+    return set_error(FCB_ERR_INVALID, "consumer wait limit must lie in (0, 2 s]");
+  for (FdkParams& P : pl->fdk) {
+    P.stop_after = stopAfterViews < 0 ? -1 : stopAfterViews;
+    P.cwait_ns = consumerWaitNs;
+  }
+  return ok();
+}
+FCB_CATCH_STATUS
+
 extern "C" int fcb_bp_plan_destroy(fcb_bp_plan* pl)
 try {
   delete pl;
@@ -1164,25 +1491,21 @@ constexpr int NOALLOC_SCRATCH_INTS = 64;  // 256 bytes; a call needs NOALLOC_NEE
 constexpr int NOALLOC_NEEDED_INTS = 3;    // [0] status word, [1..2] footprint maxima
 static __device__ __align__(256) int fcb_noalloc_scratch[NOALLOC_SCRATCH_INTS];
 
-// Device address of fcb_noalloc_scratch on the current device, looked up once per device
-// with that device current (the host-side name is only a stand-in for the symbol).
+static_assert(NOALLOC_NEEDED_INTS <= NOALLOC_SCRATCH_INTS,
+              "backprojection needs more scratch than the static array holds");
+
+// Device address of fcb_noalloc_scratch on the current device.  The host-side name is only
+// a stand-in for the symbol, so the address is looked up with the device current, on every
+// call: the lookup allocates nothing, and an address cached across calls would go stale
+// when the device's primary context is reset and created again.
 static int noalloc_scratch_address(int** out)
 {
-  static std::mutex mu;
-  static int* addr[64] = {nullptr};
-  int dev = 0;
-  FCB_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return set_error(FCB_ERR_NODEVICE, "device index out of range");
-  std::lock_guard<std::mutex> lk(mu);
-  if (!addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, fcb_noalloc_scratch);
-    if (e != cudaSuccess)
-      return set_error(FCB_ERR_CUDA, std::string("cudaGetSymbolAddress(fcb_noalloc_scratch): ") +
-                                         cudaGetErrorString(e));
-    addr[dev] = static_cast<int*>(p);
-  }
-  *out = addr[dev];
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, fcb_noalloc_scratch);
+  if (e != cudaSuccess)
+    return set_error(FCB_ERR_CUDA, std::string("cudaGetSymbolAddress(fcb_noalloc_scratch): ") +
+                                       cudaGetErrorString(e));
+  *out = static_cast<int*>(p);
   return FCB_OK;
 }
 
@@ -1191,8 +1514,6 @@ extern "C" int fcb_backproject_device_noalloc(const fcb_geometry* g, int kernelM
                                               void* stream)
 try {
   if (!proj || !volume) return set_error(FCB_ERR_INVALID, "NULL projection or volume pointer");
-  if (NOALLOC_NEEDED_INTS > NOALLOC_SCRATCH_INTS)
-    return set_error(FCB_ERR_RANGE, "backprojection needs more scratch than the static array holds");
   int* scratch = nullptr;
   FCB_TRY(noalloc_scratch_address(&scratch));
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
@@ -1208,6 +1529,52 @@ try {
   FCB_CUDA_TRY(cudaStreamSynchronize(st));
   if (status & DEV_TIMEOUT) return set_error(FCB_ERR_TIMEOUT, "a bounded device-side wait timed out");
   if (status) return set_error(FCB_ERR_RANGE, "a kernel sample fell outside its staging window");
+  return ok();
+}
+FCB_CATCH_STATUS
+
+// Exact count of the voxel-view pairs inside the PI window over the geometry's sub-volume
+// and views (helicalPitch != 0).  Synchronous; allocates a per-view table and a counter.
+extern "C" int fcb_katsevich_pi_pairs(const fcb_geometry* g, long long* pairs, void* stream)
+try {
+  if (!g || !pairs) return set_error(FCB_ERR_INVALID, "NULL geometry or output");
+  Problem pb;
+  FCB_TRY(make_problem(g, &pb));
+  if (pb.pitch == 0.0) return set_error(FCB_ERR_INVALID, "the PI window needs a helical pitch");
+  const int n = pb.nviews;
+  std::vector<PiView> hv(n);
+  for (int t = 0; t < n; t++) hv[t] = PiView{pb.views[t].ca, pb.views[t].sa, pb.views[t].hmp};
+  const double turn = n > 1 ? pb.angle[n - 1] - pb.angle[0] : 1.0;
+  const double sgn = (turn >= 0.0) == (pb.pitch >= 0.0) ? -1.0 : 1.0;
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  PiView* dv = nullptr;
+  unsigned long long* dc = nullptr;
+  struct Free {
+    PiView*& v;
+    unsigned long long*& c;
+    ~Free()
+    {
+      cudaFree(v);
+      cudaFree(c);
+    }
+  } fr{dv, dc};
+  FCB_CUDA_TRY(cudaMalloc(&dv, (size_t)n * sizeof(PiView)));
+  FCB_CUDA_TRY(cudaMalloc(&dc, sizeof(unsigned long long)));
+  FCB_CUDA_TRY(cudaMemcpyAsync(dv, hv.data(), (size_t)n * sizeof(PiView), cudaMemcpyHostToDevice, st));
+  FCB_CUDA_TRY(cudaMemsetAsync(dc, 0, sizeof(unsigned long long), st));
+  const int nx = pb.volEnd[0] - pb.volStart[0], ny = pb.volEnd[1] - pb.volStart[1];
+  const long long total = (long long)nx * ny * n;
+  if (total > 0) {
+    pi_pairs_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+        dv, n, nx, ny, (double)(pb.volStart[0] - pb.volDim[0] / 2), (double)(pb.volStart[1] - pb.volDim[1] / 2),
+        (long long)(pb.volStart[2] - pb.volDim[2] / 2), (long long)(pb.volEnd[2] - pb.volDim[2] / 2), pb.D,
+        pb.pitch, sgn, dc);
+    FCB_CUDA_TRY(cudaGetLastError());
+  }
+  unsigned long long h = 0;
+  FCB_CUDA_TRY(cudaMemcpyAsync(&h, dc, sizeof h, cudaMemcpyDeviceToHost, st));
+  FCB_CUDA_TRY(cudaStreamSynchronize(st));
+  *pairs = (long long)h;
   return ok();
 }
 FCB_CATCH_STATUS

@@ -31,6 +31,11 @@ int bp_plan_execute_chunk(fcb_bp_plan* pl, int chunk, const void* proj, float* v
 int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void* proj,
                           float* volume, cudaStream_t st);
 int bp_plan_z_tile(const fcb_bp_plan* pl);
+int filter_plan_run(fcb_filter_plan* pl, const float* in, void* out, int nviews, int pitch, float D,
+                    const float* dzorig, int cosineWeight, cudaStream_t st);
+int filter_plan_create(int nviews, int H, int W, int outType, int window, double gaussScale,
+                       fcb_filter_plan** out);
+void filter_plan_destroy(fcb_filter_plan* pl);
 }  // namespace fcb
 
 using namespace fcb;
@@ -271,18 +276,30 @@ struct HostTrace {
   }
 };
 
+// FDK pre-processing done inside the host pipeline (fcb_fbp_host): each uploaded view chunk
+// is cosine-weighted and ramp filtered in place on the device before its backprojection,
+// and the filtered views go back to the caller's buffer `out`.
+struct FbpFilter {
+  int window;
+  float D;
+  const float* zOrigin;
+  int cosine;
+  float* out;
+};
+
 // Host-buffer backprojection, pipelined over view chunks and z-slabs of the volume:
 //   copy-in stream : the first view chunk, the volume slab by slab, then the other chunks
-//   compute stream : chunk by chunk as they arrive, each over all slabs (slab s of the first
-//                    chunk as soon as slab s is in)
+//   compute stream : chunk by chunk as they arrive (filtered first when `ff` is set), each
+//                    over all slabs (slab s of the first chunk as soon as slab s is in)
 //   copy-out stream: slab s back to the host as soon as the last chunk has passed over it
+//   (filter: a fourth stream returns each filtered chunk as soon as it is filtered)
 // so the PCIe traffic (projections once, the volume in and out) hides behind the kernels
 // except for the first chunk with the first slab, and the last slab.  One plan (one staging
 // pre-pass) serves every slab: a slab is a range of the plan's z tiles.  Reference-compatible
 // windows that change the result run as one slab (their tiling starts at volStart).
-extern "C" int fcb_backproject_host(int device, const fcb_geometry* g0, int kernelMode,
-                                    const float* projections, float* volume)
-try {
+static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelMode,
+                                 const float* projections, float* volume, const FbpFilter* ff)
+{
   if (!g0 || !projections || !volume) return set_error(FCB_ERR_INVALID, "NULL argument");
   HostTrace tr;
   DeviceGuard guard(device);
@@ -333,21 +350,67 @@ try {
   const size_t plane = (size_t)nx * ny;
   const size_t nvox = plane * nz;
   Scratch sc;
-  float *dvol = nullptr, *dproj = nullptr;
+  float *dvol = nullptr, *dproj = nullptr, *dz = nullptr;
   FCB_TRY(sc.alloc((void**)&dvol, nvox * sizeof(float)));
   FCB_TRY(sc.alloc((void**)&dproj, (size_t)n * H * wpad * sizeof(float)));
-  const double t_alloc = tr.ms();
-  cudaStream_t cs, xs, os;
+  cudaStream_t cs, xs, os, ps = nullptr;
   FCB_TRY(sc.stream(&cs));
   FCB_TRY(sc.stream(&xs));
   FCB_TRY(sc.stream(&os));
+  fcb_filter_plan* fplan = nullptr;
+  struct FilterGuard {
+    fcb_filter_plan*& p;
+    cudaStream_t& s;
+    ~FilterGuard()
+    {
+      if (p) {
+        cudaStreamSynchronize(s);  // the plan's scratch is in use until the compute stream ends
+        filter_plan_destroy(p);
+      }
+    }
+  } fguard{fplan, cs};
+  std::vector<cudaEvent_t> filt_done(ranges.size(), nullptr);
+  if (ff) {
+    int maxc = 1;
+    for (const auto& r : ranges) maxc = std::max(maxc, r.second - r.first);
+    FCB_TRY(filter_plan_create(maxc, H, W, FCB_F32, ff->window, 0.125, &fplan));
+    FCB_TRY(sc.stream(&ps));
+    if (ff->cosine) {
+      FCB_TRY(sc.alloc((void**)&dz, (size_t)n * sizeof(float)));
+      FCB_CUDA_TRY(cudaMemcpyAsync(dz, ff->zOrigin, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, cs));
+    }
+  }
+  const double t_alloc = tr.ms();
   if (wpad != W) FCB_CUDA_TRY(cudaMemsetAsync(dproj, 0, (size_t)n * H * wpad * sizeof(float), xs));
   // pageable caller buffers (numpy arrays): pinned staging filled by host threads
   HostStager stager;
   const bool proj_pg = is_pageable(projections), vol_pg = is_pageable(volume);
-  FCB_TRY(stager.init((proj_pg ? (size_t)n * H * W * sizeof(float) : 0) + (vol_pg ? 2 * nvox * sizeof(float) : 0)));
+  const bool out_pg = ff && is_pageable(ff->out);
+  FCB_TRY(stager.init((proj_pg ? (size_t)n * H * W * sizeof(float) : 0) + (vol_pg ? 2 * nvox * sizeof(float) : 0) +
+                      (out_pg ? (size_t)n * H * W * sizeof(float) : 0)));
   HostStager* pst = proj_pg && stager.ok ? &stager : nullptr;
   HostStager* vst = vol_pg && stager.ok ? &stager : nullptr;
+  HostStager* fst = out_pg && stager.ok && wpad == W ? &stager : nullptr;
+  // filter chunk c in place (compute stream), then return it to the caller: on its own
+  // stream at once, or (pageable output through the pinned ring) after every kernel is queued
+  auto filter_chunk = [&](int c) -> int {
+    if (!ff) return FCB_OK;
+    const int v0 = ranges[c].first, nv = ranges[c].second - v0;
+    float* p = dproj + (size_t)v0 * H * wpad;
+    FCB_TRY(filter_plan_run(fplan, p, p, nv, wpad, ff->D, ff->cosine ? dz + v0 : nullptr, ff->cosine, cs));
+    FCB_TRY(sc.event(&filt_done[c]));
+    FCB_CUDA_TRY(cudaEventRecord(filt_done[c], cs));
+    if (!fst) {
+      FCB_CUDA_TRY(cudaStreamWaitEvent(ps, filt_done[c], 0));
+      float* h = ff->out + (size_t)v0 * H * W;
+      if (wpad == W)
+        FCB_CUDA_TRY(cudaMemcpyAsync(h, p, (size_t)nv * H * W * sizeof(float), cudaMemcpyDeviceToHost, ps));
+      else
+        FCB_CUDA_TRY(cudaMemcpy2DAsync(h, W * sizeof(float), p, wpad * sizeof(float), W * sizeof(float),
+                                       (size_t)nv * H, cudaMemcpyDeviceToHost, ps));
+    }
+    return FCB_OK;
+  };
   std::vector<cudaEvent_t> slab_done(nslab, nullptr);
   auto zoff = [&](int s) { return (size_t)z0[s] * plane; };
   auto slab_bytes = [&](int s) { return (size_t)(z1[s] - z0[s]) * plane * sizeof(float); };
@@ -391,6 +454,7 @@ try {
     FCB_TRY(sc.event(&ev));
     FCB_CUDA_TRY(cudaEventRecord(ev, xs));
     FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
+    FCB_TRY(filter_chunk(c));
     for (int s = 0; s < nslab; s++) {
       if (c == 0) FCB_TRY(copy_vol_slab(s));
       FCB_TRY(bp_plan_execute_range(plan, c, z0[s], z1[s], dproj, dvol, cs));
@@ -406,11 +470,22 @@ try {
   }
   for (int s = 0; s < nslab; s++) {
     for (int c = cm; c < nch; c++) {
-      if (s == 0) FCB_CUDA_TRY(cudaStreamWaitEvent(cs, up[c], 0));
+      if (s == 0) {
+        FCB_CUDA_TRY(cudaStreamWaitEvent(cs, up[c], 0));
+        FCB_TRY(filter_chunk(c));
+      }
       FCB_TRY(bp_plan_execute_range(plan, c, z0[s], z1[s], dproj, dvol, cs));
     }
     FCB_TRY(finish_slab(s));
   }
+  // pageable output of the filtered views: through the pinned ring, chunk by chunk
+  if (fst)
+    for (int c = 0; c < nch; c++) {
+      const int v0 = ranges[c].first, nv = ranges[c].second - v0;
+      FCB_CUDA_TRY(cudaStreamWaitEvent(os, filt_done[c], 0));
+      FCB_TRY(fst->d2h(ff->out + (size_t)v0 * H * W, dproj + (size_t)v0 * H * wpad,
+                       (size_t)nv * H * W * sizeof(float), os));
+    }
   // staged copy-out of each slab as soon as its last kernel is done (os waits for it); the
   // later slabs' kernels run meanwhile
   if (vst)
@@ -421,6 +496,7 @@ try {
   if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[2], cs));
   if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[3], os));
   FCB_CUDA_TRY(cudaStreamSynchronize(os));
+  if (ps) FCB_CUDA_TRY(cudaStreamSynchronize(ps));
   FCB_CUDA_TRY(cudaStreamSynchronize(cs));
   FCB_TRY(collect_device_status(cs));
   if (tr.on) {
@@ -436,6 +512,30 @@ try {
     for (cudaEvent_t e : tev) cudaEventDestroy(e);
   }
   return ok();
+}
+
+extern "C" int fcb_backproject_host(int device, const fcb_geometry* g, int kernelMode,
+                                    const float* projections, float* volume)
+try {
+  return backproject_host_impl(device, g, kernelMode, projections, volume, nullptr);
+}
+FCB_CATCH_STATUS
+
+// fastcone.fbp on host buffers in one pipelined call: each view chunk is uploaded, cosine-
+// weighted and ramp filtered on the device, written back over the caller's projections (the
+// reference's fbp leaves the filtered projections in its input), and backprojected (FDK)
+// into the volume while the next chunk moves.
+extern "C" int fcb_fbp_host(int device, const fcb_geometry* g, int window, float cosineD,
+                            const float* zOrigin, int cosineWeight, float* projections, float* volume)
+try {
+  if (!projections) return set_error(FCB_ERR_INVALID, "NULL argument");
+  if (cosineWeight && (!zOrigin || !(cosineD > 0.0f)))
+    return set_error(FCB_ERR_INVALID, "cosine weighting needs D > 0 and zOrigin");
+  if (window != FCB_FILTER_RAMLAK && window != FCB_FILTER_SHEPPLOGAN && window != FCB_FILTER_COSRAMP &&
+      window != FCB_FILTER_GAUSSRAMP)
+    return set_error(FCB_ERR_INVALID, "unknown filter window");
+  FbpFilter ff{window, cosineD, zOrigin, cosineWeight ? 1 : 0, projections};
+  return backproject_host_impl(device, g, FCB_MODE_FDK, projections, volume, &ff);
 }
 FCB_CATCH_STATUS
 

@@ -19,8 +19,9 @@
 
 namespace fcb {
 
+// Rows of W values at a pitch of `pitch` elements (pitch >= W) -> zero-padded rows of L.
 __global__ void pad_weight_kernel(const float* __restrict__ in, float* __restrict__ pad,
-                                  long long row0, int nrows, int H, int W, int L, float D,
+                                  long long row0, int nrows, int H, int W, int pitch, int L, float D,
                                   const float* __restrict__ zorig, int cosw)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -31,7 +32,7 @@ __global__ void pad_weight_kernel(const float* __restrict__ in, float* __restric
   float v = 0.0f;
   if (c < W) {
     const long long gr = row0 + r;
-    v = in[gr * W + c];
+    v = in[gr * pitch + c];
     if (cosw) {
       const int t = (int)(gr / H), h = (int)(gr % H);
       const float hh = (float)h - zorig[t];
@@ -65,13 +66,13 @@ __device__ __forceinline__ __nv_bfloat16 to_store<__nv_bfloat16>(float v) { retu
 
 template <typename T>
 __global__ void crop_store_kernel(const float* __restrict__ pad, T* __restrict__ out, long long row0,
-                                  int nrows, int W, int L, float scale)
+                                  int nrows, int W, int pitch, int L, float scale)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= (long long)nrows * W) return;
   const int c = (int)(i % W);
   const long long r = i / W;
-  out[(row0 + r) * W + c] = to_store<T>(pad[r * L + c] * scale);
+  out[(row0 + r) * pitch + c] = to_store<T>(pad[r * L + c] * scale);
 }
 
 // ------------------------------------------------------------------- phantom
@@ -232,26 +233,29 @@ try {
 }
 FCB_CATCH_STATUS
 
-// out = filter(in) as outType; zOrigin (host, nviews floats) is read before the call returns.
-extern "C" int fcb_filter_plan_execute(fcb_filter_plan* pl, const float* in, void* out, float D,
-                                       const float* zOrigin, int cosineWeight, void* stream)
-try {
+namespace fcb {
+// Filters the first `nviews` (<= the plan's) views of `in` into `out`, both with rows of the
+// plan's W values at a pitch of `pitch` elements (in == out allowed for FP32 output).
+// dzorig: device array of the views' zOrigin (cosine weight), or NULL without weighting.
+// Stream-ordered, no allocation.
+int filter_plan_run(fcb_filter_plan* pl, const float* in, void* out, int nviews, int pitch, float D,
+                    const float* dzorig, int cosineWeight, cudaStream_t st)
+{
   if (!pl || !in || !out) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
-  if (cosineWeight && (!zOrigin || !(D > 0.0f)))
+  if (nviews <= 0 || nviews > pl->nviews || pitch < pl->W)
+    return set_error(FCB_ERR_INVALID, "filter view count or row pitch out of range");
+  if (cosineWeight && (!dzorig || !(D > 0.0f)))
     return set_error(FCB_ERR_INVALID, "cosine weighting needs D > 0 and zOrigin");
-  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   const int n2 = pl->n2, nb = pl->nb, W = pl->W, H = pl->H, batch = pl->batch;
-  if (cosineWeight)
-    FCB_CUDA_TRY(cudaMemcpyAsync(pl->dz, zOrigin, pl->nviews * sizeof(float), cudaMemcpyHostToDevice, st));
   if (cufftSetStream(pl->pf, st) != CUFFT_SUCCESS || cufftSetStream(pl->pi, st) != CUFFT_SUCCESS)
     return set_error(FCB_ERR_CUDA, "cufftSetStream failed");
   const float scale = 1.0f / (float)n2;
-  const long long rows = (long long)pl->nviews * H;
+  const long long rows = (long long)nviews * H;
   for (long long r0 = 0; r0 < rows; r0 += batch) {
     const int nr = (int)std::min<long long>(batch, rows - r0);
     long long tot = (long long)nr * n2;
-    pad_weight_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, pl->pad, r0, nr, H, W, n2, D, pl->dz,
-                                                                   cosineWeight);
+    pad_weight_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, pl->pad, r0, nr, H, W, pitch, n2, D,
+                                                                   dzorig, cosineWeight);
     // cuFFT plans are for `batch` rows; the tail batch is zero-padded in `pad`
     if (nr < batch)
       FCB_CUDA_TRY(cudaMemsetAsync(pl->pad + (size_t)nr * n2, 0, (size_t)(batch - nr) * n2 * sizeof(float), st));
@@ -261,11 +265,37 @@ try {
     if (cufftExecC2R(pl->pi, pl->spec, pl->pad) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecC2R failed");
     tot = (long long)nr * W;
     const unsigned g = (unsigned)((tot + 255) / 256);
-    if (pl->outType == FCB_F32) crop_store_kernel<float><<<g, 256, 0, st>>>(pl->pad, (float*)out, r0, nr, W, n2, scale);
-    else if (pl->outType == FCB_F16) crop_store_kernel<__half><<<g, 256, 0, st>>>(pl->pad, (__half*)out, r0, nr, W, n2, scale);
-    else crop_store_kernel<__nv_bfloat16><<<g, 256, 0, st>>>(pl->pad, (__nv_bfloat16*)out, r0, nr, W, n2, scale);
+    if (pl->outType == FCB_F32)
+      crop_store_kernel<float><<<g, 256, 0, st>>>(pl->pad, (float*)out, r0, nr, W, pitch, n2, scale);
+    else if (pl->outType == FCB_F16)
+      crop_store_kernel<__half><<<g, 256, 0, st>>>(pl->pad, (__half*)out, r0, nr, W, pitch, n2, scale);
+    else
+      crop_store_kernel<__nv_bfloat16><<<g, 256, 0, st>>>(pl->pad, (__nv_bfloat16*)out, r0, nr, W, pitch, n2, scale);
   }
   FCB_CUDA_TRY(cudaGetLastError());
+  return FCB_OK;
+}
+
+int filter_plan_create(int nviews, int H, int W, int outType, int window, double gaussScale,
+                       fcb_filter_plan** out)
+{
+  return fcb_filter_plan_create_ex(nviews, H, W, outType, window, gaussScale, out);
+}
+
+void filter_plan_destroy(fcb_filter_plan* pl) { delete pl; }
+}  // namespace fcb
+
+// out = filter(in) as outType; zOrigin (host, nviews floats) is read before the call returns.
+extern "C" int fcb_filter_plan_execute(fcb_filter_plan* pl, const float* in, void* out, float D,
+                                       const float* zOrigin, int cosineWeight, void* stream)
+try {
+  if (!pl || !in || !out) return set_error(FCB_ERR_INVALID, "NULL plan or buffer");
+  if (cosineWeight && (!zOrigin || !(D > 0.0f)))
+    return set_error(FCB_ERR_INVALID, "cosine weighting needs D > 0 and zOrigin");
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (cosineWeight)
+    FCB_CUDA_TRY(cudaMemcpyAsync(pl->dz, zOrigin, pl->nviews * sizeof(float), cudaMemcpyHostToDevice, st));
+  FCB_TRY(filter_plan_run(pl, in, out, pl->nviews, pl->W, D, pl->dz, cosineWeight, st));
   return ok();
 }
 FCB_CATCH_STATUS

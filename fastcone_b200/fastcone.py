@@ -141,11 +141,29 @@ def fbp(vol, proj, projAngles, specimenLength, zOrigin, volStart=np.array([0, 0,
         volDims=None, GPUID=0, pixelWidth=1.0, window="ramlak"):
     """FDK: cosine pre-weight, ramp filter, FDK backprojection with norm 1/nviews
     (fastcone.py:260-270).  Like the reference, overwrites ``proj`` with the weighted,
-    filtered projections and returns the last view's cosine-weight array."""
+    filtered projections and returns the last view's cosine-weight array.  One library call
+    (fcb_fbp_host) streams the views to the GPU, filters them there, returns them into
+    ``proj`` and backprojects them while the next views are in flight."""
     zOrigin = np.asarray(zOrigin)
-    _filter_inplace(proj, specimenLength, zOrigin, cosine=True, window=window, GPUID=GPUID)
-    backproject(vol, proj, projAngles, specimenLength, zOrigin, volStart, volDims, GPUID=GPUID,
-                pixelWidth=pixelWidth)
+    if proj.dtype != FLOAT_TYPE or not proj.flags.c_contiguous:
+        raise FastconeArgumentError("Projection array must be C-contiguous np.float32")
+    projAngles = np.asarray(projAngles)
+    _check_common(vol, proj, projAngles, zOrigin, "project")
+    (angle, hmid, volDims, volStart_r, volEnd, projDims, projWHSize, projWOffset, projHOffset,
+     norm) = _prepare(vol, proj, projAngles, zOrigin, volStart, volDims, None, None, None, None,
+                      lambda pd: np.ones(projAngles.size, dtype=FLOAT_TYPE) / pd[0], True)
+    g = _lib.FcbGeometry()
+    for i in range(3):
+        g.volDim[i], g.volStart[i], g.volEnd[i], g.projDim[i] = (int(volDims[i]), int(volStart_r[i]),
+                                                                 int(volEnd[i]), int(projDims[i]))
+    g.projWHSize[0], g.projWHSize[1] = int(projWHSize[0]), int(projWHSize[1])
+    g.projWOffset, g.projHOffset = _ip(projWOffset), _ip(projHOffset)
+    g.angles, g.hMidPlane, g.normalizationFactor = _fp(angle), _fp(hmid), _fp(norm)
+    g.sourceSampleDistance = float(specimenLength)
+    g.pixelWidth = float(pixelWidth)
+    g.referenceWindows = 1  # as the GPU_CB_* entry points: the reference's windows where they matter
+    _lib.check(lib().fcb_fbp_host(int(GPUID), ctypes.byref(g), _WINDOWS[window], float(specimenLength), _fp(hmid),
+                                  1, proj.ctypes.data_as(ctypes.c_void_p), vol.ctypes.data_as(ctypes.c_void_p)))
     W, H = proj.shape[2], proj.shape[1]
     ww = (np.arange(0.0, W, 1.0) - W / 2.0)[None, :]
     hh = (np.arange(0.0, H, 1.0) - float(zOrigin[proj.shape[0] - 1]))[:, None]

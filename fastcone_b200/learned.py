@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import statistics
 import time
 
 import numpy as np
@@ -74,15 +75,25 @@ def _safe_inv(t, eps=1e-6):
     return torch.where(t > eps, 1.0 / t.clamp_min(eps), torch.zeros_like(t))
 
 
-def make_sample(ops_: Operators, seed: int, device="cuda"):
-    """Seeded phantom (attenuation per voxel) and its noisy log-transformed projections."""
+# The training distribution, and a shifted one for out-of-distribution evaluation: three
+# times the ellipsoids, denser material (mean density x 1.8) and half the photons.
+IN_DISTRIBUTION = {"n_ellipsoids": None, "density": (0.1, 1.0), "i0": None}
+OUT_OF_DISTRIBUTION = {"n_ellipsoids": 30, "density": (0.5, 1.5), "i0": 5e3}
+
+
+def make_sample(ops_: Operators, seed: int, device="cuda", n_ellipsoids=None, density=(0.1, 1.0), i0=None):
+    """Seeded phantom (attenuation per voxel) and its noisy log-transformed projections; the
+    defaults are the training distribution (N_ELLIPSOIDS ellipsoids, densities U(0.1, 1),
+    I0 photons)."""
     g = ops_.g
-    mu = ops.phantom(g.vol_xyz, random_ellipsoids(N_ELLIPSOIDS, g.vol_xyz, seed), device=device)
+    n_ellipsoids = n_ellipsoids or N_ELLIPSOIDS
+    i0 = i0 or I0
+    mu = ops.phantom(g.vol_xyz, random_ellipsoids(n_ellipsoids, g.vol_xyz, seed, density=density), device=device)
     mu.mul_(MU_PER_VOXEL)
     p = ops_.Aexact(mu)
     gen = torch.Generator(device=device).manual_seed(seed)
-    counts = torch.poisson(I0 * torch.exp(-p), generator=gen)
-    y = -torch.log(counts.clamp_min(1.0) / I0)
+    counts = torch.poisson(i0 * torch.exp(-p), generator=gen)
+    y = -torch.log(counts.clamp_min(1.0) / i0)
     return mu, y
 
 
@@ -213,19 +224,22 @@ def train(net: UnrolledNet, geom: ConeGeometry, n_phantoms: int = 2000, lr: floa
 
 
 @torch.no_grad()
-def evaluate(net: UnrolledNet, geom: ConeGeometry, seeds, sirt_iters: int = 100):
+def evaluate(net: UnrolledNet, geom: ConeGeometry, seeds, sirt_iters: int = 100, dist=None, reps: int = 3):
     """Per phantom: SIRT-sirt_iters (from zero) PSNR/SSIM/time; FDK + k SIRT steps without the
-    network; the learned steps with their cumulative times; time to reach SIRT's PSNR."""
+    network; the learned steps with their cumulative times; time to reach SIRT's PSNR.
+    `dist`: phantom / noise distribution (make_sample's keywords; default: the training one).
+    Both methods are timed the same way: one untimed pass (plans, allocator), then `reps`
+    timed passes with CUDA events; the median pass time counts (per step for the learned
+    steps)."""
     ops_ = Operators(geom)
     mask = fov_mask(ops_.g)
+    dist = {k: v for k, v in (dist or {}).items() if v is not None}
     res = []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for s in seeds:
-        mu, y = make_sample(ops_, s)
-        # SIRT (warm the plans first; the faster of two timed runs, like the learned side)
-        ops_.sirt_step_dir(torch.zeros_like(mu), y)
-        t_sirt = None
-        for rep in range(2):
+        mu, y = make_sample(ops_, s, **dist)
+        t_runs = []
+        for rep in range(reps + 1):
             x = torch.zeros_like(mu)
             torch.cuda.synchronize()
             ev0.record()
@@ -233,15 +247,14 @@ def evaluate(net: UnrolledNet, geom: ConeGeometry, seeds, sirt_iters: int = 100)
                 x = torch.relu(x + ops_.sirt_step_dir(x, y))
             ev1.record()
             torch.cuda.synchronize()
-            t = ev0.elapsed_time(ev1) / 1e3
-            t_sirt = t if t_sirt is None else min(t_sirt, t)
+            if rep > 0:
+                t_runs.append(ev0.elapsed_time(ev1) / 1e3)
+        t_sirt = statistics.median(t_runs)
         p_sirt, s_sirt = psnr(x, mu, mask), ssim3d(x, mu, mask)
-        # learned: cumulative time at each step (events between steps, no host sync); the
-        # first pass only warms the allocator and the FFT plan; of the timed passes the
-        # fastest time to each step counts (a host-side stall shows as a gap between events)
+        # learned: cumulative time at each step (events between steps, no host sync)
         marks = [torch.cuda.Event(enable_timing=True) for _ in range(STEPS + 2)]
-        times = None
-        for rep in range(4):
+        runs = []
+        for rep in range(reps + 1):
             states = []
             torch.cuda.synchronize()
             marks[0].record()
@@ -255,8 +268,8 @@ def evaluate(net: UnrolledNet, geom: ConeGeometry, seeds, sirt_iters: int = 100)
                 states.append(x)
             torch.cuda.synchronize()
             if rep > 0:
-                tr = [marks[0].elapsed_time(m) / 1e3 for m in marks[1:]]
-                times = tr if times is None else [min(a, b) for a, b in zip(times, tr)]
+                runs.append([marks[0].elapsed_time(m) / 1e3 for m in marks[1:]])
+        times = [statistics.median(c) for c in zip(*runs)]
         psnrs = [psnr(v, mu, mask) for v in states]
         # the same pipeline without the network (FDK + SIRT steps)
         xb = states[0].clone()

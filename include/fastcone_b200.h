@@ -145,6 +145,16 @@ int fcb_backproject_host(int device, const fcb_geometry* g, int kernelMode,
 int fcb_project_host(int device, const fcb_geometry* g, int method, const float* volume,
                      float* projections);
 
+/* fastcone.fbp (fastcone.py:260-270) on host buffers in one pipelined call: each view chunk
+ * of `projections` is uploaded, optionally cosine-weighted by
+ * cosineD / sqrt(cosineD^2 + (h - zOrigin[t])^2 + (w - W/2)^2) (detector pixels), filtered
+ * with `window` (FCB_FILTER_*, as fcb_fdk_filter_device), written back over `projections`
+ * (the reference's fbp leaves the filtered projections in its input) and backprojected with
+ * the FDK weight into `volume` (+=, g's normalisation) while the next chunk is in flight.
+ * Same buffer rules as fcb_backproject_host. */
+int fcb_fbp_host(int device, const fcb_geometry* g, int window, float cosineD, const float* zOrigin,
+                 int cosineWeight, float* projections, float* volume);
+
 /* Device-pointer versions, stream-ordered on `stream` (a cudaStream_t, NULL = legacy
  * default).  `proj` holds FCB_F32/F16/BF16 values with the layout above; `volume` is
  * float.  They return once the work is queued; a device-side failure is reported by
@@ -168,6 +178,23 @@ int fcb_bp_plan_execute(fcb_bp_plan* plan, const void* proj, float* volume, void
 int fcb_bp_plan_info(const fcb_bp_plan* plan, int* boxW, int* boxH, int* launches,
                      long long* voxelViewUpdates);
 int fcb_bp_plan_destroy(fcb_bp_plan* plan);
+/* Test hook for the device-side timeout path, no counterpart in the reference.  On a plan
+ * that uses the staged kernel (boxW > 0), later executes stage only the first
+ * `stopAfterViews` views of each launch (< 0: all, the default), drain their copies and
+ * leave, and each consumer wait for a staged view gives up after consumerWaitNs
+ * nanoseconds (0 < consumerWaitNs <= 2e9; the default is 2e9).  With stopAfterViews >= 0
+ * the kernels therefore end early with FCB_ERR_TIMEOUT recorded (reported by
+ * fcb_sync_status) and the volume partly updated; no copy is left in flight and the
+ * context stays usable. */
+int fcb_bp_plan_set_test_stall(fcb_bp_plan* plan, int stopAfterViews,
+                               unsigned long long consumerWaitNs);
+
+/* Exact number of voxel-view pairs of the geometry's sub-volume and views that lie inside
+ * the Katsevich PI window (the Tam-Danielsson bounds of the FP64 oracle; helicalPitch != 0):
+ * the work of the PI-window backprojection, for throughput figures.  FP64, on the GPU;
+ * synchronous (allocates a per-view table and a counter).  No counterpart in the reference,
+ * whose Katsevich kernel (coneBeamGPU.cu:258-338) has no window. */
+int fcb_katsevich_pi_pairs(const fcb_geometry* g, long long* pairs, void* stream);
 
 /* Same backprojection as fcb_backproject_device, for callers that cannot allocate device
  * memory while they run (GPU memory owned by another allocator or a fixed budget, or a
@@ -175,11 +202,13 @@ int fcb_bp_plan_destroy(fcb_bp_plan* plan);
  * reference.  It calls no cudaMalloc/cudaFree and no allocating library routine: its
  * device scratch -- the kernels' status word and the staging-box footprint maxima, 3 ints
  * -- lives in a static 256-byte device array (64 ints) that every GPU loading the library
- * holds until exit; a call whose scratch need exceeded that array would be rejected with
- * FCB_ERR_RANGE.  The first call on a device looks up the array's device address (do it
- * before any stream capture).  All calls share the array and clear it at their start, so
- * calls whose GPU work overlaps (concurrent streams or threads) race on it.  The call is
- * synchronous: it waits for `stream` and returns the kernels' device-side status. */
+ * holds until exit; the scratch need is fixed and checked against the array's size when the
+ * library is compiled.  Every call looks up the array's device address on the current
+ * device (the lookup allocates nothing).  All calls share the array and clear it at their
+ * start, so calls whose GPU work overlaps (concurrent streams or threads) race on it.
+ * Geometries whose reference-compatible windows change the result need a device window
+ * table and are refused with FCB_ERR_INVALID.  The call is synchronous: it waits for
+ * `stream` and returns the kernels' device-side status. */
 int fcb_backproject_device_noalloc(const fcb_geometry* g, int kernelMode, const void* proj,
                                    int projType, float* volume, void* stream);
 
@@ -292,6 +321,12 @@ int fcb_reference_windows(const fcb_geometry* g, int* subVolDim, int* subProjDim
  * each slab needs only these rows of each view (mpi_fastcone.py:450-526 moves whole
  * per-chunk detector windows between MPI ranks for the same purpose). */
 int fcb_detector_rows(const fcb_geometry* g, int margin, int* rowLo, int* rowHi);
+
+/* Measured ceiling for the staged kernels' rooflines, no counterpart in the reference:
+ * conflict-free shared-memory loads of bytesPerLoad (4, 8 or 16) bytes per thread by two
+ * 1024-thread CTAs per SM of the current device, 16 * iters loads per thread.  *ms = the
+ * kernel's CUDA-event time on `stream`, *bytes = the bytes loaded.  Synchronous. */
+int fcb_smem_bandwidth(int bytesPerLoad, long long iters, float* ms, double* bytes, void* stream);
 
 #ifdef __cplusplus
 }

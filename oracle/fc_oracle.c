@@ -778,6 +778,52 @@ int orc_backproject_f64(double* vol, const float* projections,
  * (Noo, Pack, Heuscher 2003, flat detector at distance D) with u the detector coordinate
  * along the source's direction of travel (u = -w for a right-handed helix here) and
  * heights relative to the source.  pitch = source rise per turn (voxels). */
+/* One voxel's PI-window Katsevich sum (global voxel indices gx, gy, gz); *cnt += the
+ * voxel-view pairs inside the window. */
+static double kats_piwin_voxel_f64(int gx, int gy, int gz, const float* projections,
+                                   const int volDim[3], const int projDim[3],
+                                   const int projWHSize[2], const int* projWOffset,
+                                   const int* projHOffset, const dview* views, double D,
+                                   const float* norm, double pw, double pitch, double sgn,
+                                   int64_t* cnt)
+{
+  const int n = projDim[2];
+  const double W2 = projDim[0] / 2, H2 = projDim[1] / 2;
+  const double x = gx - volDim[0] / 2, y = gy - volDim[1] / 2, z = gz - volDim[2] / 2;
+  double acc = 0.0;
+  int64_t c = 0;
+  for (int t = 0; t < n; t++) {
+    const dview* v = &views[t];
+    const double U = D / (D + x * v->ca + y * v->sa);
+    const double w = (y * v->ca - x * v->sa) * U; /* voxel units on the virtual detector */
+    const double h = (z - v->hmp) * U;
+    const double u = sgn * w / D;
+    const double q = (pitch / (2.0 * ORC_PI)) * (1.0 + u * u);
+    if (h > q * (ORC_PI / 2 - atan(u)) || h < -q * (ORC_PI / 2 + atan(u))) continue;
+    c++;
+    acc += norm[t] * U * bil_window(projections, projWHSize[0], projWHSize[1], t,
+                                    projWOffset[t], projHOffset[t], w / pw + W2, h / pw + H2);
+  }
+  *cnt += c;
+  return acc;
+}
+
+/* Sense of the helix relative to the detector's w axis: the window's u axis runs against
+ * the source's direction of travel for a right-handed helix (angles and height rising
+ * together). */
+static double kats_sign(const float* angles, int n, double pitch)
+{
+  const double turn = n > 1 ? (double)angles[n - 1] - (double)angles[0] : 1.0;
+  return ((turn >= 0.0) == (pitch >= 0.0)) ? -1.0 : 1.0;
+}
+
+/* Katsevich backprojection with the PI-line window, FP64: vol += sum_t norm[t] U
+ * bilinear(P_t) over views whose source angle lies in the voxel's PI interval, tested on
+ * the virtual detector through the axis by the Tam-Danielsson bounds
+ *   top(u) = (P/2pi)(1 + u^2/D^2)(pi/2 - atan(u/D)),  bottom(u) = -(P/2pi)(1 + u^2/D^2)(pi/2 + atan(u/D))
+ * (Noo, Pack, Heuscher 2003, flat detector at distance D) with u the detector coordinate
+ * along the source's direction of travel (u = -w for a right-handed helix here) and
+ * heights relative to the source.  pitch = source rise per turn (voxels). */
 int orc_katsevich_piwin_f64(double* vol, const float* projections,
                             const int volDim[3], const int volStart[3], const int volEnd[3],
                             const int projDim[3], const int projWHSize[2],
@@ -787,32 +833,41 @@ int orc_katsevich_piwin_f64(double* vol, const float* projections,
 {
   const int n = projDim[2];
   dview* views = make_views(n, angles, hMid, volDim[2], D, pw, NULL);
-  const double turn = n > 1 ? (double)angles[n - 1] - (double)angles[0] : 1.0;
-  const double sgn = ((turn >= 0.0) == (pitch >= 0.0)) ? -1.0 : 1.0;
+  const double sgn = kats_sign(angles, n, pitch);
   const int nx = volEnd[0] - volStart[0], ny = volEnd[1] - volStart[1], nz = volEnd[2] - volStart[2];
-  const double W2 = projDim[0] / 2, H2 = projDim[1] / 2;
   int64_t cnt = 0;
 #pragma omp parallel for collapse(2) schedule(dynamic, 1) reduction(+ : cnt)
   for (int k = 0; k < nz; k++)
     for (int j = 0; j < ny; j++)
-      for (int i = 0; i < nx; i++) {
-        const double x = i + volStart[0] - volDim[0] / 2, y = j + volStart[1] - volDim[1] / 2;
-        const double z = k + volStart[2] - volDim[2] / 2;
-        double acc = 0.0;
-        for (int t = 0; t < n; t++) {
-          const dview* v = &views[t];
-          const double U = D / (D + x * v->ca + y * v->sa);
-          const double w = (y * v->ca - x * v->sa) * U; /* voxel units on the virtual detector */
-          const double h = (z - v->hmp) * U;
-          const double u = sgn * w / D;
-          const double q = (pitch / (2.0 * ORC_PI)) * (1.0 + u * u);
-          if (h > q * (ORC_PI / 2 - atan(u)) || h < -q * (ORC_PI / 2 + atan(u))) continue;
-          cnt++;
-          acc += norm[t] * U * bil_window(projections, projWHSize[0], projWHSize[1], t,
-                                          projWOffset[t], projHOffset[t], w / pw + W2, h / pw + H2);
-        }
-        vol[(size_t)i + (size_t)nx * (j + (size_t)ny * k)] += acc;
-      }
+      for (int i = 0; i < nx; i++)
+        vol[(size_t)i + (size_t)nx * (j + (size_t)ny * k)] +=
+            kats_piwin_voxel_f64(i + volStart[0], j + volStart[1], k + volStart[2], projections,
+                                 volDim, projDim, projWHSize, projWOffset, projHOffset, views, D,
+                                 norm, pw, pitch, sgn, &cnt);
+  free(views);
+  if (pairs) *pairs = cnt;
+  return 0;
+}
+
+/* The same at listed voxels (global indices xyz[3n..3n+2]); *pairs = their in-window
+ * voxel-view pairs. */
+int orc_katsevich_piwin_points_f64(const int* xyz, int npts, double* out,
+                                   const float* projections,
+                                   const int volDim[3], const int projDim[3],
+                                   const int projWHSize[2], const int* projWOffset,
+                                   const int* projHOffset, const float* angles,
+                                   const float* hMid, double D, const float* norm, double pw,
+                                   double pitch, int64_t* pairs)
+{
+  const int n = projDim[2];
+  dview* views = make_views(n, angles, hMid, volDim[2], D, pw, NULL);
+  const double sgn = kats_sign(angles, n, pitch);
+  int64_t cnt = 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : cnt)
+  for (int p = 0; p < npts; p++)
+    out[p] = kats_piwin_voxel_f64(xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2], projections, volDim,
+                                  projDim, projWHSize, projWOffset, projHOffset, views, D, norm, pw,
+                                  pitch, sgn, &cnt);
   free(views);
   if (pairs) *pairs = cnt;
   return 0;

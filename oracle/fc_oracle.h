@@ -118,6 +118,16 @@ int orc_katsevich_piwin_f64(double* vol, const float* projections,
                             const float* angles, const float* hMid, double D,
                             const float* norm, double pw, double pitch, int64_t* pairs);
 
+/* orc_katsevich_piwin_f64 at listed voxels: out[n] for the voxel at global indices
+ * xyz[3n..3n+2]; *pairs = the in-window voxel-view pairs of those voxels. */
+int orc_katsevich_piwin_points_f64(const int* xyz, int npts, double* out,
+                                   const float* projections,
+                                   const int volDim[3], const int projDim[3],
+                                   const int projWHSize[2], const int* projWOffset,
+                                   const int* projHOffset, const float* angles,
+                                   const float* hMid, double D, const float* norm, double pw,
+                                   double pitch, int64_t* pairs);
+
 int orc_backproject_points_f64(const int* xyz, int npts, double* out,
                                const float* projections,
                                const int volDim[3], const int volStart[3], const int volEnd[3],

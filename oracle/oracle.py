@@ -298,6 +298,35 @@ def katsevich_piwin_f64(pb: Problem, proj, pitch):
     return vol, int(pairs.value)
 
 
+def katsevich_piwin_points_f64(pb: Problem, proj, pts, pitch):
+    """katsevich_piwin_f64 at listed voxels (rows of global [x, y, z] indices); returns
+    (values, number of voxel-view pairs of those voxels inside the window)."""
+    proj = np.ascontiguousarray(proj, dtype=np.float32)
+    pts = np.ascontiguousarray(pts, dtype=np.int32)
+    out = np.zeros(len(pts), dtype=np.float64)
+    pairs = ctypes.c_int64(0)
+    rc = lib().orc_katsevich_piwin_points_f64(_p(pts, _i32p), ctypes.c_int(len(pts)), _p(out, _f64p),
+                                              _p(proj, _f32p), _p(pb.volDim, _i32p), _p(pb.projDim, _i32p),
+                                              _p(pb.projWHSize, _i32p), _p(pb.projWOffset, _i32p),
+                                              _p(pb.projHOffset, _i32p), _p(pb.angles, _f32p),
+                                              _p(pb.hMid, _f32p), ctypes.c_double(pb.D), _p(pb.norm, _f32p),
+                                              ctypes.c_double(pb.pw), ctypes.c_double(pitch),
+                                              ctypes.byref(pairs))
+    assert rc == 0
+    return out, int(pairs.value)
+
+
+def column_points(vol_xyz, vol_start, vol_end, ncols, seed=0):
+    """`ncols` random full-z voxel columns of the sub-volume vol_start..vol_end: rows of
+    global [x, y, z] indices, column-major (all z of column 0 first)."""
+    rng = np.random.default_rng(seed)
+    x = rng.integers(vol_start[0], vol_end[0], ncols)
+    y = rng.integers(vol_start[1], vol_end[1], ncols)
+    z = np.arange(vol_start[2], vol_end[2])
+    nz = len(z)
+    return np.stack([np.repeat(x, nz), np.repeat(y, nz), np.tile(z, ncols)], 1).astype(np.int32)
+
+
 def backproject_points_f64(pb: Problem, proj, pts, kernel_mode=2):
     proj = np.ascontiguousarray(proj, dtype=np.float32)
     pts = np.ascontiguousarray(pts, dtype=np.int32)

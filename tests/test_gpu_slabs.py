@@ -1,7 +1,9 @@
 """The slab decomposition with the library's kernels: several ranks' steps driven in one
 process on one GPU (pack -> hand the pieces over -> unpack -> single-GPU kernels on the band
-geometry), assembled and compared with the whole-volume kernels' result.  No rank waits on
-another (the exchange is a list hand-over), so this runs on one GPU."""
+geometry), assembled and compared with the FP64 oracle's whole-volume backprojection
+(rel-L2 <= 2e-5, FP32 arithmetic; the PI-window Katsevich backprojection for the helix) and
+with the whole-volume kernels' result (<= 1e-6: the same kernels on the same data).  No rank
+waits on another (the exchange is a list hand-over), so this runs on one GPU."""
 import numpy as np
 import pytest
 
@@ -42,13 +44,21 @@ def test_slab_backprojection_equals_whole_volume(kind, mode, world):
 
     from fastcone_b200 import ops, slabs
 
+    import bench
+
     g = _geoms()[kind]
     proj = torch.rand(g.proj_shape, device="cuda", generator=torch.Generator("cuda").manual_seed(1))
     want = ops.backproject(proj, g, mode)
     dec = slabs.SlabDecomposition(g, world)
-    got = _emulate_backproject(dec, proj, mode)
+    got = _emulate_backproject(dec, proj, mode).cpu().numpy()
     torch.cuda.synchronize()
-    assert O.rel_l2(got.cpu().numpy(), want.cpu().numpy()) < 1e-6
+    assert O.rel_l2(got, want.cpu().numpy()) < 1e-6
+    pb, ph = bench.oracle_problem(g), proj.cpu().numpy()
+    if kind == "helical":
+        ref, _ = O.katsevich_piwin_f64(pb, ph, g.helical_pitch)
+    else:
+        ref = O.backproject_f64(pb, ph, kernel_mode=mode)
+    assert O.rel_l2(got, ref) < 2e-5, O.rel_l2(got, ref)
     if kind == "helical":
         assert all(len(b.views) < g.nviews for b in dec.bands if b.z1 > b.z0)
 
