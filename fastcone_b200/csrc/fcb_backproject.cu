@@ -275,6 +275,32 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
   return r;
 }
 
+// PI window: of the thread's NZ z-voxels (pairs k = (2k, 2k + 1)), the pairs that can lie
+// inside the window of some lane of the warp, [plo, phi]; the warp skips the others (a
+// uniform branch: no taps loaded, no arithmetic), the per-voxel test still decides inside.
+// h(z_k) = h0 + k dh with dh > 0, so a lane's inside voxels are one run of k; one step of
+// margin on each side covers the rounding of the incremental row positions.
+template <int NACC>
+__device__ __forceinline__ void piw_pairs(float lo, float hi, float h0, float dh, int& plo, int& phi)
+{
+  int a = 0, b = NACC - 1;
+  if (dh > 0.0f) {
+    const float lim = 2.0f * NACC + 4.0f;
+    const float klo = fminf(fmaxf(__fdividef(lo - h0, dh), -4.0f), lim);
+    const float khi = fminf(fmaxf(__fdividef(hi - h0, dh), -4.0f), lim);
+    const int k0 = __float2int_ru(klo) - 1, k1 = __float2int_rd(khi) + 1;
+    if (k1 < k0 || k1 < 0 || k0 > 2 * NACC - 1) {
+      a = NACC;
+      b = -1;
+    } else {
+      a = max(0, k0) >> 1;
+      b = min(2 * NACC - 1, k1) >> 1;
+    }
+  }
+  plo = __reduce_min_sync(0xffffffffu, a);
+  phi = __reduce_max_sync(0xffffffffu, b);
+}
+
 // Resident CTAs per SM the register allocation must allow: 3 (the default 64 KB staging
 // budget fits 3 CTAs) unless NZ = 64 needs the registers of 2.
 template <int NZ>
@@ -474,8 +500,14 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
       const u64 WT2 = pk2(wt, wt);
       const u64 D2 = pk2(2.0f * dh, 2.0f * dh);
       u64 H = pk2(h0, h0 + dh);
+      int plo = 0, phi = NACC - 1;
+      if constexpr (PIW) piw_pairs<NACC>(lo, hi, h0, dh, plo, phi);
 #pragma unroll
       for (int k = 0; k < NACC; k++) {
+        if (PIW && (k < plo || k > phi)) {  // warp-uniform: the pair is outside every lane's window
+          H = add2(H, D2);
+          continue;
+        }
         const u64 T2 = add2_rm(H, MAG2);
         const u64 FH = sub2(H, sub2(T2, MAG2));
         float t0, t1;
@@ -743,8 +775,14 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     const u64 WT2 = pk2(wt, wt);
     const u64 D2 = pk2(2.0f * dh, 2.0f * dh);
     u64 H = pk2(h0, h0 + dh);
+    int plo = 0, phi = NACC - 1;
+    if constexpr (PIW) piw_pairs<NACC>(lo, hi, h0, dh, plo, phi);
 #pragma unroll
     for (int k = 0; k < NACC; k++) {
+      if (PIW && (k < plo || k > phi)) {  // warp-uniform: the pair is outside every lane's window
+        H = add2(H, D2);
+        continue;
+      }
       const u64 T2 = add2_rm(H, MAG2);
       const u64 FH = sub2(H, sub2(T2, MAG2));
       float t0, t1;

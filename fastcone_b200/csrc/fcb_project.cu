@@ -132,12 +132,19 @@ struct Tri {
   int i, j, k;
   float a, b, c;
 };
+// Cell and fractions of a sample position.  Floors by the round-down magic number: for
+// |a| < 2^22, a + 1.5 * 2^23 rounded toward -inf is an integer whose bits hold
+// 0x4B400000 + floor(a), and (a + M) - M == floorf(a) exactly, so the fractions a - floor(a)
+// are the FP32 values floorf would give (sample positions lie within a voxel of the volume).
 __device__ __forceinline__ Tri tri_of(float x, float y, float z)
 {
   Tri t;
-  const float fx = floorf(x), fy = floorf(y), fz = floorf(z);
-  t.i = (int)fx; t.j = (int)fy; t.k = (int)fz;
-  t.a = x - fx; t.b = y - fy; t.c = z - fz;
+  const float M = 12582912.0f;
+  const float tx = __fadd_rd(x, M), ty = __fadd_rd(y, M), tz = __fadd_rd(z, M);
+  t.i = __float_as_int(tx) - 0x4B400000;
+  t.j = __float_as_int(ty) - 0x4B400000;
+  t.k = __float_as_int(tz) - 0x4B400000;
+  t.a = x - (tx - M); t.b = y - (ty - M); t.c = z - (tz - M);
   return t;
 }
 
@@ -334,6 +341,14 @@ __device__ __forceinline__ pj_u64 pj_fma(pj_u64 a, pj_u64 b, pj_u64 c)
 }
 // lerp of both lanes: a + t (b - a), as fmaf(t, b - a, a)
 __device__ __forceinline__ pj_u64 pj_lerp(pj_u64 t, pj_u64 a, pj_u64 b) { return pj_fma(t, pj_sub(b, a), a); }
+// a + b rounded toward -inf in both lanes: with b = 1.5 * 2^23 the result's bits hold
+// floor(a) (|a| < 2^22), and (a + b) - b == floorf(a) exactly
+__device__ __forceinline__ pj_u64 pj_add_rm(pj_u64 a, pj_u64 b)
+{
+  pj_u64 r;
+  asm("add.rm.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
 
 __device__ __forceinline__ float lds32(uint32_t a)
 {
@@ -358,6 +373,12 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
   const uint32_t rowb = (uint32_t)P.BC * 4u, planeb = rowb * (uint32_t)(T + 1);
   const uint32_t ox = XD ? rowb : 4u, oy = XD ? 4u : rowb;
   const int BC1 = P.BC - 1, BZ1 = P.BZ - 1;
+  // floors by the round-down magic number: bits(a + 1.5 * 2^23) = MAGIC_BITS + floor(a)
+  const float MAGIC = 12582912.0f;
+  const int MAGIC_BITS = 0x4B400000;
+  const pj_u64 MAG2 = pj_pk(MAGIC, MAGIC);
+  const pj_u64 D0 = pj_pk(d[0], d[0]), D1 = pj_pk(d[1], d[1]), D2 = pj_pk(d[2], d[2]);
+  const pj_u64 S0 = pj_pk(s[0], s[0]), S1 = pj_pk(s[1], s[1]), S2 = pj_pk(s[2], s[2]);
   float acc = 0.0f;
   int m = m0;
   for (int k = 0; k < nsl; k++) {
@@ -369,26 +390,28 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
     }
     const int4 o = origin[st];
     const int alo = o.y, ahi = o.y + T - 1;
+    // brick-local indices straight from the magic-number bits
+    const int offC = MAGIC_BITS + o.x, offD = MAGIC_BITS + alo, offZ = MAGIC_BITS + o.z;
     const uint32_t stb = sbase + (uint32_t)st * (uint32_t)P.stage_bytes;
     while (m <= m1) {
       if (m + 1 <= m1) {
         // samples m and m+1 in f32x2 lanes, when both are inside the slab and the brick
         const pj_u64 mm = pj_pk((float)m, (float)(m + 1));
-        float x0, x1, y0, y1, z0, z1;
-        pj_up(pj_fma(mm, pj_pk(d[0], d[0]), pj_pk(s[0], s[0])), x0, x1);
-        pj_up(pj_fma(mm, pj_pk(d[1], d[1]), pj_pk(s[1], s[1])), y0, y1);
-        pj_up(pj_fma(mm, pj_pk(d[2], d[2]), pj_pk(s[2], s[2])), z0, z1);
-        const float fx0 = floorf(x0), fx1 = floorf(x1), fy0 = floorf(y0), fy1 = floorf(y1);
-        const float fz0 = floorf(z0), fz1 = floorf(z1);
-        const int i0 = (int)fx0, i1 = (int)fx1, j0 = (int)fy0, j1 = (int)fy1, k0 = (int)fz0, k1 = (int)fz1;
-        const int d0 = XD ? i0 : j0, d1 = XD ? i1 : j1;
-        const int c0 = (XD ? j0 : i0) - o.x, c1 = (XD ? j1 : i1) - o.x;
-        const int e0 = d0 - alo, e1 = d1 - alo, q0 = k0 - o.z, q1 = k1 - o.z;
+        const pj_u64 X = pj_fma(mm, D0, S0), Y = pj_fma(mm, D1, S1), Z = pj_fma(mm, D2, S2);
+        const pj_u64 TX = pj_add_rm(X, MAG2), TY = pj_add_rm(Y, MAG2), TZ = pj_add_rm(Z, MAG2);
+        float tx0, tx1, ty0, ty1, tz0, tz1;
+        pj_up(TX, tx0, tx1);
+        pj_up(TY, ty0, ty1);
+        pj_up(TZ, tz0, tz1);
+        const int c0 = __float_as_int(XD ? ty0 : tx0) - offC, c1 = __float_as_int(XD ? ty1 : tx1) - offC;
+        const int e0 = __float_as_int(XD ? tx0 : ty0) - offD, e1 = __float_as_int(XD ? tx1 : ty1) - offD;
+        const int q0 = __float_as_int(tz0) - offZ, q1 = __float_as_int(tz1) - offZ;
         if ((unsigned)c0 < (unsigned)BC1 && (unsigned)e0 < (unsigned)T && (unsigned)q0 < (unsigned)BZ1 &&
             (unsigned)c1 < (unsigned)BC1 && (unsigned)e1 < (unsigned)T && (unsigned)q1 < (unsigned)BZ1) {
-          const pj_u64 ta = pj_sub(pj_pk(x0, x1), pj_pk(fx0, fx1));
-          const pj_u64 tb = pj_sub(pj_pk(y0, y1), pj_pk(fy0, fy1));
-          const pj_u64 tc = pj_sub(pj_pk(z0, z1), pj_pk(fz0, fz1));
+          // fractions a - floorf(a), the same FP32 operation as tri_of
+          const pj_u64 ta = pj_sub(X, pj_sub(TX, MAG2));
+          const pj_u64 tb = pj_sub(Y, pj_sub(TY, MAG2));
+          const pj_u64 tc = pj_sub(Z, pj_sub(TZ, MAG2));
           const uint32_t p0 = stb + (uint32_t)q0 * planeb + (uint32_t)e0 * rowb + (uint32_t)c0 * 4u;
           const uint32_t p1 = stb + (uint32_t)q1 * planeb + (uint32_t)e1 * rowb + (uint32_t)c1 * 4u;
           const pj_u64 v000 = pj_pk(lds32(p0), lds32(p1));

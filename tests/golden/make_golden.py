@@ -3,6 +3,8 @@ OWN fastcone.py (fastcone.py:260-319) in this container.
 
     python tests/golden/make_golden.py [/path/to/reference] [all|api]
 
+(the reference tree: the first argument, else $FASTCONE_REFERENCE)
+
 It also records the signatures of the module's public functions (names, kinds and defaults
 of their parameters, fastcone.py:52, :147, :260, :272, :294, :306) in fastcone_api.json,
 and, in fastcone_calls.json, the C-ABI arguments that its project / backproject pass for
@@ -106,7 +108,10 @@ def write_api(ref):
         f.write("\n")
 
 
-def main(ref_dir="/root/reference", what="all"):
+def main(ref_dir=None, what="all"):
+    # the reference checkout: the first argument, else $FASTCONE_REFERENCE, else the
+    # conventional location
+    ref_dir = ref_dir or os.environ.get("FASTCONE_REFERENCE", "/root/reference")
     ref = load_reference(ref_dir)
     write_api(ref)
     if what == "api":

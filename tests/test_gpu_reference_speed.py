@@ -1,13 +1,18 @@
-"""Speed against the reference's OWN CUDA path on the same B200 (oracle/_ref: the reference
-sources compiled unmodified, texture references mapped onto texture objects), through the
-same host-buffer entry point (GPU_CB_K_backproject's arguments, fastcone.backproject), on
-the small circular FDK problem: 128^3 voxels, 180 views, 192x128 detector, D = 500,
-pw = 0.5 (3.77e8 voxel-view updates).  Both calls include their host<->device copies and
-set-up; the timings (best of 3 after a warm-up) are printed with -s.
+"""Speed and agreement against the reference's OWN CUDA path on the same B200 (oracle/_ref:
+the reference sources compiled unmodified, texture references mapped onto texture objects),
+through the same host-buffer entry point (GPU_CB_K_backproject's arguments,
+fastcone.backproject, numpy buffers), on three problems:
 
-The 1024^3 / 1440-view comparison runs the same way when FCB_TIME_REFERENCE_LARGE=1 (the
-reference's host-side caching takes tens of seconds there; off by default)."""
-import os
+* the small circular FDK: 128^3 voxels, 180 views, 192x128 detector, D = 500, pw = 0.5;
+* the large circular FDK: 1024^3 voxels, 1440 views, 1536x1024 detector, D = 2000, pw = 0.8
+  (the reference's host-side caching makes its call take about 15 s);
+* the helix: 512x512x384, 4 turns x 1160 views, 736x64, Katsevich weight (the reference has
+  no PI window, so both run dense).
+
+Both calls include their host<->device copies and set-up (best of `reps` after a warm-up;
+printed with -s).  Each test asserts the results agree within the 1e-3 rel-L2 of the
+reference's 8-bit texture weights, and that ours is faster: by 5x on the two large problems
+(the measured margins are larger)."""
 import time
 
 import numpy as np
@@ -24,13 +29,14 @@ def _need_ref():
 
 
 def _best(fn, reps):
-    fn()
+    """(best time of `reps` calls after a warm-up call, the last call's result)"""
+    out = fn()
     best = float("inf")
     for _ in range(reps):
         t0 = time.perf_counter()
-        fn()
+        out = fn()
         best = min(best, time.perf_counter() - t0)
-    return best
+    return best, out
 
 
 def _compare(vol_xyz, det_wh, nviews, D, pw, reps, mode=2, hmid=None, arc=2 * np.pi):
@@ -49,9 +55,9 @@ def _compare(vol_xyz, det_wh, nviews, D, pw, reps, mode=2, hmid=None, arc=2 * np
     def ref():
         return O.reflib_backproject(pb, proj, kernel_mode=mode)
 
-    t_ours = _best(ours, reps)
-    t_ref = _best(ref, reps)
-    err = O.rel_l2(ours(), ref())
+    t_ours, v_ours = _best(ours, reps)
+    t_ref, v_ref = _best(ref, reps)
+    err = O.rel_l2(v_ours, v_ref)
     print(f"\n{vol_xyz} x {nviews} views, mode {mode}: ours {t_ours * 1e3:.1f} ms ({upd / t_ours / 1e9:.1f} GUPS), "
           f"reference CUDA path {t_ref * 1e3:.1f} ms ({upd / t_ref / 1e9:.1f} GUPS), "
           f"ratio {t_ref / t_ours:.1f}, rel-L2 {err:.2e}")
@@ -65,17 +71,13 @@ def test_faster_than_reference_cuda_path_small_fdk():
     assert t_ours < t_ref
 
 
-@pytest.mark.skipif(os.environ.get("FCB_TIME_REFERENCE_LARGE") != "1",
-                    reason="the 1024^3 comparison runs with FCB_TIME_REFERENCE_LARGE=1")
 def test_faster_than_reference_cuda_path_large_fdk():
     _need_ref()
     t_ours, t_ref, err = _compare((1024, 1024, 1024), (1536, 1024), 1440, 2000.0, 0.8, reps=1)
     assert err < 1e-3
-    assert t_ours < t_ref
+    assert t_ref > 5.0 * t_ours, (t_ours, t_ref)
 
 
-@pytest.mark.skipif(os.environ.get("FCB_TIME_REFERENCE_LARGE") != "1",
-                    reason="the helical comparison runs with FCB_TIME_REFERENCE_LARGE=1")
 def test_faster_than_reference_cuda_path_helical_katsevich():
     """The helical geometry (512x512x384, 4 turns x 1160 views, 736x64 detector) through the
     reference's Katsevich backprojection (kernelMode 1: weight U, every view, no PI window --
@@ -86,4 +88,4 @@ def test_faster_than_reference_cuda_path_helical_katsevich():
     t_ours, t_ref, err = _compare((512, 512, 384), (736, 64), n, 1140.0, 1.096, reps=1, mode=1, hmid=hmid,
                                   arc=4 * 2 * np.pi)
     assert err < 1e-3
-    assert t_ours < t_ref
+    assert t_ref > 5.0 * t_ours, (t_ours, t_ref)

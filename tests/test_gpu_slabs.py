@@ -1,9 +1,11 @@
 """The slab decomposition with the library's kernels: several ranks' steps driven in one
 process on one GPU (pack -> hand the pieces over -> unpack -> single-GPU kernels on the band
 geometry), assembled and compared with the FP64 oracle's whole-volume backprojection
-(rel-L2 <= 2e-5, FP32 arithmetic; the PI-window Katsevich backprojection for the helix) and
-with the whole-volume kernels' result (<= 1e-6: the same kernels on the same data).  No rank
-waits on another (the exchange is a list hand-over), so this runs on one GPU."""
+(rel-L2 <= 2e-5, FP32 arithmetic; for the helix the PI-window Katsevich backprojection at
+<= 1e-3: the window is a sharp cut that the kernels decide in FP32 and the oracle in FP64,
+so voxels whose window edge falls within rounding of a view gain or lose that view) and with
+the whole-volume kernels' result (<= 1e-6: the same kernels on the same data).  No rank waits
+on another (the exchange is a list hand-over), so this runs on one GPU."""
 import numpy as np
 import pytest
 
@@ -56,9 +58,11 @@ def test_slab_backprojection_equals_whole_volume(kind, mode, world):
     pb, ph = bench.oracle_problem(g), proj.cpu().numpy()
     if kind == "helical":
         ref, _ = O.katsevich_piwin_f64(pb, ph, g.helical_pitch)
+        tol = 1e-3
     else:
         ref = O.backproject_f64(pb, ph, kernel_mode=mode)
-    assert O.rel_l2(got, ref) < 2e-5, O.rel_l2(got, ref)
+        tol = 2e-5
+    assert O.rel_l2(got, ref) < tol, O.rel_l2(got, ref)
     if kind == "helical":
         assert all(len(b.views) < g.nviews for b in dec.bands if b.z1 > b.z0)
 
