@@ -203,34 +203,68 @@ struct Tap<__nv_bfloat16, OFF> {
   static __device__ __forceinline__ float ld(uint32_t a) { return __uint_as_float(lds_u16<OFF * 2>(a) << 16); }
 };
 
+// Two FP32 taps (addresses a0 + OFF, a1 + OFF) loaded straight into the halves of one 64-bit
+// f32x2 operand.
+template <int OFF>
+__device__ __forceinline__ unsigned long long lds_f32x2(uint32_t a0, uint32_t a1)
+{
+  unsigned long long r;
+  asm volatile(
+      "{\n\t.reg .f32 lo, hi;\n\t"
+      "ld.shared.f32 lo, [%1+%3];\n\t"
+      "ld.shared.f32 hi, [%2+%3];\n\t"
+      "mov.b64 %0, {lo, hi};\n\t}"
+      : "=l"(r)
+      : "r"(a0), "r"(a1), "n"(OFF));
+  return r;
+}
+
 // ---- 16-bit tap pairs: a staged 16-bit box rewritten as 32-bit words, word (r, c) holding
 // tap (r, c) in its low half and tap (r, c + 1) in its high half, so that one 32-bit
 // ld.shared gives both horizontal taps of a row
-template <int OFF>
-__device__ __forceinline__ uint32_t lds_b32(uint32_t a)
-{
-  uint32_t v;
-  asm volatile("ld.shared.b32 %0, [%1+%2];" : "=r"(v) : "r"(a), "n"(OFF));
-  return v;
-}
+// A row's taps for two voxels from their tap-pair words at shared addresses a0, a1: LO =
+// (tap c of voxel 0, tap c of voxel 1), HI = (tap c + 1 of voxel 0, of voxel 1), as f32x2
+// operands written straight into their 64-bit registers.
 template <typename T>
-struct PairTap;
+__device__ __forceinline__ void lds_pair_taps(uint32_t a0, uint32_t a1, unsigned long long& LO,
+                                              unsigned long long& HI);
 template <>
-struct PairTap<__nv_bfloat16> {
-  static __device__ __forceinline__ float lo(uint32_t w) { return __uint_as_float(w << 16); }
-  static __device__ __forceinline__ float hi(uint32_t w) { return __uint_as_float(w & 0xffff0000u); }
-};
+__device__ __forceinline__ void lds_pair_taps<__nv_bfloat16>(uint32_t a0, uint32_t a1, unsigned long long& LO,
+                                                             unsigned long long& HI)
+{
+  asm volatile(
+      "{\n\t.reg .b32 p, q, l0, l1, h0, h1;\n\t"
+      "ld.shared.b32 p, [%2];\n\t"
+      "ld.shared.b32 q, [%3];\n\t"
+      "shl.b32 l0, p, 16;\n\t"
+      "shl.b32 l1, q, 16;\n\t"
+      "and.b32 h0, p, 0xffff0000;\n\t"
+      "and.b32 h1, q, 0xffff0000;\n\t"
+      "mov.b64 %0, {l0, l1};\n\t"
+      "mov.b64 %1, {h0, h1};\n\t}"
+      : "=l"(LO), "=l"(HI)
+      : "r"(a0), "r"(a1));
+}
 template <>
-struct PairTap<__half> {
-  static __device__ __forceinline__ float lo(uint32_t w)
-  {
-    return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu)));
-  }
-  static __device__ __forceinline__ float hi(uint32_t w)
-  {
-    return __half2float(__ushort_as_half((unsigned short)(w >> 16)));
-  }
-};
+__device__ __forceinline__ void lds_pair_taps<__half>(uint32_t a0, uint32_t a1, unsigned long long& LO,
+                                                      unsigned long long& HI)
+{
+  asm volatile(
+      "{\n\t.reg .b32 p, q;\n\t.reg .b16 p0, p1, q0, q1;\n\t.reg .f32 l0, l1, h0, h1;\n\t"
+      "ld.shared.b32 p, [%2];\n\t"
+      "ld.shared.b32 q, [%3];\n\t"
+      "mov.b32 {p0, p1}, p;\n\t"
+      "mov.b32 {q0, q1}, q;\n\t"
+      "cvt.f32.f16 l0, p0;\n\t"
+      "cvt.f32.f16 l1, q0;\n\t"
+      "cvt.f32.f16 h0, p1;\n\t"
+      "cvt.f32.f16 h1, q1;\n\t"
+      "mov.b64 %0, {l0, l1};\n\t"
+      "mov.b64 %1, {h0, h1};\n\t}"
+      : "=l"(LO), "=l"(HI)
+      : "r"(a0), "r"(a1));
+}
+
 // 8 staged 16-bit taps q (columns c .. c+7) and the first two of the next 16-byte chunk
 // (nx) -> the pair words of columns c .. c+7
 __device__ __forceinline__ void pair8(uint4 q, uint32_t nx, uint4& lo, uint4& hi)
@@ -515,10 +549,10 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         const uint32_t a0 = (uint32_t)__float_as_uint(t0) * rowb + base;
         const uint32_t a1 = (uint32_t)__float_as_uint(t1) * rowb + base;
         const uint32_t c0 = a0 + rowb, c1 = a1 + rowb;
-        const u64 A = pk2(Tap<T, 0>::ld(a0), Tap<T, 0>::ld(a1));
-        const u64 B = pk2(Tap<T, 1>::ld(a0), Tap<T, 1>::ld(a1));
-        const u64 C = pk2(Tap<T, 0>::ld(c0), Tap<T, 0>::ld(c1));
-        const u64 Dd = pk2(Tap<T, 1>::ld(c0), Tap<T, 1>::ld(c1));
+        const u64 A = lds_f32x2<0>(a0, a1);
+        const u64 B = lds_f32x2<4>(a0, a1);
+        const u64 C = lds_f32x2<0>(c0, c1);
+        const u64 Dd = lds_f32x2<4>(c0, c1);
         const u64 R0 = fma2(FW2, sub2(B, A), A);
         const u64 R1 = fma2(FW2, sub2(Dd, C), C);
         const u64 VAL = fma2(FH, sub2(R1, R0), R0);
@@ -789,12 +823,9 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
       up2(T2, t0, t1);
       const uint32_t a0 = (uint32_t)__float_as_uint(t0) * rowb + base;
       const uint32_t a1 = (uint32_t)__float_as_uint(t1) * rowb + base;
-      const uint32_t p0 = lds_b32<0>(a0), p1 = lds_b32<0>(a1);
-      const uint32_t q0 = lds_b32<0>(a0 + rowb), q1 = lds_b32<0>(a1 + rowb);
-      const u64 A = pk2(PairTap<T>::lo(p0), PairTap<T>::lo(p1));
-      const u64 B = pk2(PairTap<T>::hi(p0), PairTap<T>::hi(p1));
-      const u64 C = pk2(PairTap<T>::lo(q0), PairTap<T>::lo(q1));
-      const u64 Dd = pk2(PairTap<T>::hi(q0), PairTap<T>::hi(q1));
+      u64 A, B, C, Dd;
+      lds_pair_taps<T>(a0, a1, A, B);
+      lds_pair_taps<T>(a0 + rowb, a1 + rowb, C, Dd);
       const u64 R0 = fma2(FW2, sub2(B, A), A);
       const u64 R1 = fma2(FW2, sub2(Dd, C), C);
       const u64 VAL = fma2(FH, sub2(R1, R0), R0);

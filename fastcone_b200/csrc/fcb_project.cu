@@ -379,6 +379,7 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
   const pj_u64 MAG2 = pj_pk(MAGIC, MAGIC);
   const pj_u64 D0 = pj_pk(d[0], d[0]), D1 = pj_pk(d[1], d[1]), D2 = pj_pk(d[2], d[2]);
   const pj_u64 S0 = pj_pk(s[0], s[0]), S1 = pj_pk(s[1], s[1]), S2 = pj_pk(s[2], s[2]);
+  const float sD = XD ? s[0] : s[1], dD = XD ? d[0] : d[1];  // along the dominant axis
   float acc = 0.0f;
   int m = m0;
   for (int k = 0; k < nsl; k++) {
@@ -393,61 +394,77 @@ __device__ __forceinline__ float brick_consume(const PjParams& P, unsigned char*
     // brick-local indices straight from the magic-number bits
     const int offC = MAGIC_BITS + o.x, offD = MAGIC_BITS + alo, offZ = MAGIC_BITS + o.z;
     const uint32_t stb = sbase + (uint32_t)st * (uint32_t)P.stage_bytes;
-    while (m <= m1) {
-      if (m + 1 <= m1) {
-        // samples m and m+1 in f32x2 lanes, when both are inside the slab and the brick
-        const pj_u64 mm = pj_pk((float)m, (float)(m + 1));
-        const pj_u64 X = pj_fma(mm, D0, S0), Y = pj_fma(mm, D1, S1), Z = pj_fma(mm, D2, S2);
-        const pj_u64 TX = pj_add_rm(X, MAG2), TY = pj_add_rm(Y, MAG2), TZ = pj_add_rm(Z, MAG2);
-        float tx0, tx1, ty0, ty1, tz0, tz1;
-        pj_up(TX, tx0, tx1);
-        pj_up(TY, ty0, ty1);
-        pj_up(TZ, tz0, tz1);
-        const int c0 = __float_as_int(XD ? ty0 : tx0) - offC, c1 = __float_as_int(XD ? ty1 : tx1) - offC;
-        const int e0 = __float_as_int(XD ? tx0 : ty0) - offD, e1 = __float_as_int(XD ? tx1 : ty1) - offD;
-        const int q0 = __float_as_int(tz0) - offZ, q1 = __float_as_int(tz1) - offZ;
-        if ((unsigned)c0 < (unsigned)BC1 && (unsigned)e0 < (unsigned)T && (unsigned)q0 < (unsigned)BZ1 &&
-            (unsigned)c1 < (unsigned)BC1 && (unsigned)e1 < (unsigned)T && (unsigned)q1 < (unsigned)BZ1) {
-          // fractions a - floorf(a), the same FP32 operation as tri_of
-          const pj_u64 ta = pj_sub(X, pj_sub(TX, MAG2));
-          const pj_u64 tb = pj_sub(Y, pj_sub(TY, MAG2));
-          const pj_u64 tc = pj_sub(Z, pj_sub(TZ, MAG2));
-          const uint32_t p0 = stb + (uint32_t)q0 * planeb + (uint32_t)e0 * rowb + (uint32_t)c0 * 4u;
-          const uint32_t p1 = stb + (uint32_t)q1 * planeb + (uint32_t)e1 * rowb + (uint32_t)c1 * 4u;
-          const pj_u64 v000 = pj_pk(lds32(p0), lds32(p1));
-          const pj_u64 v100 = pj_pk(lds32(p0 + ox), lds32(p1 + ox));
-          const pj_u64 v010 = pj_pk(lds32(p0 + oy), lds32(p1 + oy));
-          const pj_u64 v110 = pj_pk(lds32(p0 + ox + oy), lds32(p1 + ox + oy));
-          const pj_u64 v001 = pj_pk(lds32(p0 + planeb), lds32(p1 + planeb));
-          const pj_u64 v101 = pj_pk(lds32(p0 + planeb + ox), lds32(p1 + planeb + ox));
-          const pj_u64 v011 = pj_pk(lds32(p0 + planeb + oy), lds32(p1 + planeb + oy));
-          const pj_u64 v111 = pj_pk(lds32(p0 + planeb + ox + oy), lds32(p1 + planeb + ox + oy));
-          const pj_u64 x00 = pj_lerp(ta, v000, v100), x10 = pj_lerp(ta, v010, v110);
-          const pj_u64 x01 = pj_lerp(ta, v001, v101), x11 = pj_lerp(ta, v011, v111);
-          const pj_u64 yy0 = pj_lerp(tb, x00, x10), yy1 = pj_lerp(tb, x01, x11);
-          float r0, r1;
-          pj_up(pj_lerp(tc, yy0, yy1), r0, r1);
-          acc += r0;
-          acc += r1;
-          m += 2;
-          continue;
-        }
-      }
-      const float mf = (float)m;
+    // one sample from the staged brick, or from global memory when its taps leave the brick
+    auto single = [&](int q) -> float {
+      const float mf = (float)q;
       const Tri t = tri_of(fmaf(mf, d[0], s[0]), fmaf(mf, d[1], s[1]), fmaf(mf, d[2], s[2]));
-      const int idom = XD ? t.i : t.j;
-      if (sgn > 0 ? idom > ahi : idom < alo) break;
-      const int ic = (XD ? t.j : t.i) - o.x, id = idom - alo, iz = t.k - o.z;
-      float val;
+      const int ic = (XD ? t.j : t.i) - o.x, id = (XD ? t.i : t.j) - alo, iz = t.k - o.z;
       if ((unsigned)ic < (unsigned)BC1 && (unsigned)id < (unsigned)T && (unsigned)iz < (unsigned)BZ1) {
         // taps outside the volume are the brick's zero fill
         const uint32_t p = stb + (uint32_t)iz * planeb + (uint32_t)id * rowb + (uint32_t)ic * 4u;
-        val = tri_lerp(t, lds32(p), lds32(p + ox), lds32(p + oy), lds32(p + ox + oy), lds32(p + planeb),
-                       lds32(p + planeb + ox), lds32(p + planeb + oy), lds32(p + planeb + ox + oy));
-      } else {
-        val = tri_fetch(P.vol, P.nx, P.ny, P.nz, t);
+        return tri_lerp(t, lds32(p), lds32(p + ox), lds32(p + oy), lds32(p + ox + oy), lds32(p + planeb),
+                        lds32(p + planeb + ox), lds32(p + planeb + oy), lds32(p + planeb + ox + oy));
       }
-      acc += val;
+      return tri_fetch(P.vol, P.nx, P.ny, P.nz, t);
+    };
+    // The ray's last sample in this slab.  Samples advance along the dominant axis in the
+    // bundle's direction, so sample q is in the slab until its dominant floor (the same fmaf
+    // and floor as the sample's own position) passes the slab's far plane: estimate the
+    // crossing, then step to the exact sample.
+    int mend = m - 1;
+    if (m <= m1) {
+      auto inside = [&](int q) {
+        const int f = __float_as_int(__fadd_rd(fmaf((float)q, dD, sD), MAGIC)) - MAGIC_BITS;
+        return sgn > 0 ? f <= ahi : f >= alo;
+      };
+      const float cross = __fdividef((float)(sgn > 0 ? ahi + 1 : alo) - sD, dD);
+      int me = (int)fminf(fmaxf(floorf(cross), (float)(m - 1)), (float)m1);
+      while (me + 1 <= m1 && inside(me + 1)) me++;
+      while (me >= m && !inside(me)) me--;
+      mend = me;
+    }
+    for (; m + 1 <= mend; m += 2) {
+      // samples m and m+1 in f32x2 lanes, when both have their taps inside the brick
+      const pj_u64 mm = pj_pk((float)m, (float)(m + 1));
+      const pj_u64 X = pj_fma(mm, D0, S0), Y = pj_fma(mm, D1, S1), Z = pj_fma(mm, D2, S2);
+      const pj_u64 TX = pj_add_rm(X, MAG2), TY = pj_add_rm(Y, MAG2), TZ = pj_add_rm(Z, MAG2);
+      float tx0, tx1, ty0, ty1, tz0, tz1;
+      pj_up(TX, tx0, tx1);
+      pj_up(TY, ty0, ty1);
+      pj_up(TZ, tz0, tz1);
+      const int c0 = __float_as_int(XD ? ty0 : tx0) - offC, c1 = __float_as_int(XD ? ty1 : tx1) - offC;
+      const int e0 = __float_as_int(XD ? tx0 : ty0) - offD, e1 = __float_as_int(XD ? tx1 : ty1) - offD;
+      const int q0 = __float_as_int(tz0) - offZ, q1 = __float_as_int(tz1) - offZ;
+      if ((unsigned)c0 < (unsigned)BC1 && (unsigned)e0 < (unsigned)T && (unsigned)q0 < (unsigned)BZ1 &&
+          (unsigned)c1 < (unsigned)BC1 && (unsigned)e1 < (unsigned)T && (unsigned)q1 < (unsigned)BZ1) {
+        // fractions a - floorf(a), the same FP32 operation as tri_of
+        const pj_u64 ta = pj_sub(X, pj_sub(TX, MAG2));
+        const pj_u64 tb = pj_sub(Y, pj_sub(TY, MAG2));
+        const pj_u64 tc = pj_sub(Z, pj_sub(TZ, MAG2));
+        const uint32_t p0 = stb + (uint32_t)q0 * planeb + (uint32_t)e0 * rowb + (uint32_t)c0 * 4u;
+        const uint32_t p1 = stb + (uint32_t)q1 * planeb + (uint32_t)e1 * rowb + (uint32_t)c1 * 4u;
+        const pj_u64 v000 = pj_pk(lds32(p0), lds32(p1));
+        const pj_u64 v100 = pj_pk(lds32(p0 + ox), lds32(p1 + ox));
+        const pj_u64 v010 = pj_pk(lds32(p0 + oy), lds32(p1 + oy));
+        const pj_u64 v110 = pj_pk(lds32(p0 + ox + oy), lds32(p1 + ox + oy));
+        const pj_u64 v001 = pj_pk(lds32(p0 + planeb), lds32(p1 + planeb));
+        const pj_u64 v101 = pj_pk(lds32(p0 + planeb + ox), lds32(p1 + planeb + ox));
+        const pj_u64 v011 = pj_pk(lds32(p0 + planeb + oy), lds32(p1 + planeb + oy));
+        const pj_u64 v111 = pj_pk(lds32(p0 + planeb + ox + oy), lds32(p1 + planeb + ox + oy));
+        const pj_u64 x00 = pj_lerp(ta, v000, v100), x10 = pj_lerp(ta, v010, v110);
+        const pj_u64 x01 = pj_lerp(ta, v001, v101), x11 = pj_lerp(ta, v011, v111);
+        const pj_u64 yy0 = pj_lerp(tb, x00, x10), yy1 = pj_lerp(tb, x01, x11);
+        float r0, r1;
+        pj_up(pj_lerp(tc, yy0, yy1), r0, r1);
+        acc += r0;
+        acc += r1;
+      } else {
+        acc += single(m);
+        acc += single(m + 1);
+      }
+    }
+    if (m <= mend) {
+      acc += single(m);
       m++;
     }
     __syncwarp();
