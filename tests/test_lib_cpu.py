@@ -97,3 +97,32 @@ def test_geometry_helpers():
     assert h.nviews == 4640 and h.helical_pitch == pytest.approx(80.0)
     assert h.pw == pytest.approx(1.0 * 570 / 1040 / 0.5)
     assert np.allclose(np.diff(h.hmid.astype(np.float64)), 80.0 / 1160, atol=1e-3)
+
+
+def test_new_entry_points_refuse_bad_arguments_before_device_work():
+    """fcb_fbp_host, fcb_smem_bandwidth, fcb_bp_plan_set_test_stall and
+    fcb_katsevich_pi_pairs check their arguments first and return FCB_ERR_INVALID."""
+    from fastcone_b200 import _lib
+    from tests._cases import make_case
+
+    L = _lib.lib()
+    g, _ = make_case()
+    s = g.struct()
+    proj = np.zeros(g.proj_shape, np.float32)
+    vol = np.zeros(g.vol_shape, np.float32)
+    z = np.zeros(g.nviews, np.float32)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    fz = z.ctypes.data_as(_lib.c_float_p)
+    assert L.fcb_fbp_host(0, ctypes.byref(s), 9, 100.0, fz, 1, vp(proj), vp(vol)) == _lib.FCB_ERR_INVALID
+    assert b"window" in L.fcb_last_error()
+    assert L.fcb_fbp_host(0, ctypes.byref(s), 0, 0.0, fz, 1, vp(proj), vp(vol)) == _lib.FCB_ERR_INVALID
+    assert L.fcb_fbp_host(0, ctypes.byref(s), 0, 100.0, fz, 1, None, vp(vol)) == _lib.FCB_ERR_INVALID
+    ms, nb = ctypes.c_float(), ctypes.c_double()
+    assert L.fcb_smem_bandwidth(3, 10, ctypes.byref(ms), ctypes.byref(nb), None) == _lib.FCB_ERR_INVALID
+    assert L.fcb_smem_bandwidth(4, 0, ctypes.byref(ms), ctypes.byref(nb), None) == _lib.FCB_ERR_INVALID
+    assert L.fcb_bp_plan_set_test_stall(None, 1, 1000) == _lib.FCB_ERR_INVALID
+    n = ctypes.c_longlong()
+    assert L.fcb_katsevich_pi_pairs(None, ctypes.byref(n), None) == _lib.FCB_ERR_INVALID
+    # a circular geometry has no PI window
+    assert L.fcb_katsevich_pi_pairs(ctypes.byref(s), ctypes.byref(n), None) == _lib.FCB_ERR_INVALID
+    assert b"pitch" in L.fcb_last_error()
