@@ -289,10 +289,11 @@ struct FbpFilter {
 
 // Host-buffer backprojection, pipelined over view chunks and z-slabs of the volume:
 //   copy-in stream : the first view chunk, the volume slab by slab, then the other chunks
-//   compute stream : chunk by chunk as they arrive (filtered first when `ff` is set), each
-//                    over all slabs (slab s of the first chunk as soon as slab s is in)
+//   compute stream : chunk by chunk as they arrive, each over all slabs (slab s of the first
+//                    chunk as soon as slab s is in)
 //   copy-out stream: slab s back to the host as soon as the last chunk has passed over it
-//   (filter: a fourth stream returns each filtered chunk as soon as it is filtered)
+//   (with `ff`: a filter stream filters each chunk as it lands, ahead of its backprojection,
+//   and a fourth stream returns each filtered chunk to the caller)
 // so the PCIe traffic (projections once, the volume in and out) hides behind the kernels
 // except for the first chunk with the first slab, and the last slab.  One plan (one staging
 // pre-pass) serves every slab: a slab is a range of the plan's z tiles.  Reference-compatible
@@ -353,7 +354,7 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
   float *dvol = nullptr, *dproj = nullptr, *dz = nullptr;
   FCB_TRY(sc.alloc((void**)&dvol, nvox * sizeof(float)));
   FCB_TRY(sc.alloc((void**)&dproj, (size_t)n * H * wpad * sizeof(float)));
-  cudaStream_t cs, xs, os, ps = nullptr;
+  cudaStream_t cs, xs, os, ps = nullptr, fs = nullptr;
   FCB_TRY(sc.stream(&cs));
   FCB_TRY(sc.stream(&xs));
   FCB_TRY(sc.stream(&os));
@@ -364,20 +365,21 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
     ~FilterGuard()
     {
       if (p) {
-        cudaStreamSynchronize(s);  // the plan's scratch is in use until the compute stream ends
+        cudaStreamSynchronize(s);  // the plan's scratch is in use until the filter stream ends
         filter_plan_destroy(p);
       }
     }
-  } fguard{fplan, cs};
+  } fguard{fplan, fs};
   std::vector<cudaEvent_t> filt_done(ranges.size(), nullptr);
   if (ff) {
     int maxc = 1;
     for (const auto& r : ranges) maxc = std::max(maxc, r.second - r.first);
+    FCB_TRY(sc.stream(&fs));
     FCB_TRY(filter_plan_create(maxc, H, W, FCB_F32, ff->window, 0.125, &fplan));
     FCB_TRY(sc.stream(&ps));
     if (ff->cosine) {
       FCB_TRY(sc.alloc((void**)&dz, (size_t)n * sizeof(float)));
-      FCB_CUDA_TRY(cudaMemcpyAsync(dz, ff->zOrigin, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, cs));
+      FCB_CUDA_TRY(cudaMemcpyAsync(dz, ff->zOrigin, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, fs));
     }
   }
   const double t_alloc = tr.ms();
@@ -391,15 +393,17 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
   HostStager* pst = proj_pg && stager.ok ? &stager : nullptr;
   HostStager* vst = vol_pg && stager.ok ? &stager : nullptr;
   HostStager* fst = out_pg && stager.ok && wpad == W ? &stager : nullptr;
-  // filter chunk c in place (compute stream), then return it to the caller: on its own
-  // stream at once, or (pageable output through the pinned ring) after every kernel is queued
-  auto filter_chunk = [&](int c) -> int {
-    if (!ff) return FCB_OK;
+  // filter chunk c in place on the filter stream once `uploaded` has fired (so the next
+  // chunk's filter overlaps this chunk's backprojection), then return it to the caller: on its
+  // own stream at once, or (pageable output through the pinned ring) after every kernel is
+  // queued.  The compute stream waits for filt_done[c] before backprojecting chunk c.
+  auto filter_chunk = [&](int c, cudaEvent_t uploaded) -> int {
     const int v0 = ranges[c].first, nv = ranges[c].second - v0;
     float* p = dproj + (size_t)v0 * H * wpad;
-    FCB_TRY(filter_plan_run(fplan, p, p, nv, wpad, ff->D, ff->cosine ? dz + v0 : nullptr, ff->cosine, cs));
+    FCB_CUDA_TRY(cudaStreamWaitEvent(fs, uploaded, 0));
+    FCB_TRY(filter_plan_run(fplan, p, p, nv, wpad, ff->D, ff->cosine ? dz + v0 : nullptr, ff->cosine, fs));
     FCB_TRY(sc.event(&filt_done[c]));
-    FCB_CUDA_TRY(cudaEventRecord(filt_done[c], cs));
+    FCB_CUDA_TRY(cudaEventRecord(filt_done[c], fs));
     if (!fst) {
       FCB_CUDA_TRY(cudaStreamWaitEvent(ps, filt_done[c], 0));
       float* h = ff->out + (size_t)v0 * H * W;
@@ -453,8 +457,12 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
     FCB_TRY(copy_proj_h2d(dproj, projections, ranges[c].first, ranges[c].second, W, H, wpad, xs, pst));
     FCB_TRY(sc.event(&ev));
     FCB_CUDA_TRY(cudaEventRecord(ev, xs));
-    FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
-    FCB_TRY(filter_chunk(c));
+    if (ff) {
+      FCB_TRY(filter_chunk(c, ev));
+      FCB_CUDA_TRY(cudaStreamWaitEvent(cs, filt_done[c], 0));
+    } else {
+      FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ev, 0));
+    }
     for (int s = 0; s < nslab; s++) {
       if (c == 0) FCB_TRY(copy_vol_slab(s));
       FCB_TRY(bp_plan_execute_range(plan, c, z0[s], z1[s], dproj, dvol, cs));
@@ -467,13 +475,11 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
     FCB_TRY(copy_proj_h2d(dproj, projections, ranges[c].first, ranges[c].second, W, H, wpad, xs, pst));
     FCB_TRY(sc.event(&up[c]));
     FCB_CUDA_TRY(cudaEventRecord(up[c], xs));
+    if (ff) FCB_TRY(filter_chunk(c, up[c]));
   }
   for (int s = 0; s < nslab; s++) {
     for (int c = cm; c < nch; c++) {
-      if (s == 0) {
-        FCB_CUDA_TRY(cudaStreamWaitEvent(cs, up[c], 0));
-        FCB_TRY(filter_chunk(c));
-      }
+      if (s == 0) FCB_CUDA_TRY(cudaStreamWaitEvent(cs, ff ? filt_done[c] : up[c], 0));
       FCB_TRY(bp_plan_execute_range(plan, c, z0[s], z1[s], dproj, dvol, cs));
     }
     FCB_TRY(finish_slab(s));
@@ -497,6 +503,7 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
   if (tr.on) FCB_CUDA_TRY(cudaEventRecord(tev[3], os));
   FCB_CUDA_TRY(cudaStreamSynchronize(os));
   if (ps) FCB_CUDA_TRY(cudaStreamSynchronize(ps));
+  if (fs) FCB_CUDA_TRY(cudaStreamSynchronize(fs));
   FCB_CUDA_TRY(cudaStreamSynchronize(cs));
   FCB_TRY(collect_device_status(cs));
   if (tr.on) {

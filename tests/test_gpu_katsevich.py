@@ -94,3 +94,30 @@ def test_katsevich_plan_equals_one_shot():
         got = plan(p)
         torch.cuda.synchronize()
         assert torch.equal(got, ref)
+
+
+@pytest.mark.parametrize("dtype_name,tol", [("float16", 2e-3), ("bfloat16", 1e-2)])
+def test_pi_window_16bit_storage(dtype_name, tol):
+    """The PI-window backprojection with FP16 / BF16-stored projections (fdk_pair_kernel with
+    the window) vs the FP64 oracle on the same data, within the storage type's rounding, and
+    vs the FP32 kernel on the same 16-bit values (the same window decisions: <= 1e-5)."""
+    import dataclasses
+
+    import torch
+
+    from fastcone_b200 import _lib, ops
+
+    g = _helix()
+    dlam = float(g.angles[-1] - g.angles[0]) / (g.nviews - 1)
+    g = dataclasses.replace(g, norm=np.full(g.nviews, dlam / (2 * math.pi * g.D), np.float32))
+    pb, vol, proj = _data(g)
+    pb.norm[:] = g.norm
+    p16 = torch.from_numpy(proj).cuda().to(getattr(torch, dtype_name))
+    plan = ops.BackprojectPlan(g, mode=_lib.MODE_KATSEVICH, dtype=p16.dtype)
+    assert plan.info()["box_w"] > 0
+    got = plan(p16, torch.zeros(g.vol_shape, device="cuda"))
+    ops.sync_status()
+    ref, _ = O.katsevich_piwin_f64(pb, proj, g.helical_pitch)
+    assert O.rel_l2(got.cpu().numpy(), ref) < tol, O.rel_l2(got.cpu().numpy(), ref)
+    same = ops.backproject(p16.float(), g, mode=_lib.MODE_KATSEVICH)
+    assert O.rel_l2(got.cpu().numpy(), same.cpu().numpy()) < 1e-5
