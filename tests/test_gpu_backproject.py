@@ -276,15 +276,3 @@ def test_host_driver_staging_of_large_pageable_buffers():
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
     assert not np.array_equal(outs[0][0], vol0)
-
-
-@pytest.mark.parametrize("mode,kw", [(2, {}), (0, {}), (2, dict(vol_xyz=(70, 66, 40), det_wh=(120, 48), pw=0.45))])
-def test_compile_time_row_pitch_matches_fp64(monkeypatch, mode, kw):
-    """FCB_FDK_RP=1: the staged box's width rounded up to a compile-time row pitch (32 / 48 /
-    64 / 96 / 128 taps) gives the FP64 result like the run-time pitch (<= 2e-5)."""
-    monkeypatch.setenv("FCB_FDK_RP", "1")
-    g, pb = make_case(**kw)
-    proj, _ = smooth_projections(pb)
-    got = _bp(g, proj, mode)
-    ref64 = O.backproject_f64(pb, proj, kernel_mode=mode)
-    assert O.rel_l2(got, ref64) < 2e-5, O.rel_l2(got, ref64)
