@@ -356,6 +356,10 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   uint64_t* empty = full + P.stages;
   // per stage: box origin w, h; view (-1: end of the list); rows the tile's footprint needs
   int4* origin = reinterpret_cast<int4*>(empty + P.stages);
+  // per stage: the staged view's parameters, copied by the producer so that the consumers read
+  // them from shared memory (the views of a launch overflow the constant cache while the
+  // CTAs of an SM work on different views)
+  FdkView* vstage = reinterpret_cast<FdkView*>(origin + P.stages);
   const uint32_t smem_base = dev::smem_u32(smem_raw);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -407,6 +411,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
             } else {
               if (snw > P.BW || snh > P.BH) dev::record_status(P.status, DEV_RANGE);
               origin[s] = make_int4(sw0, sh0, vb + l, snh);
+              vstage[s] = P.v[vb + l];
               dev::mbar_arrive_expect_tx(&full[s], bytes);
               dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], sw0, sh0,
                                P.view0 + vb + l);
@@ -439,6 +444,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         }
         if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
         origin[s] = make_int4(w0, h0, v, nh);
+        vstage[s] = P.v[v];
         dev::mbar_arrive_expect_tx(&full[s], bytes);
         dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + v);
         issued++;
@@ -493,7 +499,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
     const int4 org = origin[s];
     const int v = PIW ? org.z : j;
     if (PIW && v < 0) break;
-    const FdkView& V = P.v[v];
+    const FdkView V = vstage[s];
 
     const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
     const float U = __frcp_rn(den);
@@ -632,14 +638,12 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
   const int S = P.stages, NP = P.pbufs;
   const int stage_elems = P.BW * P.BH;
   const int stage_bytes = ((stage_elems * 2) + 127) & ~127;
-  // pair-buffer row pitch in words: BW is a multiple of 8, so BW + 4 (= 4 mod 8) puts the
-  // same column of consecutive rows in different banks
-  const int PW = P.BW + 4;
-  const int pbuf_bytes = ((P.BH * PW * 4) + 127) & ~127;
+  const int pbuf_bytes = ((stage_elems * 4) + 127) & ~127;
   unsigned char* pairs = smem_raw + (size_t)S * stage_bytes;
   int4* origin2 = reinterpret_cast<int4*>(pairs + (size_t)NP * pbuf_bytes);  // per pair buffer
   int4* sorg = origin2 + NP;                                                   // per TMA stage
-  uint64_t* full = reinterpret_cast<uint64_t*>(sorg + S);
+  FdkView* vpair = reinterpret_cast<FdkView*>(sorg + S);  // per pair buffer: its view's parameters
+  uint64_t* full = reinterpret_cast<uint64_t*>(vpair + NP);
   uint64_t* full2 = full + S;
   uint64_t* empty2 = full2 + NP;
 
@@ -705,7 +709,6 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     for (int k = 0; k < S; k++) issue_next();
     const int cpr = P.BW / 8;  // 16-byte chunks per row (BW is a multiple of 8)
     const int nbox = P.BH * cpr;
-    const float inv_cpr = 1.0f / (float)cpr;  // row of chunk e: floor((e + 1/2) / cpr), exact here
     while (conv < issued) {
       const int s = conv % S, p = conv % NP;
       bool ok = dev::mbar_wait(&full[s], (conv / S) & 1);
@@ -723,14 +726,15 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
       const int nconv = min(o.w, P.BH) * cpr;
       for (int e = lane; e < nconv; e += 32) {
         const uint32_t nx = e + 1 < nbox ? reinterpret_cast<const uint32_t*>(src + e + 1)[0] : 0u;
-        const int row = __float2int_rz(((float)e + 0.5f) * inv_cpr), cc = e - row * cpr;
         uint4 lo, hi;
         pair8(src[e], nx, lo, hi);
-        uint4* d = dst + row * (PW / 4) + 2 * cc;
-        d[0] = lo;
-        d[1] = hi;
+        dst[2 * e] = lo;
+        dst[2 * e + 1] = hi;
       }
-      if (lane == 0) origin2[p] = o;
+      if (lane == 0) {
+        origin2[p] = o;
+        vpair[p] = P.v[o.z];
+      }
       __syncwarp();
       dev::mbar_arrive(&full2[p]);  // all 32 lanes: their writes are released to the consumers
       conv++;
@@ -765,7 +769,7 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
   const float x = P.ox + (float)xl, y = P.oy + (float)yl, zf = P.oz + (float)zl;
   const float MAGIC = 12582912.0f;  // 1.5 * 2^23: adding it in round-down mode floors
   const uint32_t MAGIC_BITS = 0x4B400000u;
-  const uint32_t rowb = (uint32_t)(PW * 4);  // bytes per row of a pair buffer
+  const uint32_t rowb = (uint32_t)(P.BW * 4);  // bytes per row of a pair buffer
   const uint32_t pair0 = dev::smem_u32(pairs);
   constexpr int NACC = NZ / 2;
   u64 acc2[NACC];
@@ -781,7 +785,7 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     const int4 org = origin2[p];
     const int v = org.z;
     if (v < 0) break;
-    const FdkView& V = P.v[v];
+    const FdkView V = vpair[p];
     const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
     const float U = __frcp_rn(den);
     const float wabs = fmaf(fmaf(V.a0, x, V.a1 * y), U, V.wc);
@@ -1062,7 +1066,7 @@ namespace {
 size_t fdk_smem_bytes(int BW, int BH, int stages, size_t es)
 {
   const size_t stage_bytes = ((size_t)BW * BH * es + 127) & ~(size_t)127;
-  return stages * stage_bytes + stages * (2 * sizeof(uint64_t) + sizeof(int4));
+  return stages * stage_bytes + stages * (2 * sizeof(uint64_t) + sizeof(int4) + sizeof(FdkView));
 }
 
 // Dynamic shared memory of one fdk_pair_kernel CTA: `stages` boxes of 16-bit taps, `pbufs`
@@ -1070,9 +1074,9 @@ size_t fdk_smem_bytes(int BW, int BH, int stages, size_t es)
 size_t fdk_pair_smem_bytes(int BW, int BH, int stages, int pbufs)
 {
   const size_t stage_bytes = ((size_t)BW * BH * 2 + 127) & ~(size_t)127;
-  const size_t pbuf_bytes = ((size_t)(BW + 4) * BH * 4 + 127) & ~(size_t)127;  // row pitch BW + 4
+  const size_t pbuf_bytes = ((size_t)BW * BH * 4 + 127) & ~(size_t)127;
   return stages * stage_bytes + pbufs * pbuf_bytes + (size_t)(stages + pbufs) * sizeof(int4) +
-         (size_t)(stages + 2 * pbufs) * sizeof(uint64_t);
+         (size_t)pbufs * sizeof(FdkView) + (size_t)(stages + 2 * pbufs) * sizeof(uint64_t);
 }
 
 // Launches chunk `chunk` (-1: all) over the z-tile layers [tz0, tz1) of the plan.
