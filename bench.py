@@ -593,9 +593,11 @@ def run_slabs(args, rank, world, local):
     from fastcone_b200 import _lib, ops, slabs
     from fastcone_b200 import dist as fd
 
-    # NCCL's communicator log (one line per rank with nranks) on stderr
+    # NCCL's communicator log (one line per rank with nranks) on stderr, so that stdout
+    # carries only the JSON line
     os.environ.setdefault("NCCL_DEBUG", "INFO")
     os.environ.setdefault("NCCL_DEBUG_SUBSYS", "INIT")
+    os.environ.setdefault("NCCL_DEBUG_FILE", "/dev/stderr")
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     fd.init("nccl", device=dev)
