@@ -217,8 +217,8 @@ def parse():
                          "exchanged as detector-row bands by an NCCL all-to-all (strong scaling; the "
                          "default for N > 1); z: one volume in z-slabs, every rank holding all views")
     ap.add_argument("--case", default=None,
-                    choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "conv-256", "katsevich", "pipeline",
-                             "misaligned-256"],
+                    choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "proj-256", "conv-256", "katsevich",
+                             "pipeline", "misaligned-256"],
                     help="profiling case: run only this kernel on a reduced workload (no JSON line)")
     return ap.parse_args()
 
@@ -228,7 +228,7 @@ def run_case(args):
     fdk-slab[-bf16]: the 1024^3 geometry restricted to a 1024x1024x128 z-slab (z 448..575),
     64 views (0.5 GB volume + 0.4 GB projections);
     proj-512: the staged, unstaged and texture projectors on 512^3, 90 views, 768x512
-    detector (0.5 GB volume);
+    detector (0.5 GB volume); proj-256: the same on 256^3, 360 views, 384x256;
     conv-256: one unrolled step's convolutions at 256^3 x 16 BF16 channels (0.54 GB per
     activation): forward (three kernel forms) and weight gradient (tensor cores and the
     CUDA-core kernel), all on tcgen05 except the last;
@@ -387,7 +387,12 @@ def run_case(args):
             res[name] = {"ms": ms, "TFLOP/s": flop / ms / 1e9}
         print(json.dumps({"case": args.case, **res}))
     else:
-        g = ConeGeometry.circular((512, 512, 512), 1.0, (768, 512), 1.0, 1000.0, 2000.0, 90)
+        if args.case == "proj-256":
+            from fastcone_b200 import configs
+
+            g = configs.diff_batch()  # 256^3, 360 views, 384x256
+        else:
+            g = ConeGeometry.circular((512, 512, 512), 1.0, (768, 512), 1.0, 1000.0, 2000.0, 90)
         from fastcone_b200.phantom import random_ellipsoids
 
         v = ops.phantom(g.vol_xyz, random_ellipsoids(10, g.vol_xyz, 1), device=dev)
