@@ -100,8 +100,8 @@ def oracle_problem(g):
 
 def fdk_parity(dev, ncols=256, seed=11, nellip=50):
     """Error of the large circular FDK backprojection (1024^3, 1440 views, 1536x1024) against
-    the FP64 oracle, with FP32- and with BF16-stored filtered projections (FP32 accumulation
-    both): a seeded 50-ellipsoid phantom projected by the explicit projector, cosine-weighted
+    the FP64 oracle, with FP32-, BF16- and FP16-stored filtered projections (FP32 accumulation
+    all): a seeded 50-ellipsoid phantom projected by the explicit projector, cosine-weighted
     and Shepp-Logan filtered on the GPU, backprojected over the whole volume; `ncols` random
     full-z voxel columns are compared with the oracle's FP64 backprojection of the same FP32
     filtered projections."""
@@ -122,7 +122,7 @@ def fdk_parity(dev, ncols=256, seed=11, nellip=50):
                        f"Shepp-Logan filter; {ncols} random full-z voxel columns vs the FP64 oracle",
            "points": int(len(pts))}
     got = {}
-    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16)):
+    for name, dt in (("f32", torch.float32), ("bf16", torch.bfloat16), ("f16", torch.float16)):
         p = proj if dt == torch.float32 else proj.to(dt)
         v = torch.zeros(g.vol_shape, device=dev)
         ops.BackprojectPlan(g, mode=_lib.MODE_FDK, dtype=dt)(p, v)

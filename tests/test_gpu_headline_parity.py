@@ -8,7 +8,7 @@
   Bounds: FP32 storage rel-L2 <= 2e-5 and max-abs <= 2e-5 of the largest reference value
   (FP32 arithmetic, as the small-size parity tests); BF16 storage rel-L2 <= 1e-3 and max-abs
   <= 1e-3 of it (BF16 keeps 8 significant bits of each filtered value; the rounding errors of
-  the 1440 views average out in the sum).
+  the 1440 views average out in the sum); FP16 storage (11 significant bits) <= 2e-4 both.
 * Helical Katsevich (512x512x384, 4 turns x 1160 views, 736x64): the projected phantom is
   Katsevich-filtered on the GPU and backprojected with the PI window; 64 random full-z
   columns vs the oracle's FP64 PI-window backprojection (coneBeamGPU.cu:258-338 plus the
@@ -24,15 +24,16 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def test_fdk_1024_fp32_and_bf16_storage_vs_fp64():
+def test_fdk_1024_fp32_bf16_fp16_storage_vs_fp64():
     import torch
 
     import bench
 
     r = bench.fdk_parity(torch.device("cuda", 0), ncols=64)
-    f32, b16 = r["f32"], r["bf16"]
+    f32, b16, h16 = r["f32"], r["bf16"], r["f16"]
     assert f32["rel_l2"] <= 2e-5 and f32["max_abs"] <= 2e-5 * f32["ref_max_abs"], r
     assert b16["rel_l2"] <= 1e-3 and b16["max_abs"] <= 1e-3 * b16["ref_max_abs"], r
+    assert h16["rel_l2"] <= 2e-4 and h16["max_abs"] <= 2e-4 * h16["ref_max_abs"], r
 
 
 def test_helix_pi_window_vs_fp64():

@@ -286,3 +286,24 @@ def test_fdk_oracle_reconstructs_a_phantom():
     c = (slice(12, 20), slice(10, 38), slice(10, 38))
     assert O.rel_l2(rec[c], vol[c]) < 0.2, O.rel_l2(rec[c], vol[c])
     assert abs(rec[c].mean() / vol[c].mean() - 1.0) < 0.03, rec[c].mean() / vol[c].mean()
+
+
+def test_piwin_points_equal_whole_volume_oracle():
+    """The FP64 PI-window backprojection at listed voxels (katsevich_piwin_points_f64, used on
+    sampled columns at the full helical size) equals the whole-volume function at those voxels,
+    values and in-window pair counts alike; column_points lists whole z columns."""
+    from fastcone_b200.geometry import ConeGeometry
+
+    g = ConeGeometry.helical((20, 18, 16), 1.0, (40, 12), 1.0, 60.0, 120.0, 2, 40, 8.0, pi_window=True)
+    pb = O.make_problem(g.vol_xyz, g.det_wh, g.nviews, D=g.D, pw=g.pw, angles=g.angles, hmid=g.hmid)
+    proj = np.random.default_rng(2).random(g.proj_shape, dtype=np.float32)
+    vol, pairs = O.katsevich_piwin_f64(pb, proj, g.helical_pitch)
+    pts = O.column_points(g.vol_xyz, (0, 0, 0), g.vol_xyz, 5, seed=3)
+    assert pts.shape == (5 * 16, 3) and np.array_equal(pts[:16, 2], np.arange(16))
+    got, npairs = O.katsevich_piwin_points_f64(pb, proj, pts, g.helical_pitch)
+    want = vol[pts[:, 2], pts[:, 1], pts[:, 0]]
+    assert np.array_equal(got, want)
+    # every voxel listed once: the pair counts add up to the whole volume's
+    allpts = np.stack(np.meshgrid(np.arange(20), np.arange(18), np.arange(16), indexing="ij"), -1).reshape(-1, 3)
+    _, allpairs = O.katsevich_piwin_points_f64(pb, proj, allpts.astype(np.int32), g.helical_pitch)
+    assert allpairs == pairs and 0 < npairs < pairs
