@@ -871,11 +871,12 @@ namespace fcb {
 // =====================================================================================
 // Generic projective-matrix kernel
 // =====================================================================================
-constexpr int GEN_MAXV = 560;
+constexpr int GEN_MAXV = 480;
 struct GenView {
   float m[12];
   float kappa;
   float wt;
+  float wc, hc;  // local window column of the detector centre, row of the source (PI window)
 };
 struct GenParams {
   float* vol;
@@ -886,8 +887,10 @@ struct GenParams {
   int WH0, WH1;
   int nviews, view0;
   int wexp;
-  int piwin;
-  float td_a, td_r, td_sign, pw;
+  int piwin;    // Tam-Danielsson window (aligned helical geometry), as fdk_tma_kernel
+  float td_a;   // window half-height scale P / (2 pi pw), pixels
+  float td_r;   // source-axis distance in pixels (D / pw)
+  float td_sign; // +1/-1: sense of the helix relative to the w axis
   // reference-compatible windows (NULL: ideal operator).  win[tile * wviews + view] holds
   // the first/last texel column and row of the sub-problem window, data-local; tiles are
   // sv0 x sv1 x sv2 voxels from volStart, ntx x nty of them per z layer.
@@ -966,6 +969,13 @@ __global__ void __launch_bounds__(256) bp_generic_kernel(const __grid_constant__
         continue;
       }
       if (!(wl > -1.0f && wl < (float)P.WH0 && hl > -1.0f && hl < (float)P.WH1)) continue;
+      if (P.piwin) {
+        // the voxel sees the view only inside its PI interval (the staged kernel's test)
+        const float u = (wl - V.wc) * P.td_sign / P.td_r;
+        const float q = P.td_a * (1.0f + u * u);
+        const float at = atanf(u);
+        if (hl > V.hc + q * (1.5707963267948966f - at) || hl < V.hc - q * (1.5707963267948966f + at)) continue;
+      }
       const float fw0 = floorf(wl), fh0 = floorf(hl);
       const int iw = (int)fw0, ih = (int)fh0;
       const float a = wl - fw0, b = hl - fh0;
@@ -1052,6 +1062,7 @@ struct fcb_bp_plan {
   long long updates = 0;
   std::vector<FdkParams> fdk;  // one per view chunk
   std::vector<GenParams> gen;
+  std::vector<int> gen_parent;  // the view chunk (launch of `fdk`, or itself) each `gen` entry belongs to
   int4* d_win = nullptr;  // reference-compatible window table (device), when in use
   ~fcb_bp_plan()
   {
@@ -1140,6 +1151,21 @@ void fill_fdk_views(const Problem& pb, int mode, int v0, int n, FdkParams* P)
     V.wt = (float)pb.norm[t];
   }
   (void)mode;
+}
+
+// Fill GenParams views [v0, v0+n): projective matrices, weights, window centre and source row.
+void fill_gen_views(const Problem& pb, int v0, int n, GenParams* P)
+{
+  for (int k = 0; k < n; k++) {
+    const int t = v0 + k;
+    double M[12], kappa;
+    view_matrix(pb, t, M, &kappa);
+    for (int j = 0; j < 12; j++) P->v[k].m[j] = (float)M[j];
+    P->v[k].kappa = (float)kappa;
+    P->v[k].wt = (float)pb.norm[t];
+    P->v[k].wc = (float)(pb.projDim[0] / 2 - pb.woff[t]);
+    P->v[k].hc = (float)(pb.projDim[1] / 2 - pb.hoff[t]);
+  }
 }
 
 }  // namespace
@@ -1344,19 +1370,16 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
       P.wexp = wexp;
       P.nviews = std::min(gmax, pb.nviews - v0);
       P.view0 = v0;
-      for (int k = 0; k < P.nviews; k++) {
-        double M[12], kappa;
-        view_matrix(pb, v0 + k, M, &kappa);
-        for (int j = 0; j < 12; j++) P.v[k].m[j] = (float)M[j];
-        P.v[k].kappa = (float)kappa;
-        P.v[k].wt = (float)pb.norm[v0 + k];
-      }
+      P.piwin = piwin ? 1 : 0;
+      P.td_a = td_a; P.td_r = td_r; P.td_sign = td_sign;
+      fill_gen_views(pb, v0, P.nviews, &P);
       if (compat) {
         P.win = pl->d_win;
         P.sv0 = rw.subVolDim[0]; P.sv1 = rw.subVolDim[1]; P.sv2 = rw.subVolDim[2];
         P.ntx = rw.ntx; P.nty = rw.nty;
         P.wviews = pb.nviews;
       }
+      pl->gen_parent.push_back((int)pl->gen.size());
       pl->gen.push_back(P);
     }
   }
@@ -1454,30 +1477,32 @@ int bp_plan_execute_range(fcb_bp_plan* pl, int chunk, int z0, int z1, const void
   }
   if (pl->gen.empty()) {
     // TMA path planned but this buffer cannot be described by a descriptor: build the
-    // generic parameters on the fly, with the same view chunks.
-    for (int v0 = 0; v0 < pb.nviews; v0 += pl->maxv) {
-      GenParams P;
-      memset(&P, 0, sizeof(P));
-      const FdkParams& F = pl->fdk[0];
-      P.nx = F.nx; P.ny = F.ny; P.nz = F.nz;
-      P.ox = F.ox; P.oy = F.oy; P.oz = F.oz;
-      P.WH0 = pb.projWHSize[0]; P.WH1 = pb.projWHSize[1];
-      P.ptype = pl->ptype;
-      P.wexp = F.wexp;
-      P.nviews = std::min(pl->maxv, pb.nviews - v0);
-      P.view0 = v0;
-      for (int k = 0; k < P.nviews; k++) {
-        double M[12], kappa;
-        view_matrix(pb, v0 + k, M, &kappa);
-        for (int j = 0; j < 12; j++) P.v[k].m[j] = (float)M[j];
-        P.v[k].kappa = (float)kappa;
-        P.v[k].wt = (float)pb.norm[v0 + k];
+    // generic parameters on the fly, each staged launch's views in pieces of at most
+    // GEN_MAXV (the generic kernel's parameter space holds fewer views)
+    for (int fc = 0; fc < (int)pl->fdk.size(); fc++) {
+      const FdkParams& F = pl->fdk[fc];
+      for (int v0 = F.view0; v0 < F.view0 + F.nviews; v0 += GEN_MAXV) {
+        GenParams P;
+        memset(&P, 0, sizeof(P));
+        P.nx = F.nx; P.ny = F.ny; P.nz = F.nz;
+        P.ox = F.ox; P.oy = F.oy; P.oz = F.oz;
+        P.WH0 = pb.projWHSize[0]; P.WH1 = pb.projWHSize[1];
+        P.ptype = pl->ptype;
+        P.wexp = F.wexp;
+        P.nviews = std::min(GEN_MAXV, F.view0 + F.nviews - v0);
+        P.view0 = v0;
+        P.piwin = F.piwin;
+        P.td_a = F.td_a;
+        P.td_r = F.td_r;
+        P.td_sign = F.td_sign;
+        fill_gen_views(pb, v0, P.nviews, &P);
+        pl->gen_parent.push_back(fc);
+        pl->gen.push_back(P);
       }
-      pl->gen.push_back(P);
     }
   }
   for (int c = 0; c < (int)pl->gen.size(); c++) {
-    if (chunk >= 0 && c != chunk) continue;
+    if (chunk >= 0 && pl->gen_parent[c] != chunk) continue;
     GenParams& P = pl->gen[c];
     P.vol = volume;
     P.proj = proj;

@@ -30,22 +30,18 @@ int ok()
 }
 
 // ------------------------------------------------------------------- device status
-static std::mutex g_status_mu;
-static int* g_status[64] = {nullptr};
+// The kernels' status words (and the small scratch of the plan pre-passes) live in a
+// file-scope device array: every context that loads the library gets its own copy, zeroed
+// when the module loads, so nothing is allocated and no address is cached across calls
+// (a cached pointer would go stale when a device's primary context is reset and made
+// again).  The address is looked up with the caller's device current, on every call.
+static __device__ __align__(64) int g_status_words[16];
 
 int device_status_ptr(int** p)
 {
-  int dev = 0;
-  FCB_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return set_error(FCB_ERR_NODEVICE, "device index out of range");
-  std::lock_guard<std::mutex> lk(g_status_mu);
-  if (!g_status[dev]) {
-    int* d = nullptr;
-    FCB_CUDA_TRY(cudaMalloc(&d, 16 * sizeof(int)));
-    FCB_CUDA_TRY(cudaMemset(d, 0, 16 * sizeof(int)));
-    g_status[dev] = d;
-  }
-  *p = g_status[dev];
+  void* a = nullptr;
+  FCB_CUDA_TRY(cudaGetSymbolAddress(&a, g_status_words));
+  *p = static_cast<int*>(a);
   return FCB_OK;
 }
 
