@@ -378,7 +378,9 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   if (warp == FDK_CWARPS) {
     // ------------------------------------------------------------- producer warp
     const uint32_t bytes = (uint32_t)(stage_elems * ES);
-    int issued = 0;  // staged views so far (= ring position)
+    int issued = 0;  // staged views so far
+    int ps = 0;      // its ring slot (issued mod stages), kept by increments: no division
+    uint32_t pround = 0;  // parity of issued / stages
     bool failed = false, stalled = false;
     if constexpr (PIW) {
       // the whole warp tests 32 views at a time against the PI window (most views miss a
@@ -405,8 +407,8 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
           const int snw = __shfl_sync(0xffffffffu, nw, l), snh = __shfl_sync(0xffffffffu, nh, l);
           int ok = 1;
           if (lane == 0) {
-            const int s = issued % P.stages;
-            if (issued >= P.stages && !dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
+            const int s = ps;
+            if (issued >= P.stages && !dev::mbar_wait(&empty[s], pround ^ 1u)) {
               ok = 0;
             } else {
               if (snw > P.BW || snh > P.BH) dev::record_status(P.status, DEV_RANGE);
@@ -422,6 +424,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
             break;
           }
           issued++;
+          if (++ps == P.stages) { ps = 0; pround ^= 1u; }
         }
       }
       if (lane != 0) return;
@@ -435,9 +438,9 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         }
         int w0, h0, nw, nh;
         fdk_box_origin(P, P.v[v], tx, ty, tz, NZ, w0, h0, nw, nh);
-        const int s = issued % P.stages;
+        const int s = ps;
         if (issued >= P.stages) {
-          if (!dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
+          if (!dev::mbar_wait(&empty[s], pround ^ 1u)) {
             failed = true;
             break;
           }
@@ -448,12 +451,13 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         dev::mbar_arrive_expect_tx(&full[s], bytes);
         dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + v);
         issued++;
+        if (++ps == P.stages) { ps = 0; pround ^= 1u; }
       }
     }
     if (PIW && !failed && !stalled) {
       // end of the view list: a slot whose phase completes without data, view -1
-      const int s = issued % P.stages;
-      if (issued < P.stages || dev::mbar_wait(&empty[s], ((issued / P.stages) - 1) & 1)) {
+      const int s = ps;
+      if (issued < P.stages || dev::mbar_wait(&empty[s], pround ^ 1u)) {
         origin[s] = make_int4(0, 0, -1, 0);
         dev::mbar_arrive(&full[s]);
       } else {
@@ -489,10 +493,12 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   }
 
   // ring position j carries view j (all views staged) or the view the producer chose (PI
-  // window: only views that reach the tile, then an end marker)
+  // window: only views that reach the tile, then an end marker); its slot s = j mod stages
+  // and the phase parity are kept by increments (no integer division per view)
+  int s = 0;
+  uint32_t ph = 0;
   for (int j = 0; PIW || j < P.nviews; j++) {
-    const int s = j % P.stages;
-    if (!dev::mbar_wait(&full[s], (j / P.stages) & 1, P.cwait_ns)) {
+    if (!dev::mbar_wait(&full[s], ph, P.cwait_ns)) {
       dev::record_status(P.status, DEV_TIMEOUT);
       return;
     }
@@ -591,6 +597,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
     }
     __syncwarp();
     if (lane == 0) dev::mbar_arrive(&empty[s]);
+    if (++s == P.stages) { s = 0; ph ^= 1u; }
   }
 
   if (xl < P.nx && yl < P.ny) {
@@ -671,6 +678,7 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     int lw0 = 0, lh0 = 0, lnw = 0, lnh = 0;
     bool exhausted = false, stalled = false, failed = false;
     int issued = 0, conv = 0;
+    int is = 0;  // issued mod S, kept by increments (no division per view)
     auto issue_next = [&]() {
       if (exhausted) return;
       if (issued == P.stop_after) {  // test hook
@@ -696,7 +704,7 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
       msk &= msk - 1;
       const int w0 = __shfl_sync(0xffffffffu, lw0, l), h0 = __shfl_sync(0xffffffffu, lh0, l);
       const int nw = __shfl_sync(0xffffffffu, lnw, l), nh = __shfl_sync(0xffffffffu, lnh, l);
-      const int s = issued % S;  // free: its previous view has been rewritten
+      const int s = is;  // free: its previous view has been rewritten
       if (lane == 0) {
         if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
         sorg[s] = make_int4(w0, h0, vb + l, nh);
@@ -705,14 +713,18 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
       }
       __syncwarp();
       issued++;
+      if (++is == S) is = 0;
     };
     for (int k = 0; k < S; k++) issue_next();
     const int cpr = P.BW / 8;  // 16-byte chunks per row (BW is a multiple of 8)
     const int nbox = P.BH * cpr;
+    // conv mod S / mod NP and the parities of conv / S and conv / NP
+    int cs = 0, cp = 0;
+    uint32_t cph = 0, cpph = 0;
     while (conv < issued) {
-      const int s = conv % S, p = conv % NP;
-      bool ok = dev::mbar_wait(&full[s], (conv / S) & 1);
-      if (ok && conv >= NP) ok = dev::mbar_wait(&empty2[p], ((conv / NP) - 1) & 1);
+      const int s = cs, p = cp;
+      bool ok = dev::mbar_wait(&full[s], cph);
+      if (ok && conv >= NP) ok = dev::mbar_wait(&empty2[p], cpph ^ 1u);
       if (!__all_sync(0xffffffffu, ok)) {
         failed = true;
         break;
@@ -738,6 +750,8 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
       __syncwarp();
       dev::mbar_arrive(&full2[p]);  // all 32 lanes: their writes are released to the consumers
       conv++;
+      if (++cs == S) { cs = 0; cph ^= 1u; }
+      if (++cp == NP) { cp = 0; cpph ^= 1u; }
       issue_next();  // stage s is free again
     }
     if (failed) {
@@ -750,8 +764,8 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     }
     if (stalled) return;  // every issued copy has landed and been handed over
     // end of the view list: a pair buffer whose phase completes without data, view -1
-    const int p = conv % NP;
-    const bool ok = conv < NP || dev::mbar_wait(&empty2[p], ((conv / NP) - 1) & 1);
+    const int p = cp;
+    const bool ok = conv < NP || dev::mbar_wait(&empty2[p], cpph ^ 1u);
     if (__all_sync(0xffffffffu, ok)) {
       if (lane == 0) origin2[p] = make_int4(0, 0, -1, 0);
       __syncwarp();
@@ -776,9 +790,12 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
 #pragma unroll
   for (int k = 0; k < NACC; k++) acc2[k] = 0ull;
 
-  for (int j = 0;; j++) {
-    const int p = j % NP;
-    if (!dev::mbar_wait(&full2[p], (j / NP) & 1, P.cwait_ns)) {
+  // pair buffer of the next view (the views cycle through the NP buffers) and the parity of
+  // its phase, kept by increments (no integer division per view)
+  int p = 0;
+  uint32_t ph = 0;
+  for (;;) {
+    if (!dev::mbar_wait(&full2[p], ph, P.cwait_ns)) {
       dev::record_status(P.status, DEV_TIMEOUT);
       return;
     }
@@ -850,6 +867,7 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     }
     __syncwarp();
     if (lane == 0) dev::mbar_arrive(&empty2[p]);
+    if (++p == NP) { p = 0; ph ^= 1u; }
   }
 
   if (xl < P.nx && yl < P.ny) {
