@@ -22,6 +22,7 @@
 
 #include <algorithm>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "fcb_internal.h"
@@ -309,9 +310,37 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c)
   return r;
 }
 
+// f(integral_constant<int, K>) for K = lo, lo + 1, ..., hi, entered through a jump table on lo
+// (nothing is tested for the K outside); lo <= hi < N, or lo >= N for none; N <= 32.
+#define FCB_RUN_PAIR(K)                      \
+  case K:                                    \
+    if constexpr (K < N) {                   \
+      f(std::integral_constant<int, K>{});   \
+      if (hi == K) break;                    \
+    }                                        \
+    [[fallthrough]];
+template <int N, typename F>
+__device__ __forceinline__ void run_pairs(int lo, int hi, F&& f)
+{
+  static_assert(N <= 32, "pairs per thread");
+  switch (lo) {
+    FCB_RUN_PAIR(0) FCB_RUN_PAIR(1) FCB_RUN_PAIR(2) FCB_RUN_PAIR(3) FCB_RUN_PAIR(4)
+    FCB_RUN_PAIR(5) FCB_RUN_PAIR(6) FCB_RUN_PAIR(7) FCB_RUN_PAIR(8) FCB_RUN_PAIR(9)
+    FCB_RUN_PAIR(10) FCB_RUN_PAIR(11) FCB_RUN_PAIR(12) FCB_RUN_PAIR(13) FCB_RUN_PAIR(14)
+    FCB_RUN_PAIR(15) FCB_RUN_PAIR(16) FCB_RUN_PAIR(17) FCB_RUN_PAIR(18) FCB_RUN_PAIR(19)
+    FCB_RUN_PAIR(20) FCB_RUN_PAIR(21) FCB_RUN_PAIR(22) FCB_RUN_PAIR(23) FCB_RUN_PAIR(24)
+    FCB_RUN_PAIR(25) FCB_RUN_PAIR(26) FCB_RUN_PAIR(27) FCB_RUN_PAIR(28) FCB_RUN_PAIR(29)
+    FCB_RUN_PAIR(30) FCB_RUN_PAIR(31)
+    default:
+      break;
+  }
+}
+#undef FCB_RUN_PAIR
+
 // PI window: of the thread's NZ z-voxels (pairs k = (2k, 2k + 1)), the pairs that can lie
-// inside the window of some lane of the warp, [plo, phi]; the warp skips the others (a
-// uniform branch: no taps loaded, no arithmetic), the per-voxel test still decides inside.
+// inside the window of some lane of the warp, [plo, phi]; the warp runs only those
+// (run_pairs: no taps loaded, no arithmetic for the others), the per-voxel test still decides
+// inside.
 // h(z_k) = h0 + k dh with dh > 0, so a lane's inside voxels are one run of k; one step of
 // margin on each side covers the rounding of the incremental row positions.
 template <int NACC>
@@ -354,7 +383,8 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
   const int stage_bytes = ((stage_elems * ES) + 127) & ~127;
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + (size_t)P.stages * stage_bytes);
   uint64_t* empty = full + P.stages;
-  // per stage: box origin w, h; view (-1: end of the list); rows the tile's footprint needs
+  // per stage: box origin w, h (as float bits: the consumers use them as floats); view (-1:
+  // end of the list); rows the tile's footprint needs
   int4* origin = reinterpret_cast<int4*>(empty + P.stages);
   // per stage: the staged view's parameters, copied by the producer so that the consumers read
   // them from shared memory (the views of a launch overflow the constant cache while the
@@ -412,7 +442,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
               ok = 0;
             } else {
               if (snw > P.BW || snh > P.BH) dev::record_status(P.status, DEV_RANGE);
-              origin[s] = make_int4(sw0, sh0, vb + l, snh);
+              origin[s] = make_int4(__float_as_int((float)sw0), __float_as_int((float)sh0), vb + l, snh);
               vstage[s] = P.v[vb + l];
               dev::mbar_arrive_expect_tx(&full[s], bytes);
               dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], sw0, sh0,
@@ -446,7 +476,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
           }
         }
         if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
-        origin[s] = make_int4(w0, h0, v, nh);
+        origin[s] = make_int4(__float_as_int((float)w0), __float_as_int((float)h0), v, nh);
         vstage[s] = P.v[v];
         dev::mbar_arrive_expect_tx(&full[s], bytes);
         dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + v);
@@ -508,10 +538,11 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
     const FdkView V = vstage[s];
 
     const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
-    const float U = __frcp_rn(den);
+    // the approximate reciprocal (within 2 ulp): the staging box keeps a pixel of margin
+    const float U = __fdividef(1.0f, den);
     const float wabs = fmaf(fmaf(V.a0, x, V.a1 * y), U, V.wc);
-    float wl = wabs - (float)org.x;
-    float h0 = fmaf(U, fmaf(P.hb, zf, V.e), V.hc) - (float)org.y;
+    float wl = wabs - __int_as_float(org.x);
+    float h0 = fmaf(U, fmaf(P.hb, zf, V.e), V.hc) - __int_as_float(org.y);
     float dh = U * P.hb;
     float wt = V.wt;
     if (P.wexp >= 1) wt *= U;
@@ -532,7 +563,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
       const float u = (wabs - V.wc) * P.td_sign / P.td_r;
       const float q = P.td_a * (1.0f + u * u);
       const float at = atanf(u);
-      const float hsrc = V.hc - (float)org.y;
+      const float hsrc = V.hc - __int_as_float(org.y);
       hi = hsrc + q * (1.5707963267948966f - at);
       lo = hsrc - q * (1.5707963267948966f + at);
     }
@@ -545,15 +576,12 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
       const u64 FW2 = pk2(fw, fw);
       const u64 WT2 = pk2(wt, wt);
       const u64 D2 = pk2(2.0f * dh, 2.0f * dh);
-      u64 H = pk2(h0, h0 + dh);
-      int plo = 0, phi = NACC - 1;
-      if constexpr (PIW) piw_pairs<NACC>(lo, hi, h0, dh, plo, phi);
-#pragma unroll
-      for (int k = 0; k < NACC; k++) {
-        if (PIW && (k < plo || k > phi)) {  // warp-uniform: the pair is outside every lane's window
-          H = add2(H, D2);
-          continue;
-        }
+      // PI-window path, one voxel pair: taps from the staged box, the view's weight for the
+      // voxels inside the window, accumulated into pair k; H holds the pair's two row
+      // positions and steps to the next pair's.  (The path without the window keeps the
+      // plain unrolled loop below: written through this lambda it ran 6 % slower.)
+      auto pair = [&](auto kc, u64& H) {
+        constexpr int k = decltype(kc)::value;
         const u64 T2 = add2_rm(H, MAG2);
         const u64 FH = sub2(H, sub2(T2, MAG2));
         float t0, t1;
@@ -576,6 +604,36 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
         }
         acc2[k] = fma2(W, VAL, acc2[k]);
         H = add2(H, D2);
+      };
+      if constexpr (PIW) {
+        // only the pairs plo..phi that can lie inside some lane's window, entered through a
+        // jump table: the pairs outside cost no test (57.4 against 60.6 ms per helical pass
+        // with a warp-uniform test of every pair)
+        int plo = 0, phi = NACC - 1;
+        piw_pairs<NACC>(lo, hi, h0, dh, plo, phi);
+        u64 H = fma2(pk2((float)plo, (float)plo), D2, pk2(h0, h0 + dh));
+        run_pairs<NACC>(plo, phi, [&](auto kc) { pair(kc, H); });
+      } else {
+        u64 H = pk2(h0, h0 + dh);
+#pragma unroll
+        for (int k = 0; k < NACC; k++) {
+          const u64 T2 = add2_rm(H, MAG2);
+          const u64 FH = sub2(H, sub2(T2, MAG2));
+          float t0, t1;
+          up2(T2, t0, t1);
+          const uint32_t a0 = (uint32_t)__float_as_uint(t0) * rowb + base;
+          const uint32_t a1 = (uint32_t)__float_as_uint(t1) * rowb + base;
+          const uint32_t c0 = a0 + rowb, c1 = a1 + rowb;
+          const u64 A = lds_f32x2<0>(a0, a1);
+          const u64 B = lds_f32x2<4>(a0, a1);
+          const u64 C = lds_f32x2<0>(c0, c1);
+          const u64 Dd = lds_f32x2<4>(c0, c1);
+          const u64 R0 = fma2(FW2, sub2(B, A), A);
+          const u64 R1 = fma2(FW2, sub2(Dd, C), C);
+          const u64 VAL = fma2(FH, sub2(R1, R0), R0);
+          acc2[k] = fma2(WT2, VAL, acc2[k]);
+          H = add2(H, D2);
+        }
       }
     } else {
 #pragma unroll
@@ -647,8 +705,9 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
   const int stage_bytes = ((stage_elems * 2) + 127) & ~127;
   const int pbuf_bytes = ((stage_elems * 4) + 127) & ~127;
   unsigned char* pairs = smem_raw + (size_t)S * stage_bytes;
-  int4* origin2 = reinterpret_cast<int4*>(pairs + (size_t)NP * pbuf_bytes);  // per pair buffer
-  int4* sorg = origin2 + NP;                                                   // per TMA stage
+  // box origins (w, h as float bits, view, rows needed): per pair buffer and per TMA stage
+  int4* origin2 = reinterpret_cast<int4*>(pairs + (size_t)NP * pbuf_bytes);
+  int4* sorg = origin2 + NP;
   FdkView* vpair = reinterpret_cast<FdkView*>(sorg + S);  // per pair buffer: its view's parameters
   uint64_t* full = reinterpret_cast<uint64_t*>(vpair + NP);
   uint64_t* full2 = full + S;
@@ -707,7 +766,7 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
       const int s = is;  // free: its previous view has been rewritten
       if (lane == 0) {
         if (nw > P.BW || nh > P.BH) dev::record_status(P.status, DEV_RANGE);
-        sorg[s] = make_int4(w0, h0, vb + l, nh);
+        sorg[s] = make_int4(__float_as_int((float)w0), __float_as_int((float)h0), vb + l, nh);
         dev::mbar_arrive_expect_tx(&full[s], bytes);
         dev::tma_load_3d(smem_raw + (size_t)s * stage_bytes, &tmap, &full[s], w0, h0, P.view0 + vb + l);
       }
@@ -804,10 +863,11 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     if (v < 0) break;
     const FdkView V = vpair[p];
     const float den = fmaf(V.c0, x, fmaf(V.c1, y, 1.0f));
-    const float U = __frcp_rn(den);
+    // the approximate reciprocal (within 2 ulp): the staging box keeps a pixel of margin
+    const float U = __fdividef(1.0f, den);
     const float wabs = fmaf(fmaf(V.a0, x, V.a1 * y), U, V.wc);
-    float wl = wabs - (float)org.x;
-    float h0 = fmaf(U, fmaf(P.hb, zf, V.e), V.hc) - (float)org.y;
+    float wl = wabs - __int_as_float(org.x);
+    float h0 = fmaf(U, fmaf(P.hb, zf, V.e), V.hc) - __int_as_float(org.y);
     float dh = U * P.hb;
     float wt = V.wt;
     if (P.wexp >= 1) wt *= U;
@@ -825,7 +885,7 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
       const float u = (wabs - V.wc) * P.td_sign / P.td_r;
       const float q = P.td_a * (1.0f + u * u);
       const float at = atanf(u);
-      const float hsrc = V.hc - (float)org.y;
+      const float hsrc = V.hc - __int_as_float(org.y);
       hi = hsrc + q * (1.5707963267948966f - at);
       lo = hsrc - q * (1.5707963267948966f + at);
     }
@@ -835,15 +895,9 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     const u64 FW2 = pk2(fw, fw);
     const u64 WT2 = pk2(wt, wt);
     const u64 D2 = pk2(2.0f * dh, 2.0f * dh);
-    u64 H = pk2(h0, h0 + dh);
-    int plo = 0, phi = NACC - 1;
-    if constexpr (PIW) piw_pairs<NACC>(lo, hi, h0, dh, plo, phi);
-#pragma unroll
-    for (int k = 0; k < NACC; k++) {
-      if (PIW && (k < plo || k > phi)) {  // warp-uniform: the pair is outside every lane's window
-        H = add2(H, D2);
-        continue;
-      }
+    // PI-window path, one voxel pair, as in fdk_tma_kernel, from the tap-pair words
+    auto pair = [&](auto kc, u64& H) {
+      constexpr int k = decltype(kc)::value;
       const u64 T2 = add2_rm(H, MAG2);
       const u64 FH = sub2(H, sub2(T2, MAG2));
       float t0, t1;
@@ -864,6 +918,32 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
       }
       acc2[k] = fma2(W, VAL, acc2[k]);
       H = add2(H, D2);
+    };
+    if constexpr (PIW) {
+      // the pairs plo..phi only (see fdk_tma_kernel)
+      int plo = 0, phi = NACC - 1;
+      piw_pairs<NACC>(lo, hi, h0, dh, plo, phi);
+      u64 H = fma2(pk2((float)plo, (float)plo), D2, pk2(h0, h0 + dh));
+      run_pairs<NACC>(plo, phi, [&](auto kc) { pair(kc, H); });
+    } else {
+      u64 H = pk2(h0, h0 + dh);
+#pragma unroll
+      for (int k = 0; k < NACC; k++) {
+        const u64 T2 = add2_rm(H, MAG2);
+        const u64 FH = sub2(H, sub2(T2, MAG2));
+        float t0, t1;
+        up2(T2, t0, t1);
+        const uint32_t a0 = (uint32_t)__float_as_uint(t0) * rowb + base;
+        const uint32_t a1 = (uint32_t)__float_as_uint(t1) * rowb + base;
+        u64 A, B, C, Dd;
+        lds_pair_taps<T>(a0, a1, A, B);
+        lds_pair_taps<T>(a0 + rowb, a1 + rowb, C, Dd);
+        const u64 R0 = fma2(FW2, sub2(B, A), A);
+        const u64 R1 = fma2(FW2, sub2(Dd, C), C);
+        const u64 VAL = fma2(FH, sub2(R1, R0), R0);
+        acc2[k] = fma2(WT2, VAL, acc2[k]);
+        H = add2(H, D2);
+      }
     }
     __syncwarp();
     if (lane == 0) dev::mbar_arrive(&empty2[p]);
