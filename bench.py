@@ -42,10 +42,11 @@ WORKLOAD = "circular FDK backprojection 1024^3 voxels, 1440 views, 1536x1024 det
 
 # DRAM bytes per FDK launch (1024^3, 180 views per launch): ncu dram__bytes_read.sum +
 # dram__bytes_write.sum of every launch of one step of this benchmark, mean over the step's 8
-# launches; they range from 15.2 GB (views near 0 and 180 degrees) to 68.3 GB (near 90 and
-# 270 degrees), 326 GB per step.
-FDK_TRAFFIC_PER_LAUNCH = 40.72e9
-FDK_TRAFFIC_NOTE = "measured by ncu on the 8 launches of one step (mean; 15.2-68.3 GB per launch)"
+# launches; they range from 14.9 to 16.7 GB (the volume's read-modify-write, 8.6 GB, plus the
+# detector rows), 125.5 GB per step, since each launch runs its tiles along the axis that
+# moves the detector column less.
+FDK_TRAFFIC_PER_LAUNCH = 15.69e9
+FDK_TRAFFIC_NOTE = "measured by ncu on the 8 launches of one step (mean; 14.9-16.7 GB per launch)"
 
 
 def smem_probe(stream, target_s=0.4):
