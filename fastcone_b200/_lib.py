@@ -51,6 +51,7 @@ EXPORTED_SYMBOLS = [
     "fcb_katsevich_plan_create", "fcb_katsevich_plan_execute", "fcb_katsevich_plan_destroy",
     "fcb_detector_rows",
     "fcb_bp_plan_set_test_stall", "fcb_katsevich_pi_pairs", "fcb_smem_bandwidth", "fcb_fbp_host",
+    "fcb_release_device_cache",
 ]
 
 
@@ -113,6 +114,7 @@ def lib():
                                            ctypes.POINTER(ctypes.c_longlong)]
             L.fcb_bp_plan_destroy.argtypes = [vp]
             L.fcb_sync_status.argtypes = [vp]
+            L.fcb_release_device_cache.argtypes = []
             L.fcb_fdk_filter_device.argtypes = [vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, ctypes.c_float, c_float_p,
                                                 ctypes.c_int, ctypes.c_int, vp]

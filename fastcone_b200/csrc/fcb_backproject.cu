@@ -62,6 +62,7 @@ struct FdkParams {
   float td_a;                   // window half-height scale P / (2 pi pw), pixels
   float td_r;                   // source-axis distance in pixels (D / pw)
   float td_sign;                // +1/-1: sense of the helix relative to the w axis
+  float td_usc;                 // td_sign / td_r (a multiply per staged view instead of a division)
   // Bounded waits.  cwait_ns limits each consumer wait for a staged view (2 s by default).
   // stop_after >= 0 is a test hook: the producer stages only that many views, drains its
   // copies and leaves, so the consumers' next wait runs out and the kernel reports
@@ -570,7 +571,7 @@ __global__ void __launch_bounds__(FDK_THREADS, MINB) fdk_tma_kernel(const __grid
 
     float lo = -3.0e38f, hi = 3.0e38f;  // Tam-Danielsson bounds (local h)
     if constexpr (PIW) {
-      const float u = (wabs - V.wc) * P.td_sign / P.td_r;
+      const float u = (wabs - V.wc) * P.td_usc;
       const float q = P.td_a * (1.0f + u * u);
       const float at = atanf(u);
       const float hsrc = V.hc - __int_as_float(org.y);
@@ -892,7 +893,7 @@ __global__ void __launch_bounds__(FDK_THREADS, 3) fdk_pair_kernel(const __grid_c
     const float fw = wl - (float)iw;
     float lo = -3.0e38f, hi = 3.0e38f;  // Tam-Danielsson bounds (local h)
     if constexpr (PIW) {
-      const float u = (wabs - V.wc) * P.td_sign / P.td_r;
+      const float u = (wabs - V.wc) * P.td_usc;
       const float q = P.td_a * (1.0f + u * u);
       const float at = atanf(u);
       const float hsrc = V.hc - __int_as_float(org.y);
@@ -1397,6 +1398,7 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
       P.wexp = wexp;
       P.piwin = piwin ? 1 : 0;
       P.td_a = td_a; P.td_r = td_r; P.td_sign = td_sign;
+      P.td_usc = (float)((double)td_sign / (double)td_r);
       P.cwait_ns = 2000000000ull;
       P.stop_after = -1;
       fill_fdk_views(pb, pl->mode, v0, std::min(pl->maxv, pb.nviews - v0), &P);

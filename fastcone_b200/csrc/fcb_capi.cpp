@@ -67,9 +67,57 @@ struct DeviceGuard {
   }
 };
 
+// ------------------------------------------------------------------- device block cache
+// The host entry points move whole problems through device memory on every call (13.4 GB
+// for a 1024^3 / 1440-view backprojection); cudaMalloc and cudaFree of that much take from a
+// few to over a hundred milliseconds per call.  A call's blocks are therefore kept per device
+// when it ends and handed to later calls that fit in them (the smallest cached block of at
+// least the request and at most twice it).  At most 8 blocks per device are kept (the oldest
+// go back to the driver), fcb_release_device_cache returns them all, and FCB_HOST_CACHE=0
+// frees every block when its call ends.
+namespace {
+struct CachedBlock {
+  int dev;
+  void* p;
+  size_t bytes;
+};
+std::mutex g_cache_mu;
+std::vector<CachedBlock> g_cache;  // oldest first
+constexpr int CACHE_BLOCKS_PER_DEVICE = 8;
+
+bool cache_enabled()
+{
+  const char* e = getenv("FCB_HOST_CACHE");
+  return !(e && e[0] == '0');
+}
+
+// Frees the cached blocks of `dev` (-1: of every device); the caller holds g_cache_mu.
+void cache_drop_locked(int dev)
+{
+  if (g_cache.empty()) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  for (size_t i = 0; i < g_cache.size();) {
+    if (dev < 0 || g_cache[i].dev == dev) {
+      cudaSetDevice(g_cache[i].dev);
+      cudaFree(g_cache[i].p);
+      g_cache.erase(g_cache.begin() + (long)i);
+    } else {
+      i++;
+    }
+  }
+  if (cur >= 0) cudaSetDevice(cur);
+}
+}  // namespace
+
 // RAII bundle of device buffers/streams/events of one host-driver call.
 struct Scratch {
-  std::vector<void*> dev;
+  struct Block {
+    void* p;
+    size_t bytes;
+  };
+  int dev = -1;
+  std::vector<Block> blocks;
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;
   ~Scratch()
@@ -77,15 +125,58 @@ struct Scratch {
     for (cudaStream_t s : streams) cudaStreamSynchronize(s);
     for (cudaEvent_t e : events) cudaEventDestroy(e);
     for (cudaStream_t s : streams) cudaStreamDestroy(s);
-    for (void* p : dev) cudaFree(p);
+    if (blocks.empty()) return;
+    if (!cache_enabled()) {
+      for (const Block& b : blocks) cudaFree(b.p);
+      return;
+    }
+    // every stream of the call has finished: the blocks are free for the next call
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (const Block& b : blocks) g_cache.push_back(CachedBlock{dev, b.p, b.bytes});
+    int n = 0;
+    for (const CachedBlock& c : g_cache) n += c.dev == dev;
+    for (size_t i = 0; i < g_cache.size() && n > CACHE_BLOCKS_PER_DEVICE;) {
+      if (g_cache[i].dev == dev) {
+        cudaFree(g_cache[i].p);
+        g_cache.erase(g_cache.begin() + (long)i);
+        n--;
+      } else {
+        i++;
+      }
+    }
   }
   int alloc(void** p, size_t bytes)
   {
+    if (dev < 0) FCB_CUDA_TRY(cudaGetDevice(&dev));
+    if (cache_enabled()) {
+      std::lock_guard<std::mutex> lk(g_cache_mu);
+      long best = -1;
+      for (size_t i = 0; i < g_cache.size(); i++) {
+        const CachedBlock& c = g_cache[i];
+        if (c.dev == dev && c.bytes >= bytes && c.bytes <= 2 * bytes &&
+            (best < 0 || c.bytes < g_cache[(size_t)best].bytes))
+          best = (long)i;
+      }
+      if (best >= 0) {
+        *p = g_cache[(size_t)best].p;
+        blocks.push_back(Block{*p, g_cache[(size_t)best].bytes});
+        g_cache.erase(g_cache.begin() + best);
+        return FCB_OK;
+      }
+    }
     if (cudaMalloc(p, bytes) != cudaSuccess) {
       cudaGetLastError();
-      return set_error(FCB_ERR_NOMEM, "device allocation failed");
+      // memory held by the cache goes back to the driver, then one more try
+      {
+        std::lock_guard<std::mutex> lk(g_cache_mu);
+        cache_drop_locked(dev);
+      }
+      if (cudaMalloc(p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return set_error(FCB_ERR_NOMEM, "device allocation failed");
+      }
     }
-    dev.push_back(*p);
+    blocks.push_back(Block{*p, bytes});
     return FCB_OK;
   }
   int stream(cudaStream_t* s)
@@ -587,6 +678,14 @@ try {
     FCB_CUDA_TRY(cudaMemcpyAsync(projections, dproj, np * sizeof(float), cudaMemcpyDeviceToHost, cs));
   FCB_CUDA_TRY(cudaStreamSynchronize(cs));
   FCB_TRY(collect_device_status(cs));
+  return ok();
+}
+FCB_CATCH_STATUS
+
+extern "C" int fcb_release_device_cache(void)
+try {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  cache_drop_locked(-1);
   return ok();
 }
 FCB_CATCH_STATUS

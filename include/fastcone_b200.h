@@ -231,6 +231,13 @@ int fcb_proj_plan_info(const fcb_proj_plan* plan, int* staged, int* brickC, int*
  * library recorded a device-side failure since the previous check, else FCB_OK. */
 int fcb_sync_status(void* stream);
 
+/* The host-buffer entry points (GPU_CB_*, fcb_backproject_host, fcb_project_host,
+ * fcb_fbp_host) keep the device blocks of a finished call and reuse them in later calls
+ * that fit (at most 8 blocks per device; a failed allocation first returns them).  This
+ * returns every kept block to the driver.  FCB_HOST_CACHE=0 in the environment frees each
+ * call's blocks when it ends instead. */
+int fcb_release_device_cache(void);
+
 /* FDK pre-processing on the GPU (fastcone.py:260-292): optional cosine weight
  * D / sqrt(D^2 + (h - zOrigin[t])^2 + (w - W/2)^2) in detector pixels, then the ramp
  * filter of fastcone.rampfilter (zero-pad rows to 2W, pi*|f| with DC = 1/8 of the first

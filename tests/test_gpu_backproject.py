@@ -63,6 +63,24 @@ def test_fdk_edge_cases(case):
     assert O.rel_l2(got, ref64) < 3e-5
 
 
+@pytest.mark.parametrize("vol_xyz", [(80, 48, 40), (40, 96, 36)])
+@pytest.mark.parametrize("arc0, arc1, nviews", [
+    (-0.17, 0.17, 24),        # views near 0 degrees: tiles run x fastest
+    (1.40, 1.74, 24),         # near 90 degrees: y fastest
+    (0.0, 2 * np.pi, 400),    # three launches of up to 180 views, each choosing its raster
+])
+def test_fdk_tile_raster(vol_xyz, arc0, arc1, nviews):
+    """Each launch runs its tiles with x or y fastest (the axis that moves the detector column
+    less over its views); on tile grids that are not square both orders must cover every tile
+    exactly once."""
+    angles = np.linspace(arc0, arc1, nviews, endpoint=False).astype(np.float32)
+    g, pb = make_case(vol_xyz=vol_xyz, det_wh=(128, 64), nviews=nviews, D=200.0, pw=1.0, angles=angles)
+    proj, _ = smooth_projections(pb)
+    got = _bp(g, proj, 2)
+    ref64 = O.backproject_f64(pb, proj, kernel_mode=2)
+    assert O.rel_l2(got, ref64) < 2e-5, O.rel_l2(got, ref64)
+
+
 def test_bp_accumulates():
     import torch
 
@@ -276,3 +294,36 @@ def test_host_driver_staging_of_large_pageable_buffers():
     assert np.array_equal(outs[0][0], outs[1][0])
     assert np.array_equal(outs[0][1], outs[1][1])
     assert not np.array_equal(outs[0][0], vol0)
+
+
+def test_host_driver_device_block_cache(monkeypatch):
+    """The host entry points keep a finished call's device blocks for later calls: calls that
+    reuse them (blocks holding the previous call's data), calls after the cache was released
+    and calls with the cache switched off give the same result, equal to the FP64 oracle."""
+    import ctypes
+
+    from fastcone_b200 import _lib
+
+    g, pb = make_case(vol_xyz=(64, 56, 40), det_wh=(96, 64), nviews=90, D=200.0, pw=1.0, seed=6)
+    proj, _ = smooth_projections(pb)
+    gs = g.struct()
+    L = _lib.lib()
+
+    def host_bp(p):
+        vol = np.zeros(g.vol_shape, np.float32)
+        _lib.check(L.fcb_backproject_host(0, ctypes.byref(gs), 2, p.ctypes.data_as(_lib.c_float_p),
+                                          vol.ctypes.data_as(_lib.c_float_p)))
+        return vol
+
+    first = host_bp(proj)
+    other = host_bp(np.ascontiguousarray(proj[::-1]))     # different data through the same blocks
+    again = host_bp(proj)
+    _lib.check(L.fcb_release_device_cache())
+    released = host_bp(proj)
+    monkeypatch.setenv("FCB_HOST_CACHE", "0")
+    uncached = host_bp(proj)
+    _lib.check(L.fcb_release_device_cache())
+    for v in (again, released, uncached):
+        assert np.array_equal(v, first)
+    assert not np.array_equal(other, first)
+    assert O.rel_l2(first, O.backproject_f64(pb, proj, kernel_mode=2)) < 2e-5

@@ -30,6 +30,13 @@ def test_library_loads_and_exports_header_symbols():
     assert L.fcb_version() >= 10000
 
 
+def test_release_device_cache_without_blocks():
+    """With no host call made there is nothing cached: releasing touches no device."""
+    from fastcone_b200 import _lib
+
+    assert _lib.lib().fcb_release_device_cache() == 0
+
+
 def test_invalid_arguments_return_status():
     from fastcone_b200 import _lib
     from tests._cases import make_case
