@@ -153,14 +153,23 @@ __device__ __forceinline__ bool fdk_tile_outside_window(const FdkParams& P, cons
 }
 
 // Pre-pass: the largest footprint over all (tile, view) pairs sizes the staging box.
+// Only the first and the last layer of z tiles are evaluated: for one view and one column of
+// tiles the box width does not depend on z (w depends on x, y only) and the continuous
+// extent of the rows, max over the corners of U (hb z1 + e) minus min of U (hb z0 + e), grows
+// with the tile's distance from the source plane on either side, so it is largest in one of
+// the two outer layers.  The plan adds one row for the floors of the box corners.
 __global__ void fdk_footprint_kernel(const __grid_constant__ FdkParams P, int nzt, int ntiles,
                                      int* out_need)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long total = (long long)ntiles * P.nviews;
+  const int layer = P.tiles_x * P.tiles_y;
+  const int nlayers = P.tiles_z > 1 ? 2 : 1;
+  const long long total = (long long)layer * nlayers * P.nviews;
+  (void)ntiles;
   int mw = 0, mh = 0;
   if (i < total) {
-    const int tile = (int)(i / P.nviews), v = (int)(i % P.nviews);
+    const int t = (int)(i / P.nviews), v = (int)(i % P.nviews);
+    const int tile = (t >= layer ? P.tiles_z - 1 : 0) * layer + t % layer;
     int tx, ty, tz;
     fdk_tile(P, tile, tx, ty, tz);
     int w0, h0, nw, nh;
@@ -1427,7 +1436,7 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
                                          cudaGetErrorString(cudaGetLastError()));
     }
     for (const FdkParams& P : pl->fdk) {
-      const long long total = (long long)ntiles * P.nviews;
+      const long long total = (long long)tiles_x * tiles_y * (tiles_z > 1 ? 2 : 1) * P.nviews;
       const int blocks = (int)((total + 255) / 256);
       fdk_footprint_kernel<<<blocks, 256, 0, st>>>(P, NZ, ntiles, need);
     }
@@ -1441,7 +1450,7 @@ static int bp_plan_build(const fcb_geometry* g, int kernelMode, int projType, in
     // different shared-memory banks (a multiple of 8 or 16 makes rows collide: at 48 the
     // slab case ran 13 % slower than at 44)
     if (projType == FCB_F32 && pl->BW % 8 == 0) pl->BW += 4;
-    pl->BH = h[1];
+    pl->BH = h[1] + 1;  // + 1: the inner z layers' corner floors (see fdk_footprint_kernel)
     if (pl->BW < align) pl->BW = align;
     if (pl->BH < 2) pl->BH = 2;
     // the largest dynamic shared memory a CTA of this device may opt into
