@@ -91,9 +91,27 @@ bool cache_enabled()
   return !(e && e[0] == '0');
 }
 
-// Frees the cached blocks of `dev` (-1: of every device); the caller holds g_cache_mu.
+// fcb_fbp_host's filter plans (cuFFT plans and about half a gigabyte of scratch each) are
+// kept the same way, keyed by their parameters, at most 4 per device.
+struct CachedFilter {
+  int dev, nviews, H, W, window;
+  fcb_filter_plan* p;
+};
+std::vector<CachedFilter> g_fcache;  // oldest first
+constexpr int CACHE_FILTERS_PER_DEVICE = 4;
+
+// Frees the cached blocks and filter plans of `dev` (-1: of every device); the caller holds
+// g_cache_mu.
 void cache_drop_locked(int dev)
 {
+  for (size_t i = 0; i < g_fcache.size();) {
+    if (dev < 0 || g_fcache[i].dev == dev) {
+      filter_plan_destroy(g_fcache[i].p);
+      g_fcache.erase(g_fcache.begin() + (long)i);
+    } else {
+      i++;
+    }
+  }
   if (g_cache.empty()) return;
   int cur = -1;
   cudaGetDevice(&cur);
@@ -179,9 +197,13 @@ struct Scratch {
     blocks.push_back(Block{*p, bytes});
     return FCB_OK;
   }
-  int stream(cudaStream_t* s)
+  // high: the device's highest stream priority (its kernels' CTAs take SMs ahead of the
+  // other streams' waiting CTAs)
+  int stream(cudaStream_t* s, bool high = false)
   {
-    FCB_CUDA_TRY(cudaStreamCreateWithFlags(s, cudaStreamNonBlocking));
+    int least = 0, greatest = 0;
+    if (high) FCB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    FCB_CUDA_TRY(cudaStreamCreateWithPriority(s, cudaStreamNonBlocking, high ? greatest : 0));
     streams.push_back(*s);
     return FCB_OK;
   }
@@ -450,23 +472,56 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
   FCB_TRY(sc.stream(&xs));
   FCB_TRY(sc.stream(&os));
   fcb_filter_plan* fplan = nullptr;
+  int fdev = -1, fkey[4] = {0, 0, 0, 0};  // the plan's device and (views, H, W, window)
   struct FilterGuard {
     fcb_filter_plan*& p;
     cudaStream_t& s;
+    int& dev;
+    int* key;
     ~FilterGuard()
     {
-      if (p) {
-        cudaStreamSynchronize(s);  // the plan's scratch is in use until the filter stream ends
+      if (!p) return;
+      cudaStreamSynchronize(s);  // the plan's scratch is in use until the filter stream ends
+      if (!cache_enabled()) {
         filter_plan_destroy(p);
+        return;
+      }
+      std::lock_guard<std::mutex> lk(g_cache_mu);
+      g_fcache.push_back(CachedFilter{dev, key[0], key[1], key[2], key[3], p});
+      int n = 0;
+      for (const CachedFilter& c : g_fcache) n += c.dev == dev;
+      for (size_t i = 0; i < g_fcache.size() && n > CACHE_FILTERS_PER_DEVICE;) {
+        if (g_fcache[i].dev == dev) {
+          filter_plan_destroy(g_fcache[i].p);
+          g_fcache.erase(g_fcache.begin() + (long)i);
+          n--;
+        } else {
+          i++;
+        }
       }
     }
-  } fguard{fplan, fs};
+  } fguard{fplan, fs, fdev, fkey};
   std::vector<cudaEvent_t> filt_done(ranges.size(), nullptr);
   if (ff) {
     int maxc = 1;
     for (const auto& r : ranges) maxc = std::max(maxc, r.second - r.first);
-    FCB_TRY(sc.stream(&fs));
-    FCB_TRY(filter_plan_create(maxc, H, W, FCB_F32, ff->window, 0.125, &fplan));
+    // the filter of chunk c + 1 runs while chunk c is backprojected; at high priority its
+    // CTAs are placed as the backprojection's retire instead of after all of them
+    FCB_TRY(sc.stream(&fs, true));
+    FCB_CUDA_TRY(cudaGetDevice(&fdev));
+    fkey[0] = maxc; fkey[1] = H; fkey[2] = W; fkey[3] = ff->window;
+    if (cache_enabled()) {
+      std::lock_guard<std::mutex> lk(g_cache_mu);
+      for (size_t i = 0; i < g_fcache.size(); i++) {
+        const CachedFilter& c = g_fcache[i];
+        if (c.dev == fdev && c.nviews == maxc && c.H == H && c.W == W && c.window == ff->window) {
+          fplan = c.p;
+          g_fcache.erase(g_fcache.begin() + (long)i);
+          break;
+        }
+      }
+    }
+    if (!fplan) FCB_TRY(filter_plan_create(maxc, H, W, FCB_F32, ff->window, 0.125, &fplan));
     FCB_TRY(sc.stream(&ps));
     if (ff->cosine) {
       FCB_TRY(sc.alloc((void**)&dz, (size_t)n * sizeof(float)));

@@ -19,40 +19,51 @@
 
 namespace fcb {
 
+// The three element-wise passes run on 2-D grids: x over a row's elements, y over the
+// batch's rows (at most 65535), so no thread divides its index (a 64-bit division and
+// remainder per element had made these passes several times slower than their memory
+// traffic).
+
 // Rows of W values at a pitch of `pitch` elements (pitch >= W) -> zero-padded rows of L.
 __global__ void pad_weight_kernel(const float* __restrict__ in, float* __restrict__ pad,
                                   long long row0, int nrows, int H, int W, int pitch, int L, float D,
                                   const float* __restrict__ zorig, int cosw)
 {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long total = (long long)nrows * L;
-  if (i >= total) return;
-  const int c = (int)(i % L);
-  const long long r = i / L;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  const long long gr = row0 + r;
+  __shared__ float s_hh;  // the row's detector height relative to its view's zOrigin
+  if (cosw) {
+    if (threadIdx.x == 0) {
+      const long long t = gr / H;
+      s_hh = (float)(gr - t * H) - zorig[t];
+    }
+    __syncthreads();
+  }
+  if (c >= L || r >= nrows) return;
   float v = 0.0f;
   if (c < W) {
-    const long long gr = row0 + r;
     v = in[gr * pitch + c];
     if (cosw) {
-      const int t = (int)(gr / H), h = (int)(gr % H);
-      const float hh = (float)h - zorig[t];
+      const float hh = s_hh;
       const float ww = (float)c - 0.5f * (float)W;
       v *= D / sqrtf(D * D + hh * hh + ww * ww);
     }
   }
-  pad[i] = v;
+  pad[(size_t)r * L + c] = v;
 }
 
 __global__ void spectrum_mul_kernel(cufftComplex* __restrict__ spec, const float* __restrict__ filt,
                                     int nrows, int nbins)
 {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nrows * nbins) return;
-  const float f = filt[i % nbins];
-  cufftComplex z = spec[i];
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (c >= nbins || r >= nrows) return;
+  const float f = filt[c];
+  cufftComplex z = spec[(size_t)r * nbins + c];
   z.x *= f;
   z.y *= f;
-  spec[i] = z;
+  spec[(size_t)r * nbins + c] = z;
 }
 
 template <typename T>
@@ -68,11 +79,10 @@ template <typename T>
 __global__ void crop_store_kernel(const float* __restrict__ pad, T* __restrict__ out, long long row0,
                                   int nrows, int W, int pitch, int L, float scale)
 {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= (long long)nrows * W) return;
-  const int c = (int)(i % W);
-  const long long r = i / W;
-  out[(row0 + r) * pitch + c] = to_store<T>(pad[r * L + c] * scale);
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int r = blockIdx.y;
+  if (c >= W || r >= nrows) return;
+  out[(row0 + r) * pitch + c] = to_store<T>(pad[(size_t)r * L + c] * scale);
 }
 
 // ------------------------------------------------------------------- phantom
@@ -195,7 +205,9 @@ try {
   pl->n2 = L;
   pl->nb = L / 2 + 1;
   const long long rows = (long long)nviews * H;
-  pl->batch = (int)std::min<long long>(rows, std::max<long long>(1, (256ll << 20) / (8ll * pl->n2)));
+  // rows per cuFFT batch: about 256 MB of padded rows, at most 65535 (the kernels' grid y)
+  pl->batch = (int)std::min<long long>(std::min<long long>(rows, 65535),
+                                       std::max<long long>(1, (256ll << 20) / (8ll * pl->n2)));
   int rc = FCB_OK;
   do {
     if (cudaMalloc(&pl->pad, (size_t)pl->batch * pl->n2 * sizeof(float)) != cudaSuccess ||
@@ -253,18 +265,16 @@ int filter_plan_run(fcb_filter_plan* pl, const float* in, void* out, int nviews,
   const long long rows = (long long)nviews * H;
   for (long long r0 = 0; r0 < rows; r0 += batch) {
     const int nr = (int)std::min<long long>(batch, rows - r0);
-    long long tot = (long long)nr * n2;
-    pad_weight_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(in, pl->pad, r0, nr, H, W, pitch, n2, D,
-                                                                   dzorig, cosineWeight);
+    pad_weight_kernel<<<dim3((unsigned)((n2 + 255) / 256), (unsigned)nr), 256, 0, st>>>(
+        in, pl->pad, r0, nr, H, W, pitch, n2, D, dzorig, cosineWeight);
     // cuFFT plans are for `batch` rows; the tail batch is zero-padded in `pad`
     if (nr < batch)
       FCB_CUDA_TRY(cudaMemsetAsync(pl->pad + (size_t)nr * n2, 0, (size_t)(batch - nr) * n2 * sizeof(float), st));
     if (cufftExecR2C(pl->pf, pl->pad, pl->spec) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecR2C failed");
-    tot = (long long)nr * nb;
-    spectrum_mul_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(pl->spec, pl->dfilt, nr, nb);
+    spectrum_mul_kernel<<<dim3((unsigned)((nb + 255) / 256), (unsigned)nr), 256, 0, st>>>(pl->spec, pl->dfilt,
+                                                                                         nr, nb);
     if (cufftExecC2R(pl->pi, pl->spec, pl->pad) != CUFFT_SUCCESS) return set_error(FCB_ERR_CUDA, "cufftExecC2R failed");
-    tot = (long long)nr * W;
-    const unsigned g = (unsigned)((tot + 255) / 256);
+    const dim3 g((unsigned)((W + 255) / 256), (unsigned)nr);
     if (pl->outType == FCB_F32)
       crop_store_kernel<float><<<g, 256, 0, st>>>(pl->pad, (float*)out, r0, nr, W, pitch, n2, scale);
     else if (pl->outType == FCB_F16)

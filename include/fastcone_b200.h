@@ -233,9 +233,10 @@ int fcb_sync_status(void* stream);
 
 /* The host-buffer entry points (GPU_CB_*, fcb_backproject_host, fcb_project_host,
  * fcb_fbp_host) keep the device blocks of a finished call and reuse them in later calls
- * that fit (at most 8 blocks per device; a failed allocation first returns them).  This
- * returns every kept block to the driver.  FCB_HOST_CACHE=0 in the environment frees each
- * call's blocks when it ends instead. */
+ * that fit (at most 8 blocks per device; a failed allocation first returns them), and
+ * fcb_fbp_host keeps its filter plans (cuFFT plans and scratch, at most 4 per device).  This
+ * returns everything kept to the driver.  FCB_HOST_CACHE=0 in the environment frees each
+ * call's blocks and plans when it ends instead. */
 int fcb_release_device_cache(void);
 
 /* FDK pre-processing on the GPU (fastcone.py:260-292): optional cosine weight
