@@ -126,3 +126,38 @@ def test_fbp_host_pipeline_vs_oracle(window, case):
     fc.fbp(vol, p, pb.angles, D, zorig, pixelWidth=case["pw"], window=window)
     assert O.rel_l2(p, filt) < 1e-5, O.rel_l2(p, filt)
     assert O.rel_l2(vol, want) < 2e-5, O.rel_l2(vol, want)
+
+
+def test_fbp_host_kept_filter_plans(monkeypatch):
+    """fcb_fbp_host keeps its filter plans between calls (keyed by views per chunk, detector
+    size and window): repeated calls, a call with another window in between, and calls with
+    the cache released or switched off give the same volume and filtered views."""
+    from fastcone_b200 import _lib
+    from fastcone_b200 import fastcone as fc
+    from tests._cases import make_case, smooth_projections
+
+    # a detector that covers the volume's shadow: the reference's sub-problem windows (which
+    # fastcone.fbp reproduces) then equal the ideal operator the oracle computes
+    g, pb = make_case(vol_xyz=(40, 36, 32), det_wh=(64, 48), nviews=130, D=130.0, pw=0.75,
+                      norm=np.full(130, 1.0 / 130, np.float32))
+    proj, _ = smooth_projections(pb)
+
+    def run(window):
+        vol = np.zeros((32, 36, 40), np.float32)
+        p = proj.copy()
+        fc.fbp(vol, p, pb.angles, 130.0, pb.hMid, pixelWidth=0.75, window=window)
+        return vol, p
+
+    first = run("shepplogan")
+    ramp = run("ramlak")
+    again = run("shepplogan")
+    _lib.check(_lib.lib().fcb_release_device_cache())
+    released = run("shepplogan")
+    monkeypatch.setenv("FCB_HOST_CACHE", "0")
+    uncached = run("shepplogan")
+    for v, p in (again, released, uncached):
+        assert np.array_equal(v, first[0]) and np.array_equal(p, first[1])
+    assert not np.array_equal(ramp[0], first[0])
+    want = O.backproject_f64(pb, O.rampfilter(O.fbp_cosine_weight(proj.astype(np.float64), 130.0, pb.hMid),
+                                              window="shepplogan").astype(np.float32), kernel_mode=2)
+    assert O.rel_l2(first[0], want) < 2e-5
