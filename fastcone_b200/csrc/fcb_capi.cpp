@@ -78,6 +78,7 @@ struct DeviceGuard {
 namespace {
 struct CachedBlock {
   int dev;
+  unsigned long long ctx;  // the context the block belongs to (a reset device has a new one)
   void* p;
   size_t bytes;
 };
@@ -94,37 +95,56 @@ bool cache_enabled()
 // fcb_fbp_host's filter plans (cuFFT plans and about half a gigabyte of scratch each) are
 // kept the same way, keyed by their parameters, at most 4 per device.
 struct CachedFilter {
-  int dev, nviews, H, W, window;
+  int dev;
+  unsigned long long ctx;
+  int nviews, H, W, window;
   fcb_filter_plan* p;
 };
 std::vector<CachedFilter> g_fcache;  // oldest first
 constexpr int CACHE_FILTERS_PER_DEVICE = 4;
 
-// Frees the cached blocks and filter plans of `dev` (-1: of every device); the caller holds
-// g_cache_mu.
+// Forgets the cached entries of `dev` made in another context than `ctx` (the device was
+// reset: their memory and plans went with the old context); the caller holds g_cache_mu.
+void cache_forget_stale_locked(int dev, unsigned long long ctx)
+{
+  for (size_t i = 0; i < g_cache.size();) {
+    if (g_cache[i].dev == dev && g_cache[i].ctx != ctx) g_cache.erase(g_cache.begin() + (long)i);
+    else i++;
+  }
+  for (size_t i = 0; i < g_fcache.size();) {
+    if (g_fcache[i].dev == dev && g_fcache[i].ctx != ctx) g_fcache.erase(g_fcache.begin() + (long)i);
+    else i++;
+  }
+}
+
+// Frees the cached blocks and filter plans of `dev` (-1: of every device); entries of a
+// context that is gone are only forgotten.  The caller holds g_cache_mu.
 void cache_drop_locked(int dev)
 {
+  if (g_cache.empty() && g_fcache.empty()) return;
+  int cur = -1;
+  cudaGetDevice(&cur);
+  auto live = [](int d, unsigned long long c) {
+    return cudaSetDevice(d) == cudaSuccess && current_context_id() == c;
+  };
   for (size_t i = 0; i < g_fcache.size();) {
     if (dev < 0 || g_fcache[i].dev == dev) {
-      filter_plan_destroy(g_fcache[i].p);
+      if (live(g_fcache[i].dev, g_fcache[i].ctx)) filter_plan_destroy(g_fcache[i].p);
       g_fcache.erase(g_fcache.begin() + (long)i);
     } else {
       i++;
     }
   }
-  if (g_cache.empty()) return;
-  int cur = -1;
-  cudaGetDevice(&cur);
   for (size_t i = 0; i < g_cache.size();) {
     if (dev < 0 || g_cache[i].dev == dev) {
-      cudaSetDevice(g_cache[i].dev);
-      cudaFree(g_cache[i].p);
+      if (live(g_cache[i].dev, g_cache[i].ctx)) cudaFree(g_cache[i].p);
       g_cache.erase(g_cache.begin() + (long)i);
     } else {
       i++;
     }
   }
   if (cur >= 0) cudaSetDevice(cur);
+  cudaGetLastError();
 }
 }  // namespace
 
@@ -135,6 +155,7 @@ struct Scratch {
     size_t bytes;
   };
   int dev = -1;
+  unsigned long long ctx = 0;
   std::vector<Block> blocks;
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;
@@ -150,7 +171,7 @@ struct Scratch {
     }
     // every stream of the call has finished: the blocks are free for the next call
     std::lock_guard<std::mutex> lk(g_cache_mu);
-    for (const Block& b : blocks) g_cache.push_back(CachedBlock{dev, b.p, b.bytes});
+    for (const Block& b : blocks) g_cache.push_back(CachedBlock{dev, ctx, b.p, b.bytes});
     int n = 0;
     for (const CachedBlock& c : g_cache) n += c.dev == dev;
     for (size_t i = 0; i < g_cache.size() && n > CACHE_BLOCKS_PER_DEVICE;) {
@@ -165,9 +186,14 @@ struct Scratch {
   }
   int alloc(void** p, size_t bytes)
   {
-    if (dev < 0) FCB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0) {
+      FCB_CUDA_TRY(cudaGetDevice(&dev));
+      FCB_CUDA_TRY(cudaFree(nullptr));  // make sure the device's context exists
+      ctx = current_context_id();
+    }
     if (cache_enabled()) {
       std::lock_guard<std::mutex> lk(g_cache_mu);
+      cache_forget_stale_locked(dev, ctx);
       long best = -1;
       for (size_t i = 0; i < g_cache.size(); i++) {
         const CachedBlock& c = g_cache[i];
@@ -473,10 +499,12 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
   FCB_TRY(sc.stream(&os));
   fcb_filter_plan* fplan = nullptr;
   int fdev = -1, fkey[4] = {0, 0, 0, 0};  // the plan's device and (views, H, W, window)
+  unsigned long long fctx = 0;             // and context
   struct FilterGuard {
     fcb_filter_plan*& p;
     cudaStream_t& s;
     int& dev;
+    unsigned long long& ctx;
     int* key;
     ~FilterGuard()
     {
@@ -487,7 +515,7 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
         return;
       }
       std::lock_guard<std::mutex> lk(g_cache_mu);
-      g_fcache.push_back(CachedFilter{dev, key[0], key[1], key[2], key[3], p});
+      g_fcache.push_back(CachedFilter{dev, ctx, key[0], key[1], key[2], key[3], p});
       int n = 0;
       for (const CachedFilter& c : g_fcache) n += c.dev == dev;
       for (size_t i = 0; i < g_fcache.size() && n > CACHE_FILTERS_PER_DEVICE;) {
@@ -500,7 +528,7 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
         }
       }
     }
-  } fguard{fplan, fs, fdev, fkey};
+  } fguard{fplan, fs, fdev, fctx, fkey};
   std::vector<cudaEvent_t> filt_done(ranges.size(), nullptr);
   if (ff) {
     int maxc = 1;
@@ -509,9 +537,11 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
     // CTAs are placed as the backprojection's retire instead of after all of them
     FCB_TRY(sc.stream(&fs, true));
     FCB_CUDA_TRY(cudaGetDevice(&fdev));
+    fctx = current_context_id();
     fkey[0] = maxc; fkey[1] = H; fkey[2] = W; fkey[3] = ff->window;
     if (cache_enabled()) {
       std::lock_guard<std::mutex> lk(g_cache_mu);
+      cache_forget_stale_locked(fdev, fctx);
       for (size_t i = 0; i < g_fcache.size(); i++) {
         const CachedFilter& c = g_fcache[i];
         if (c.dev == fdev && c.nviews == maxc && c.H == H && c.W == W && c.window == ff->window) {

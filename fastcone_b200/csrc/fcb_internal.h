@@ -55,6 +55,9 @@ enum : int { DEV_TIMEOUT = 1, DEV_RANGE = 2 };
 
 // Per-device status word (one int in global memory, allocated once per device).
 int device_status_ptr(int** p);
+// Unique id of the calling thread's current CUDA context (a reset device gets a new one);
+// 0 when there is none or the driver cannot tell.
+unsigned long long current_context_id();
 // Reads and clears the status word after synchronising `stream`.
 int collect_device_status(cudaStream_t stream);
 
