@@ -79,6 +79,21 @@ def _safe_inv(t, eps=1e-6):
 # times the ellipsoids, denser material (mean density x 1.8) and half the photons.
 IN_DISTRIBUTION = {"n_ellipsoids": None, "density": (0.1, 1.0), "i0": None}
 OUT_OF_DISTRIBUTION = {"n_ellipsoids": 30, "density": (0.5, 1.5), "i0": 5e3}
+# beyond every range of the mixed training distribution below (more ellipsoids, denser,
+# fewer photons)
+FAR_OUT_OF_DISTRIBUTION = {"n_ellipsoids": 40, "density": (1.0, 2.2), "i0": 2.5e3}
+
+
+def mixed_params(seed: int) -> dict:
+    """Phantom and noise parameters of the mixed training distribution, drawn per phantom from
+    its seed: 5-30 ellipsoids, densities U(lo, hi) with lo ~ U(0.05, 0.6) and hi - lo ~
+    U(0.5, 1.0), I0 log-uniform in [4e3, 2e4] photons."""
+    rng = np.random.default_rng(seed + 7919)
+    k = int(rng.integers(5, 31))
+    lo = float(rng.uniform(0.05, 0.6))
+    hi = lo + float(rng.uniform(0.5, 1.0))
+    i0 = float(10.0 ** rng.uniform(math.log10(4e3), math.log10(2e4)))
+    return {"n_ellipsoids": k, "density": (lo, hi), "i0": i0}
 
 
 def make_sample(ops_: Operators, seed: int, device="cuda", n_ellipsoids=None, density=(0.1, 1.0), i0=None):
@@ -192,9 +207,12 @@ def step_weights(steps: int = STEPS, final: float = 2.0):
 
 
 def train(net: UnrolledNet, geom: ConeGeometry, n_phantoms: int = 2000, lr: float = 1e-3, seed0: int = 1000,
-          log_every: int = 50, checkpoint: str | None = None, log=print, deep: bool = True):
+          log_every: int = 50, checkpoint: str | None = None, log=print, deep: bool = True,
+          mixed: bool = False):
     """Trains on seeded phantoms generated (and projected) on the GPU, one per step.
-    deep=True supervises every step's output (step_weights), else only the last."""
+    deep=True supervises every step's output (step_weights), else only the last.
+    mixed=True draws each phantom's parameters from mixed_params (else the fixed training
+    distribution: N_ELLIPSOIDS ellipsoids, densities U(0.1, 1), I0 photons)."""
     ops_ = Operators(geom)
     mask = fov_mask(ops_.g)
     opt = torch.optim.Adam(net.parameters(), lr=lr)
@@ -202,7 +220,7 @@ def train(net: UnrolledNet, geom: ConeGeometry, n_phantoms: int = 2000, lr: floa
     wk = step_weights(net.steps) if deep else [0.0] * (net.steps - 1) + [1.0]
     t0 = time.time()
     for i in range(n_phantoms):
-        mu, y = make_sample(ops_, seed0 + i)
+        mu, y = make_sample(ops_, seed0 + i, **(mixed_params(seed0 + i) if mixed else {}))
         with torch.no_grad():
             x0 = ops_.fdk(y)
         outs = []
@@ -219,7 +237,7 @@ def train(net: UnrolledNet, geom: ConeGeometry, n_phantoms: int = 2000, lr: floa
                 f"t {time.time() - t0:.0f}s")
         if checkpoint and (i + 1) % 500 == 0:
             torch.save({"model": net.state_dict(), "optim": opt.state_dict(), "phantoms_seen": i + 1,
-                        "seed0": seed0, "deep": deep}, checkpoint)
+                        "seed0": seed0, "deep": deep, "mixed": mixed}, checkpoint)
     return net
 
 
@@ -299,6 +317,7 @@ def main():
     ap.add_argument("--eval", type=int, default=0, help="number of held-out phantoms to evaluate")
     ap.add_argument("--out", default=None, help="write the evaluation JSON here")
     ap.add_argument("--final-only", action="store_true", help="supervise only the last step")
+    ap.add_argument("--mixed", action="store_true", help="train on the mixed distribution (mixed_params)")
     a = ap.parse_args()
     torch.manual_seed(0)
     geom = configs.learned_sparse()
@@ -306,10 +325,10 @@ def main():
     if a.weights and a.train == 0:
         net.load_state_dict(torch.load(a.weights, map_location="cuda")["model"])
     if a.train:
-        train(net, geom, a.train, a.lr, checkpoint=a.weights, deep=not a.final_only)
+        train(net, geom, a.train, a.lr, checkpoint=a.weights, deep=not a.final_only, mixed=a.mixed)
         if a.weights:
-            torch.save({"model": net.state_dict(), "phantoms_seen": a.train, "deep": not a.final_only},
-                       a.weights)
+            torch.save({"model": net.state_dict(), "phantoms_seen": a.train, "deep": not a.final_only,
+                        "mixed": a.mixed}, a.weights)
     if a.eval:
         r = evaluate(net, geom, list(range(1, a.eval + 1)))
         s = json.dumps(r)
