@@ -907,14 +907,19 @@ def main():
 
         gl = configs.learned_sparse()
         r_in = learned.evaluate(net, gl, seeds=[1, 2], sirt_iters=100)
-        r_out = learned.evaluate(net, gl, seeds=[3, 4], sirt_iters=100, dist=learned.OUT_OF_DISTRIBUTION)
+        r_shift = learned.evaluate(net, gl, seeds=[3, 4], sirt_iters=100, dist=learned.OUT_OF_DISTRIBUTION)
+        r_far = learned.evaluate(net, gl, seeds=[5, 6], sirt_iters=100, dist=learned.FAR_OUT_OF_DISTRIBUTION)
         learned_res = {
             "workload": "256^3, 90 views, 384x256; 8 unrolled steps vs SIRT-100 from zero; each method timed "
                         "as the median of 3 passes after one untimed pass (CUDA events)",
-            "in_distribution": summary(r_in, "training distribution, held-out seeds 1, 2: 10 ellipsoids, "
-                                             "densities U(0.1, 1), Poisson I0 = 1e4"),
-            "out_of_distribution": summary(r_out, "seeds 3, 4: 30 ellipsoids, densities U(0.5, 1.5), "
-                                                  "Poisson I0 = 5e3"),
+            "training": "2000 seeded phantoms, each with 5-30 ellipsoids, densities U(lo, lo + 0.5..1.0) with "
+                        "lo in 0.05..0.6, Poisson I0 log-uniform in 4e3..2e4 (learned.mixed_params)",
+            "in_distribution": summary(r_in, "held-out seeds 1, 2: 10 ellipsoids, densities U(0.1, 1), "
+                                             "Poisson I0 = 1e4 (inside the training ranges)"),
+            "shifted": summary(r_shift, "seeds 3, 4: 30 ellipsoids, densities U(0.5, 1.5), Poisson I0 = 5e3 "
+                                        "(at the edge of the training ranges)"),
+            "out_of_distribution": summary(r_far, "seeds 5, 6: 40 ellipsoids, densities U(1.0, 2.2), Poisson "
+                                                  "I0 = 2.5e3 (outside every training range)"),
         }
         del net
         torch.cuda.empty_cache()

@@ -49,8 +49,9 @@ def test_training_gains_over_fallback():
 
 
 def test_committed_weights_beat_sirt100_at_full_size():
-    """The shipped network (trained on 2000 seeded phantoms at 256^3 / 90 views, weights in
-    fastcone_b200/weights) on a phantom outside its training seeds: one learned step already
+    """The shipped network (trained on 2000 seeded phantoms of learned.mixed_params at 256^3 /
+    90 views, weights in fastcone_b200/weights) on a phantom outside its training seeds, drawn
+    from the fixed 10-ellipsoid distribution: one learned step already
     exceeds the PSNR of 100 SIRT iterations, and the full 8 steps beat the fallback
     (FDK + 8 SIRT steps) by a wide margin."""
     import os
