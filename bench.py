@@ -543,14 +543,19 @@ class CpuReferencePath:
                 f"(oracle/fc_oracle.c, {self.cores} threads), {dt:.1f} s")
 
 
-def cpu_baseline(g, target_s=12.0):
-    """One bounded sample of the CPU reference path (about `target_s` seconds); returns the
-    cpu_baseline object of the JSON line."""
+def cpu_baseline(g, target_s=6.0, runs=2):
+    """The best of `runs` bounded samples of the CPU reference path (about `target_s` seconds
+    each, different random columns); returns the cpu_baseline object of the JSON line."""
     ref = CpuReferencePath(g)
     ref.calibrate(target_s)
-    dt, upd = ref.sample()
+    best = None
+    for _ in range(runs):
+        dt, upd = ref.sample()
+        if best is None or upd / dt > best[1] / best[0]:
+            best = (dt, upd)
+    dt, upd = best
     return {"value": upd / dt / 1e9, "unit": UNIT, "cores": ref.cores, "kind": "port",
-            "sample": ref.describe(dt, upd)}
+            "sample": f"best of {runs}: " + ref.describe(dt, upd)}
 
 
 def reference_line(args, g, budget_s=150.0):

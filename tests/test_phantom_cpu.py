@@ -36,3 +36,23 @@ def test_voxelised_phantom_is_the_sum_of_its_ellipsoids():
     parts = sum(O.phantom_voxelize(vol, p[k:k + 1]) for k in range(3))
     assert np.allclose(whole, parts, atol=1e-6)
     assert whole.max() > 0 and whole.shape == vol[::-1]
+
+
+def test_mixed_training_distribution():
+    """learned.mixed_params: deterministic per seed, inside its stated ranges, and the far
+    evaluation set lies outside every one of them."""
+    import math
+
+    from fastcone_b200 import learned
+
+    ps = [learned.mixed_params(s) for s in range(1000, 1400)]
+    assert ps[0] == learned.mixed_params(1000)
+    for p in ps:
+        lo, hi = p["density"]
+        assert 5 <= p["n_ellipsoids"] <= 30
+        assert 0.05 <= lo <= 0.6 and 0.5 <= hi - lo <= 1.0
+        assert 4e3 * (1 - 1e-9) <= p["i0"] <= 2e4 * (1 + 1e-9)
+    assert len({p["n_ellipsoids"] for p in ps}) > 20
+    assert min(math.log10(p["i0"]) for p in ps) < 3.7 and max(math.log10(p["i0"]) for p in ps) > 4.2
+    far = learned.FAR_OUT_OF_DISTRIBUTION
+    assert far["n_ellipsoids"] > 30 and far["density"][1] > 1.6 and far["i0"] < 4e3
