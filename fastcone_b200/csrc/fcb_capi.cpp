@@ -481,11 +481,29 @@ static int backproject_host_impl(int device, const fcb_geometry* g0, int kernelM
   int nslab = g.referenceWindows ? 1 : std::max(1, std::min(8, nz / 64));
   const int slab = ((nz + nslab - 1) / nslab + zt - 1) / zt * zt;
   nslab = (nz + slab - 1) / slab;
-  std::vector<int> z0(nslab), z1(nslab);
-  for (int s = 0; s < nslab; s++) {
-    z0[s] = s * slab;
-    z1[s] = std::min(nz, z0[s] + slab);
+  std::vector<int> z0, z1;
+  // With four slabs or more the first and the last are small (64 planes rounded up to the z
+  // tile): the first slab's upload delays the first kernel and the last slab's download
+  // follows the last one, and neither overlaps anything.  Slab boundaries stay on z-tile
+  // boundaries (a slab is a range of the plan's z tiles).
+  const int ntz = (nz + zt - 1) / zt, et = (64 + zt - 1) / zt;  // tiles: all, per edge slab
+  if (nslab >= 4 && ntz >= 4 * et) {
+    const int nmid = nslab - 2, mt = (ntz - 2 * et + nmid - 1) / nmid;
+    z0.push_back(0);
+    z1.push_back(et * zt);
+    for (int t = et; t < ntz - et; t += mt) {
+      z0.push_back(t * zt);
+      z1.push_back(std::min(ntz - et, t + mt) * zt);
+    }
+    z0.push_back((ntz - et) * zt);
+    z1.push_back(nz);
+  } else {
+    for (int s = 0; s < nslab; s++) {
+      z0.push_back(s * slab);
+      z1.push_back(std::min(nz, s * slab + slab));
+    }
   }
+  nslab = (int)z0.size();
 
   const size_t plane = (size_t)nx * ny;
   const size_t nvox = plane * nz;
