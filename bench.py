@@ -219,7 +219,7 @@ def parse():
                          "default for N > 1); z: one volume in z-slabs, every rank holding all views")
     ap.add_argument("--case", default=None,
                     choices=["fdk-slab", "fdk-slab-bf16", "proj-512", "proj-256", "conv-256", "katsevich",
-                             "pipeline", "misaligned-256"],
+                             "pipeline", "misaligned-256", "fdk-filter"],
                     help="profiling case: run only this kernel on a reduced workload (no JSON line)")
     return ap.parse_args()
 
@@ -234,6 +234,8 @@ def run_case(args):
     activation): forward (three kernel forms) and weight gradient (tensor cores and the
     CUDA-core kernel), all on tcgen05 except the last;
     katsevich: the helical PI-window backprojection (512x512x384, 4640 views; 1.3 GB);
+    fdk-filter: the FDK filter (cosine weight + Shepp-Logan) of the 1440 x 1024 x 1536
+    projections of the 1024^3 workload through a filter plan, in place (9.06 GB);
     misaligned-256: the general-matrix backprojector (a misaligned detector, unweighted) on
     256^3 / 360 views / 384x256 through a plan, CUDA events over the timed calls;
     pipeline: every other kernel once at a moderate size, inputs above L2 where the workload
@@ -270,6 +272,19 @@ def run_case(args):
         ms = e0.elapsed_time(e1) / args.steps
         upd = 1024 * 1024 * 128 * n
         print(json.dumps({"case": args.case, "ms": ms, "GUPS": upd / ms / 1e6, "box": plan.info()}))
+    elif args.case == "fdk-filter":
+        p = torch.randn((NVIEWS, DET[1], DET[0]), device=dev)
+        zorig = np.full(NVIEWS, DET[1] / 2.0, np.float32)
+        plan = ops.FilterPlan(tuple(p.shape), window=_lib.FILTER_SHEPPLOGAN)
+        for _ in range(args.warmup):
+            plan(p, zorigin=zorig, D=2500.0, out=p)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            plan(p, zorigin=zorig, D=2500.0, out=p)
+        e1.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"case": args.case, "ms": e0.elapsed_time(e1) / args.steps, "views": NVIEWS}))
     elif args.case == "katsevich":
         from fastcone_b200 import configs
 
